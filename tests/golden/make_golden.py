@@ -1,0 +1,97 @@
+"""Generate the golden fixtures in this directory by running the reference
+extension itself.
+
+Run on a machine with a CUDA GPU, after ``python oracle/build_ref.py`` has
+compiled the reference's own ``csrc`` sources into ``oracle/_ref/knn_ref_C.so``:
+
+    python tests/golden/make_golden.py --out tests/golden
+
+Each case draws seeded inputs on the CPU, copies them to ``cuda:0``, calls the
+reference ops ``knn_aggregate_aniso_forward`` (``csrc/forward.cu:286-338``),
+``knn_aggregate_aniso_backward`` (``csrc/backward.cu:331-389``) and
+``knn_aggregate_aniso_backward_2nd`` (``csrc/backward.cu:392-455``) exactly as
+the reference's autograd Functions do (``cuda_knn_aggregate/__init__.py:88,
+235, 276``, with a zero ``grad_w_out``), and stores inputs and outputs in one
+compressed ``.npz`` per case.  The inputs are stored too, so the fixtures
+stand alone: the CPU tests never regenerate them.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import os
+import sys
+
+import numpy as np
+import torch
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.join(ROOT, "cuda-knn-aniso-gaussian-feature-aggregation_b200"))
+from cuda_knn_aggregate import workloads as W  # noqa: E402
+
+
+def load_ref():
+    path = os.path.join(ROOT, "oracle", "_ref", "knn_ref_C.so")
+    spec = importlib.util.spec_from_file_location("knn_ref_C", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def cases():
+    """(name, (q,p,f,sigma,R), K, seed for the incoming gradients)."""
+    out = []
+    shape, t = W.make("small")
+    out.append(("small", t, shape.K))
+    out.append(("readme", W.readme_cloud(2, 300, 200, 16, seed=11), 8))
+    out.append(("ties", W.lattice_ties(B=2, n_side=4, Q=96, F=8, seed=7), 8))
+    _, t = W.make("small", B=1, Q=128, P=16, F=8, seed=21)
+    out.append(("k_eq_p", t, 16))
+    _, t = W.make("small", B=2, Q=200, P=300, F=5, seed=22)
+    out.append(("k1_f5", t, 1))
+    _, t = W.make("small", B=1, Q=150, P=200, F=1, seed=23)
+    out.append(("f1", t, 7))
+    _, t = W.make("small", B=1, Q=256, P=128, F=4, seed=24)
+    out.append(("allkeys", t, 128))
+    _, t = W.make("small", B=1, Q=128, P=4096, F=8, seed=25)
+    out.append(("table_slice", t, 16))
+    return out
+
+
+def run_case(ref, tensors, K, seed):
+    q, p, f, sigma, R = [x.cuda().contiguous() for x in tensors]
+    B, Q, F = q.shape[0], q.shape[1], f.shape[2]
+    f_out, w_out, dists, idxs = ref.knn_aggregate_aniso_forward(q, p, f, sigma, R, K)
+    g = torch.Generator().manual_seed(seed)
+    gfo = torch.randn(B, Q, F, generator=g).cuda()
+    ggq = torch.randn(B, Q, 3, generator=g).cuda()
+    gwo = torch.zeros(B, Q, K, device="cuda")
+    b1 = ref.knn_aggregate_aniso_backward(gfo, gwo, q, p, f, sigma, R, w_out, idxs)
+    b2 = ref.knn_aggregate_aniso_backward_2nd(ggq, gfo, gwo, q, p, f, sigma, R, w_out, idxs)
+    torch.cuda.synchronize()
+    c = lambda x: x.detach().cpu().numpy()
+    rec = dict(q=c(q), p=c(p), f=c(f), sigma=c(sigma), R=c(R), K=np.int64(K),
+               f_out=c(f_out), w_out=c(w_out), dists=c(dists), idxs=c(idxs).astype(np.int32),
+               gfo=c(gfo), ggq=c(ggq))
+    for n, v in zip(("dq", "dp", "df", "dsigma", "dR"), b1):
+        rec["b1_" + n] = c(v)
+    for n, v in zip(("dgfo", "dq", "dp", "df", "dsigma", "dR"), b2):
+        rec["b2_" + n] = c(v)
+    return rec
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=os.path.dirname(os.path.abspath(__file__)))
+    a = ap.parse_args()
+    os.makedirs(a.out, exist_ok=True)
+    ref = load_ref()
+    for i, (name, t, K) in enumerate(cases()):
+        rec = run_case(ref, t, K, seed=500 + i)
+        path = os.path.join(a.out, f"ref_{name}.npz")
+        np.savez_compressed(path, **rec)
+        print(f"{name}: {os.path.getsize(path)} bytes")
+
+
+if __name__ == "__main__":
+    main()
