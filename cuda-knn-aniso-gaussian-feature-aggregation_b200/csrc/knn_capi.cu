@@ -1,0 +1,199 @@
+// C ABI of libknn_aniso.so (declared in include/knn_aniso.h): argument
+// validation, workspace sizing, and dispatch to the kernels.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "knn_aniso.h"
+#include "knn_common.cuh"
+#include "knn_internal.h"
+
+using namespace knnag;
+
+namespace {
+
+constexpr int64_t kI32Max = 2147483647;
+
+int check_sizes(int B, int Q, int P, int F, int K) {
+  if (B < 0 || Q < 0 || P < 0 || F < 0) return KNNAG_ERR_ARG;
+  if (K < 1 || K > P) return KNNAG_ERR_K;
+  if ((int64_t)B * Q * K > kI32Max || (int64_t)B * P > kI32Max / kRecLen ||
+      (int64_t)B * round_up(P, kTilePoints) * kRecLen > kI32Max * 4LL)
+    return KNNAG_ERR_TOO_LARGE;
+  return KNNAG_OK;
+}
+
+inline bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+}  // namespace
+
+extern "C" {
+
+const char* knnag_status_string(int status) {
+  switch (status) {
+    case KNNAG_OK: return "ok";
+    case KNNAG_ERR_ARG: return "invalid argument (null pointer or negative size)";
+    case KNNAG_ERR_K: return "K must satisfy 1 <= K <= P";
+    case KNNAG_ERR_DTYPE: return "unsupported dtype (float32 or float64 only)";
+    case KNNAG_ERR_WORKSPACE: return "workspace too small or not 16-byte aligned";
+    case KNNAG_ERR_TOO_LARGE: return "problem exceeds the 32-bit entry index range";
+    case KNNAG_ERR_CUDA: return "CUDA launch failed";
+    case KNNAG_ERR_DEVICE: return "device-side error latched (a bounded wait gave up)";
+    default: return "unknown status";
+  }
+}
+
+int knnag_version(void) { return 10000; }
+
+size_t knnag_forward_workspace_bytes(int B, int Q, int P, int F, int K, int dtype) {
+  (void)F;
+  if (B < 0 || Q < 0 || P < 0 || K < 1) return 0;
+  return fwd_layout(B, Q, P, K, dtype, true).total;
+}
+
+size_t knnag_points_bytes(int B, int P, int dtype) {
+  return (size_t)B * P * kRecLen * (dtype == KNNAG_F64 ? 8 : 4);
+}
+
+size_t knnag_adjacency_bytes(int B, int Q, int P, int K) { return adj_layout(B, Q, P, K).total; }
+
+size_t knnag_backward_workspace_bytes(int B, int Q, int P, int F, int K, int dtype) {
+  return bwd_layout(B, Q, P, F, K, dtype).total;
+}
+
+int knnag_forward(const void* q, const void* p, const void* f, const void* sigma, const void* R, int B, int Q,
+                  int P, int F, int K, int dtype, void* f_out, void* w_out, void* dists, int64_t* idxs,
+                  void* points, void* workspace, size_t workspace_bytes, void* stream) {
+  if (dtype != KNNAG_F32 && dtype != KNNAG_F64) return KNNAG_ERR_DTYPE;
+  int rc = check_sizes(B, Q, P, F, K);
+  if (rc) return rc;
+  if ((int64_t)B * Q == 0) return KNNAG_OK;
+  if (!q || !p || !sigma || !R || !w_out || !dists || !idxs || !workspace) return KNNAG_ERR_ARG;
+  if (F > 0 && (!f || !f_out)) return KNNAG_ERR_ARG;
+  if (workspace_bytes < fwd_layout(B, Q, P, K, dtype, points == nullptr).total || !aligned16(workspace) ||
+      (points && !aligned16(points)))
+    return KNNAG_ERR_WORKSPACE;
+  return forward_impl(q, p, f, sigma, R, B, Q, P, F, K, dtype, f_out, w_out, dists, idxs, points, workspace,
+                      static_cast<cudaStream_t>(stream));
+}
+
+int knnag_pack_points(const void* p, const void* sigma, const void* R, int B, int P, int dtype, void* points,
+                      void* stream) {
+  if (dtype != KNNAG_F32 && dtype != KNNAG_F64) return KNNAG_ERR_DTYPE;
+  if (B < 0 || P < 0) return KNNAG_ERR_ARG;
+  if ((int64_t)B * P == 0) return KNNAG_OK;
+  if (!p || !sigma || !R || !points) return KNNAG_ERR_ARG;
+  return launch_pack_points(p, sigma, R, B, P, dtype, points, static_cast<cudaStream_t>(stream));
+}
+
+int knnag_build_adjacency(const int64_t* idxs, int B, int Q, int P, int K, void* adjacency, void* stream) {
+  int rc = check_sizes(B, Q, P, 0, K);
+  if (rc) return rc;
+  if (!adjacency || (!idxs && (int64_t)B * Q > 0)) return KNNAG_ERR_ARG;
+  if ((int64_t)B * P == 0) return KNNAG_OK;
+  return launch_build_adjacency(idxs, B, Q, P, K, adjacency, static_cast<cudaStream_t>(stream));
+}
+
+static int backward_common(BwdArgs& x, size_t workspace_bytes, void* stream) {
+  if (x.dtype != KNNAG_F32 && x.dtype != KNNAG_F64) return KNNAG_ERR_DTYPE;
+  int rc = check_sizes(x.B, x.Q, x.P, x.F, x.K);
+  if (rc) return rc;
+  if (x.needs & ~KNNAG_NEED_ALL) return KNNAG_ERR_ARG;
+  if ((int64_t)x.B * x.Q == 0 && (int64_t)x.B * x.P == 0) return KNNAG_OK;
+  if (!x.gfo || !x.q || !x.p || !x.sigma || !x.R || !x.idxs || !x.workspace) return KNNAG_ERR_ARG;
+  if (x.F > 0 && !x.f) return KNNAG_ERR_ARG;
+  if (x.order == 2 && !x.ggq) return KNNAG_ERR_ARG;
+  if (((x.needs & KNNAG_NEED_DQ) && !x.dq) || ((x.needs & KNNAG_NEED_DP) && !x.dp) ||
+      ((x.needs & KNNAG_NEED_DF) && !x.df && x.F > 0) || ((x.needs & KNNAG_NEED_DSIGMA) && !x.dsigma) ||
+      ((x.needs & KNNAG_NEED_DR) && !x.dR) || ((x.needs & KNNAG_NEED_DGFO) && !x.dgfo && x.F > 0))
+    return KNNAG_ERR_ARG;
+  if (workspace_bytes < bwd_layout(x.B, x.Q, x.P, x.F, x.K, x.dtype).total || !aligned16(x.workspace))
+    return KNNAG_ERR_WORKSPACE;
+  return backward_impl(x, static_cast<cudaStream_t>(stream));
+}
+
+int knnag_backward(const void* grad_f_out, const void* grad_w_out, const void* q, const void* p, const void* f,
+                   const void* sigma, const void* R, const void* w_out, const int64_t* idxs, int B, int Q, int P,
+                   int F, int K, int dtype, int needs, const void* points, const void* adjacency, void* dq,
+                   void* dp, void* df, void* dsigma, void* dR, void* coef_out, void* workspace,
+                   size_t workspace_bytes, void* stream) {
+  (void)grad_w_out;  // ignored, as in the reference
+  BwdArgs x{};
+  x.order = 1;
+  x.gfo = grad_f_out;
+  x.q = q;
+  x.p = p;
+  x.f = f;
+  x.sigma = sigma;
+  x.R = R;
+  x.w_in = w_out;
+  x.idxs = idxs;
+  x.B = B;
+  x.Q = Q;
+  x.P = P;
+  x.F = F;
+  x.K = K;
+  x.dtype = dtype;
+  x.needs = needs & ~KNNAG_NEED_DGFO;
+  x.points = points;
+  x.adjacency = adjacency;
+  x.dq = dq;
+  x.dp = dp;
+  x.df = df;
+  x.dsigma = dsigma;
+  x.dR = dR;
+  x.coef_out = coef_out;
+  x.workspace = workspace;
+  return backward_common(x, workspace_bytes, stream);
+}
+
+int knnag_backward_2nd(const void* grad_grad_q, const void* grad_f_out, const void* grad_w_out, const void* q,
+                       const void* p, const void* f, const void* sigma, const void* R, const void* w_out,
+                       const int64_t* idxs, int B, int Q, int P, int F, int K, int dtype, int needs,
+                       const void* points, const void* adjacency, const void* coef, void* dgfo, void* dq, void* dp,
+                       void* df, void* dsigma, void* dR, void* workspace, size_t workspace_bytes, void* stream) {
+  (void)grad_w_out;
+  BwdArgs x{};
+  x.order = 2;
+  x.ggq = grad_grad_q;
+  x.gfo = grad_f_out;
+  x.q = q;
+  x.p = p;
+  x.f = f;
+  x.sigma = sigma;
+  x.R = R;
+  x.w_in = w_out;
+  x.idxs = idxs;
+  x.B = B;
+  x.Q = Q;
+  x.P = P;
+  x.F = F;
+  x.K = K;
+  x.dtype = dtype;
+  x.needs = needs;
+  x.points = points;
+  x.adjacency = adjacency;
+  x.coef_in = coef;
+  x.dgfo = dgfo;
+  x.dq = dq;
+  x.dp = dp;
+  x.df = df;
+  x.dsigma = dsigma;
+  x.dR = dR;
+  x.workspace = workspace;
+  return backward_common(x, workspace_bytes, stream);
+}
+
+int knnag_read_device_status(void* workspace, void* stream) {
+  if (!workspace) return KNNAG_ERR_ARG;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int h = 0;
+  if (cudaMemcpyAsync(&h, workspace, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return KNNAG_ERR_CUDA;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return KNNAG_ERR_CUDA;
+  if (h != 0) {
+    cudaMemsetAsync(workspace, 0, sizeof(int), st);
+    return KNNAG_ERR_DEVICE;
+  }
+  return KNNAG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,162 @@
+// Shared device/host definitions for the anisotropic kNN aggregation kernels.
+//
+// Key arithmetic.  For a query q and point i the reference computes
+// (csrc/forward.cu:85-92)
+//     x = q0 - p0, y = q1 - p1, z = q2 - p2
+//     j = R00*x + R01*y + R02*z   (k, l likewise with rows 1 and 2)
+//     s = j*j*s0 + k*k*s1 + l*l*s2
+// and nvcc (-fmad=true) contracts it to
+//     j = fma(R02, z, fma(R00, x, R01*y))
+//     s = fma(l*l, s2, fma(j*j, s0, (k*k)*s1))
+// -- pinned bit for bit against the reference extension on a B200 over 2.7M
+// keys.  Every key below is written with explicit round-to-nearest
+// intrinsics in exactly that order so the compiler cannot re-contract it;
+// x is formed as q + (-p) from pre-negated coordinates, which IEEE defines
+// to be the same value as q - p.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "knn_aniso.h"
+
+namespace knnag {
+
+// ---------------------------------------------------------------- records
+// Per-point record (16 values of T): the packed form every kernel gathers.
+enum RecField {
+  kNPX = 0, kNPY = 1, kNPZ = 2,   // -p
+  kR00 = 3,                       // R row-major, 9 values: kR00 + 3*row + col
+  kS0 = 12, kS1 = 13, kS2 = 14,   // sigma
+  kRecPad = 15,
+  kRecLen = 16
+};
+
+// Points per search tile and the pair-interleaved tile layout: a pair of
+// points (2m, 2m+1) is 16 float2 = 128 bytes, field f of the pair at float2
+// slot f, so packed f32x2 arithmetic reads both points' field with one load.
+constexpr int kTilePoints = 256;
+constexpr int kPairFloats = 32;
+
+__host__ __device__ inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+// ---------------------------------------------------------------- status
+// Word 0 of every workspace: device-side error latch.  Word 1: number of
+// queries flagged for the exact MinK replay.
+constexpr int kStatusWaitTimeout = 1;
+
+// ---------------------------------------------------------------- keys
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// One rotated coordinate u = r0*x + r1*y + r2*z in the reference's rounding.
+template <typename T>
+__device__ __forceinline__ T row_dot(T r0, T r1, T r2, T x, T y, T z) {
+  return fma_rn(r2, z, fma_rn(r0, x, mul_rn(r1, y)));
+}
+
+// s = j*j*s0 + k*k*s1 + l*l*s2 in the reference's rounding.
+template <typename T>
+__device__ __forceinline__ T quad_form(T j, T k, T l, T s0, T s1, T s2) {
+  return fma_rn(mul_rn(l, l), s2, fma_rn(mul_rn(j, j), s0, mul_rn(mul_rn(k, k), s1)));
+}
+
+// Key from an already formed offset (x, y, z) and a row-major R.
+template <typename T>
+__device__ __forceinline__ T key_from_offset(T x, T y, T z, const T* r, T s0, T s1, T s2) {
+  const T j = row_dot(r[0], r[1], r[2], x, y, z);
+  const T k = row_dot(r[3], r[4], r[5], x, y, z);
+  const T l = row_dot(r[6], r[7], r[8], x, y, z);
+  return quad_form(j, k, l, s0, s1, s2);
+}
+
+// Key of query (qx,qy,qz) against a per-point record.
+template <typename T>
+__device__ __forceinline__ T key_rec(T qx, T qy, T qz, const T* rec) {
+  T x = add_rn(qx, rec[kNPX]);
+  T y = add_rn(qy, rec[kNPY]);
+  T z = add_rn(qz, rec[kNPZ]);
+  return key_from_offset(x, y, z, rec + kR00, rec[kS0], rec[kS1], rec[kS2]);
+}
+
+// Packed key of one query (duplicated into both halves of qx2..) against a
+// point pair: 18 packed FP32 instructions for two keys.
+__device__ __forceinline__ float2 key_pair(float2 qx2, float2 qy2, float2 qz2, const float2* pr) {
+  float2 x = __fadd2_rn(qx2, pr[kNPX]);
+  float2 y = __fadd2_rn(qy2, pr[kNPY]);
+  float2 z = __fadd2_rn(qz2, pr[kNPZ]);
+  const float2* r = pr + kR00;
+  float2 j = __ffma2_rn(r[2], z, __ffma2_rn(r[0], x, __fmul2_rn(r[1], y)));
+  float2 k = __ffma2_rn(r[5], z, __ffma2_rn(r[3], x, __fmul2_rn(r[4], y)));
+  float2 l = __ffma2_rn(r[8], z, __ffma2_rn(r[6], x, __fmul2_rn(r[7], y)));
+  return __ffma2_rn(__fmul2_rn(l, l), pr[kS2],
+                    __ffma2_rn(__fmul2_rn(j, j), pr[kS0], __fmul2_rn(__fmul2_rn(k, k), pr[kS1])));
+}
+
+// Weight of a key: the reference's fast-math __expf in FP32
+// (csrc/forward.cu:102); full-precision exp in FP64.
+__device__ __forceinline__ float weight_of(float s) { return __expf(-s); }
+__device__ __forceinline__ double weight_of(double s) { return exp(-s); }
+
+// ---------------------------------------------------------------- mbarrier
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Wait for phase `parity` of `bar` to complete, giving up after roughly a
+// second; returns false on timeout (the caller latches the error and leaves).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  for (int spin = 0; spin < 256; ++spin)
+    if (mbar_test_wait(bar, parity)) return true;
+  for (int spin = 0; spin < (1 << 22); ++spin) {
+    if (mbar_test_wait(bar, parity)) return true;
+    __nanosleep(256);
+  }
+  return false;
+}
+
+// 1-D bulk copy global -> shared completing on `bar` (bytes % 16 == 0,
+// both addresses 16-byte aligned).  No multicast.
+__device__ __forceinline__ void bulk_copy_g2s(void* smem_dst, const void* gmem_src, uint32_t bytes,
+                                              uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(smem_dst)),
+      "l"(gmem_src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+}  // namespace knnag

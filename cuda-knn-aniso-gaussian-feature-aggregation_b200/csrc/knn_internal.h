@@ -1,0 +1,110 @@
+// Internal parameter blocks and workspace layout shared by the .cu files of
+// libknn_aniso.so.  Not part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace knnag {
+
+template <typename T>
+struct ExactParams {
+  const T* q;
+  const T* rec;  // per-point records [B*P*16]
+  const T* f;
+  int B, Q, P, F, K;
+  int use_list;            // 1: process list[0 .. *list_count), 0: every query
+  const int* list;
+  const int* list_count;
+  T* f_out;
+  T* w_out;
+  T* dists;
+  int64_t* idxs;
+};
+
+struct SearchParams {
+  const float* q;
+  const float* pairs;  // pair-interleaved tiles [B][P_pad/2][32]
+  const float* rec;    // per-point records [B*P*16]
+  const float* f;
+  int B, Q, P, P_pad, F, K;
+  int vec4;            // f and f_out rows may be read/written as float4
+  float* f_out;
+  float* w_out;
+  float* dists;
+  int64_t* idxs;
+  int* status;
+  int* flag_count;
+  int* flag_list;
+};
+
+// Search CTA: 4 warps; G warps split the points of one 32-query group.
+constexpr int kSearchThreads = 128;
+constexpr int kQueueCap = 8;
+
+// Shared-memory bytes of the search kernel for (KMAX, G).
+__host__ __device__ inline constexpr size_t search_merge_bytes(int kmax, int g) {
+  return (g > 1) ? (size_t)kSearchThreads * (kmax + 1) * 8 + (size_t)kSearchThreads * 4 : 0;
+}
+__host__ __device__ inline constexpr size_t search_region_a_bytes(int kmax, int g) {
+  // phase 1: two tiles of 128 pairs x 128 B
+  size_t tiles = 2 * 128 * 128;
+  int qpc = 32 * (4 / g);
+  int L = kmax + 1;
+  size_t merge = (g > 1) ? (size_t)kSearchThreads * L * 8 + (size_t)kSearchThreads * 4 : 0;
+  size_t out = (size_t)qpc * ((size_t)L * 12 + 4);
+  size_t phase2 = merge + out;
+  return tiles > phase2 ? tiles : phase2;
+}
+__host__ __device__ inline constexpr size_t search_region_b_bytes() {
+  // candidate queues (keys + idx), shared thresholds (double-buffered), 2 mbarriers
+  return (size_t)kQueueCap * kSearchThreads * 8 + 2 * (size_t)kSearchThreads * 4 + 64;
+}
+__host__ __device__ inline constexpr size_t search_smem_bytes(int kmax, int g) {
+  return search_region_a_bytes(kmax, g) + search_region_b_bytes();
+}
+
+// ------------------------------------------------------------- workspace
+// Forward workspace: [status, flag_count] | flag_list [B*Q] | records (when
+// the caller passed no points buffer) | pair tiles (FP32 fast path).
+struct FwdLayout {
+  size_t status, flag_list, rec, pairs, total;
+  int P_pad;
+};
+FwdLayout fwd_layout(int B, int Q, int P, int K, int dtype, bool own_rec);
+
+// Adjacency (CSR) layout: rowptr [B*P+1] | cursor [B*P] | unsorted [N] | entries [N].
+struct AdjLayout {
+  size_t rowptr, cursor, unsorted, entries, total;
+};
+AdjLayout adj_layout(int B, int Q, int P, int K);
+
+inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+// Backward workspace: status | records | adjacency | per-entry coefficients.
+struct BwdLayout {
+  size_t status, rec, adj, coef, total;
+};
+BwdLayout bwd_layout(int B, int Q, int P, int F, int K, int dtype);
+
+// Arguments of one backward call (order 1 or 2).
+struct BwdArgs {
+  int order;
+  const void *ggq, *gfo, *q, *p, *f, *sigma, *R, *w_in;
+  const int64_t* idxs;
+  int B, Q, P, F, K, dtype, needs;
+  const void *points, *adjacency, *coef_in;
+  void *dgfo, *dq, *dp, *df, *dsigma, *dR, *coef_out;
+  void* workspace;
+};
+int backward_impl(const BwdArgs& x, cudaStream_t st);
+
+int launch_pack_points(const void* p, const void* sigma, const void* R, int B, int P, int dtype, void* rec,
+                       cudaStream_t st);
+int forward_impl(const void* q, const void* p, const void* f, const void* sigma, const void* R, int B, int Q,
+                 int P, int F, int K, int dtype, void* f_out, void* w_out, void* dists, int64_t* idxs,
+                 void* points, void* workspace, cudaStream_t st);
+int launch_build_adjacency(const int64_t* idxs, int B, int Q, int P, int K, void* adjacency, cudaStream_t st);
+
+}  // namespace knnag

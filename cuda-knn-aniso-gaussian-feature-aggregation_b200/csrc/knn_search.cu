@@ -1,0 +1,642 @@
+// Forward path: point packing, the fused kNN search + aggregation kernel
+// (FP32, K <= 32), and the exact MinK kernel that replays the reference's
+// selection rules for flagged queries (and serves FP64 and K > 32).
+//
+// Replaces csrc/forward.cu:56-110 (kernel), csrc/forward.cu:286-338
+// (launcher) and csrc/mink.cuh of the reference.
+#include <math.h>
+
+#include "knn_common.cuh"
+#include "knn_internal.h"
+
+namespace knnag {
+
+// ------------------------------------------------------------------ packing
+
+// rec[(b*P+i)*16 + field]: -p, R (row-major), sigma, pad.
+template <typename T>
+__global__ void pack_points_kernel(const T* __restrict__ p, const T* __restrict__ sigma,
+                                   const T* __restrict__ R, int64_t n_points, T* __restrict__ rec) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_points;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    T v[kRecLen];
+    v[kNPX] = -p[i * 3 + 0];
+    v[kNPY] = -p[i * 3 + 1];
+    v[kNPZ] = -p[i * 3 + 2];
+#pragma unroll
+    for (int m = 0; m < 9; ++m) v[kR00 + m] = R[i * 9 + m];
+    v[kS0] = sigma[i * 3 + 0];
+    v[kS1] = sigma[i * 3 + 1];
+    v[kS2] = sigma[i * 3 + 2];
+    v[kRecPad] = T(0);
+#pragma unroll
+    for (int m = 0; m < kRecLen; ++m) rec[i * kRecLen + m] = v[m];
+  }
+}
+
+// Pair-interleaved FP32 tiles: pairs[((b*P_pad/2 + m)*16 + field)*2 + half]
+// holds field `field` of point 2m+half.  Points beyond P are padding whose
+// sigma is NaN, so their key is NaN and never selected.
+__global__ void pack_pairs_kernel(const float* __restrict__ rec, int B, int P, int P_pad,
+                                  float* __restrict__ pairs) {
+  const int64_t total = (int64_t)B * P_pad * kRecLen;
+  for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < total;
+       o += (int64_t)gridDim.x * blockDim.x) {
+    const int half = (int)(o & 1);
+    const int field = (int)((o >> 1) & (kRecLen - 1));
+    const int64_t pair = o >> 5;  // 32 floats per pair
+    const int64_t b = pair / (P_pad / 2);
+    const int64_t m = pair - b * (P_pad / 2);
+    const int64_t i = 2 * m + half;
+    float v;
+    if (i < P) {
+      v = rec[(b * P + i) * kRecLen + field];
+    } else {
+      v = (field == kS0 || field == kS1 || field == kS2) ? __int_as_float(0x7fc00000) : 0.0f;
+    }
+    pairs[o] = v;
+  }
+}
+
+// ------------------------------------------------------------ exact MinK
+//
+// One warp per query.  Keys are computed 32 points at a time (one per lane,
+// same arithmetic as everywhere else); the selection then follows the
+// reference's MinK rules literally (csrc/mink.cuh:60-81):
+//   fill:  the first K points take slots 0..K-1; the tracked maximum moves
+//          only for the very first key or a strictly larger one;
+//   full:  a point is taken only if strictly below the tracked maximum; it
+//          overwrites the maximum's slot, then the maximum is re-found with a
+//          strict '>' scan starting from the new key (the old slot is kept
+//          when no slot is strictly larger);
+//   sort:  bubble sort with a strict '<' swap (csrc/mink.cuh:99-112).
+// A ballot skips 32-point chunks in which no lane is below the maximum;
+// since the maximum only falls, lanes outside the ballot would be rejected
+// anyway.  All lanes hold the same (size, max) state; slot arrays live in
+// shared memory and lane 0 writes them.
+template <typename T>
+__global__ void __launch_bounds__(128) mink_exact_kernel(ExactParams<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  T* sk = reinterpret_cast<T*>(smem_raw) + (size_t)warp * a.K;
+  int* sv = reinterpret_cast<int*>(reinterpret_cast<T*>(smem_raw) + (size_t)4 * a.K) + (size_t)warp * a.K;
+
+  const int64_t n_items = a.use_list ? (int64_t)(*a.list_count) : (int64_t)a.B * a.Q;
+  const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int K = a.K, P = a.P, F = a.F;
+
+  for (int64_t item = gwarp; item < n_items; item += nwarps) {
+    const int64_t bq = a.use_list ? (int64_t)a.list[item] : item;
+    const int64_t b = bq / a.Q;
+    const T qx = a.q[bq * 3 + 0], qy = a.q[bq * 3 + 1], qz = a.q[bq * 3 + 2];
+    const T* recb = a.rec + b * (int64_t)P * kRecLen;
+
+    int size = 0, max_idx = 0;
+    T max_key = T(0);
+    for (int base = 0; base < P; base += 32) {
+      const int i = base + lane;
+      const int nvalid = min(32, P - base);
+      T key = T(0);
+      if (i < P) key = key_rec<T>(qx, qy, qz, recb + (int64_t)i * kRecLen);
+      int j = 0;
+      while (j < nvalid && size < K) {  // fill phase (uniform)
+        const T kj = __shfl_sync(0xffffffffu, key, j);
+        if (lane == 0) {
+          sk[size] = kj;
+          sv[size] = base + j;
+        }
+        if (size == 0 || kj > max_key) {
+          max_key = kj;
+          max_idx = size;
+        }
+        ++size;
+        ++j;
+      }
+      __syncwarp();
+      if (j < nvalid) {
+        unsigned cand = __ballot_sync(0xffffffffu, lane >= j && lane < nvalid && key < max_key);
+        while (cand) {
+          const int l = __ffs(cand) - 1;
+          cand &= cand - 1;
+          const T kl = __shfl_sync(0xffffffffu, key, l);
+          if (kl < max_key) {
+            if (lane == 0) {
+              sk[max_idx] = kl;
+              sv[max_idx] = base + l;
+            }
+            __syncwarp();
+            max_key = kl;
+            for (int s = 0; s < K; ++s) {
+              const T c = sk[s];
+              if (c > max_key) {
+                max_key = c;
+                max_idx = s;
+              }
+            }
+            __syncwarp();
+          }
+        }
+      }
+    }
+    if (lane == 0) {
+      for (int x = 0; x < size - 1; ++x)
+        for (int y = 0; y < size - x - 1; ++y)
+          if (sk[y + 1] < sk[y]) {
+            const T tk = sk[y];
+            const int tv = sv[y];
+            sk[y] = sk[y + 1];
+            sv[y] = sv[y + 1];
+            sk[y + 1] = tk;
+            sv[y + 1] = tv;
+          }
+    }
+    __syncwarp();
+    for (int k = lane; k < K; k += 32) {
+      const int64_t e = bq * K + k;
+      a.dists[e] = sk[k];
+      a.idxs[e] = (int64_t)sv[k];
+      a.w_out[e] = weight_of(sk[k]);
+    }
+    const T* fb = a.f + b * (int64_t)P * F;
+    for (int c = lane; c < F; c += 32) {
+      T acc = T(0);
+      for (int k = 0; k < K; ++k) acc = fma_rn(fb[(int64_t)sv[k] * F + c], weight_of(sk[k]), acc);
+      a.f_out[bq * F + c] = acc;
+    }
+    __syncwarp();
+  }
+}
+
+// ------------------------------------------------------- fused FP32 search
+//
+// CTA = 4 warps.  Each thread owns one query; G warps of the CTA share one
+// 32-query group and split every point tile between them (G = 1, 2, 4), so
+// small query counts still fill the GPU.  Point tiles (256 points, 16 KB, in
+// the pair-interleaved layout) are streamed into shared memory by one-
+// dimensional bulk copies (TMA), double-buffered on two mbarriers; all lanes
+// read the same pair at a time (broadcast), and both keys of a pair come out
+// of one packed f32x2 key evaluation.
+//
+// Selection.  Each thread keeps the K+1 smallest keys it has accepted in a
+// sorted register list of KMAX+1 slots whose lowest KMAX-K slots hold -inf
+// sentinels, so the (K+1)-th smallest real key is always the last slot.  A
+// key is a candidate when key <= tau (the tightest list top known to the
+// group); candidates are appended to a per-thread queue in shared memory and
+// folded into the list when any lane's queue is nearly full and at every
+// tile end, when the G splits also exchange their list tops.
+//
+// Exactness.  The result equals the reference's MinK selection whenever the
+// K+1 smallest keys are pairwise distinct (then the top-K set and its order
+// are unique) and no NaN key falls in MinK's fill phase (points 0..K-1).  A
+// query is flagged for the exact replay kernel when its merged top-(K+1)
+// holds equal keys or an empty slot, when a dropped or evicted key equalled
+// the threshold it was compared with, or when a fill-phase key is NaN.
+// Dropped keys are > a threshold that is itself >= the global (K+1)-th key,
+// so they can tie with nothing that matters.
+
+template <int L>
+__device__ __forceinline__ void list_insert(float (&keys)[L], int (&vals)[L], float k, int i, bool& tie) {
+#pragma unroll
+  for (int s = 0; s < L; ++s) {
+    const bool lt = k < keys[s];
+    const float nk = lt ? k : keys[s];
+    const float ek = lt ? keys[s] : k;
+    const int ni = lt ? i : vals[s];
+    const int ei = lt ? vals[s] : i;
+    keys[s] = nk;
+    vals[s] = ni;
+    k = ek;
+    i = ei;
+  }
+  // (k, i) was evicted from the top: equal to the new top means a tie.
+  if (i >= 0 && k == keys[L - 1]) tie = true;
+}
+
+template <int L>
+__device__ __forceinline__ void flush_queue(float (&keys)[L], int (&vals)[L], int& qn, bool& tie, float& tau,
+                                            const float* qk, const int* qv, int tid) {
+  for (int e = 0; e < qn; ++e) {
+    const float k = qk[e * kSearchThreads + tid];
+    const int i = qv[e * kSearchThreads + tid];
+    const float top = keys[L - 1];
+    if (k < top) {
+      list_insert<L>(keys, vals, k, i, tie);
+    } else if (k == top) {
+      tie = true;
+    }
+  }
+  qn = 0;
+  tau = fminf(tau, keys[L - 1]);
+}
+
+template <int KMAX, int G>
+__global__ void __launch_bounds__(kSearchThreads) search_f32_kernel(SearchParams a) {
+  constexpr int L = KMAX + 1;
+  constexpr int QPC = 32 * (4 / G);
+  constexpr int PPS = 128 / G;  // pairs per split per tile
+  constexpr size_t RA = search_region_a_bytes(KMAX, G);
+  constexpr uint32_t kTileBytes = 128 * kPairFloats * 4;
+
+  extern __shared__ __align__(128) unsigned char smem[];
+  unsigned char* regA = smem;
+  float* qk = reinterpret_cast<float*>(smem + RA);
+  int* qv = reinterpret_cast<int*>(qk + kQueueCap * kSearchThreads);
+  float* tau_share = reinterpret_cast<float*>(qv + kQueueCap * kSearchThreads);  // [2][128]
+  uint64_t* full = reinterpret_cast<uint64_t*>(tau_share + 2 * kSearchThreads);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int split = warp % G, grp = warp / G;
+  const int lq = grp * 32 + lane;
+  const int b = blockIdx.y;
+  const int qi = blockIdx.x * QPC + lq;
+  const bool valid = qi < a.Q;
+  const int64_t bq = (int64_t)b * a.Q + (valid ? qi : 0);
+  const int K = a.K, P = a.P;
+
+  const float qx = a.q[bq * 3 + 0], qy = a.q[bq * 3 + 1], qz = a.q[bq * 3 + 2];
+  const float2 qx2 = make_float2(qx, qx), qy2 = make_float2(qy, qy), qz2 = make_float2(qz, qz);
+  const float* recb = a.rec + (int64_t)b * P * kRecLen;
+
+  // MinK's fill phase stores points 0..K-1 whatever their key: a NaN there
+  // changes the result in ways only the replay reproduces.
+  bool tie = false;
+  if (split == 0)
+    for (int i = 0; i < K; ++i) {
+      const float s = key_rec<float>(qx, qy, qz, recb + (int64_t)i * kRecLen);
+      if (s != s) tie = true;
+    }
+
+  float keys[L];
+  int vals[L];
+#pragma unroll
+  for (int s = 0; s < L; ++s) {
+    keys[s] = (s < KMAX - K) ? -INFINITY : INFINITY;
+    vals[s] = -1;
+  }
+  float tau = INFINITY;
+  int qn = 0;
+
+  const int ntile = a.P_pad / kTilePoints;
+  const float* pairs_b = a.pairs + (int64_t)b * (a.P_pad / 2) * kPairFloats;
+  if (tid == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    for (int t = 0; t < 2 && t < ntile; ++t) {
+      mbar_arrive_expect_tx(&full[t], kTileBytes);
+      bulk_copy_g2s(regA + t * kTileBytes, pairs_b + (int64_t)t * 128 * kPairFloats, kTileBytes, &full[t]);
+    }
+  }
+
+  for (int t = 0; t < ntile; ++t) {
+    const int buf = t & 1;
+    const bool ok = mbar_wait_bounded(&full[buf], (t >> 1) & 1);
+    const float4* tp = reinterpret_cast<const float4*>(regA + buf * kTileBytes) + split * PPS * 8;
+    const int ibase = t * kTilePoints + split * PPS * 2;
+#pragma unroll 2
+    for (int m = 0; m < PPS; ++m) {
+      float2 pr[16];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const float4 v = tp[m * 8 + u];
+        pr[2 * u] = make_float2(v.x, v.y);
+        pr[2 * u + 1] = make_float2(v.z, v.w);
+      }
+      const float2 s2 = key_pair(qx2, qy2, qz2, pr);
+      const int ia = ibase + 2 * m;
+      if (s2.x <= tau) {
+        qk[qn * kSearchThreads + tid] = s2.x;
+        qv[qn * kSearchThreads + tid] = ia;
+        ++qn;
+      }
+      if (s2.y <= tau) {
+        qk[qn * kSearchThreads + tid] = s2.y;
+        qv[qn * kSearchThreads + tid] = ia + 1;
+        ++qn;
+      }
+      if (__any_sync(0xffffffffu, qn > kQueueCap - 2)) flush_queue<L>(keys, vals, qn, tie, tau, qk, qv, tid);
+    }
+    flush_queue<L>(keys, vals, qn, tie, tau, qk, qv, tid);
+    tau_share[buf * kSearchThreads + split * QPC + lq] = keys[L - 1];
+    const int abort = __syncthreads_or(!ok);
+    if (abort) {
+      if (tid == 0) {
+        atomicOr(a.status, kStatusWaitTimeout);
+        mbar_wait_bounded(&full[buf], (t >> 1) & 1);
+        if (t + 1 < ntile) mbar_wait_bounded(&full[buf ^ 1], ((t + 1) >> 1) & 1);
+      }
+      return;
+    }
+    float tm = keys[L - 1];
+#pragma unroll
+    for (int g = 0; g < G; ++g) tm = fminf(tm, tau_share[buf * kSearchThreads + g * QPC + lq]);
+    tau = fminf(tau, tm);
+    if (tid == 0 && t + 2 < ntile) {
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(&full[buf], kTileBytes);
+      bulk_copy_g2s(regA + buf * kTileBytes, pairs_b + (int64_t)(t + 2) * 128 * kPairFloats, kTileBytes,
+                    &full[buf]);
+    }
+  }
+
+  // ---- merge the G split lists; region A is free (no copy in flight, all
+  // tile reads ended before the last barrier).
+  constexpr size_t kMerge = search_merge_bytes(KMAX, G);
+  float* mk = reinterpret_cast<float*>(regA);
+  int* mv = reinterpret_cast<int*>(regA + (size_t)kSearchThreads * L * 4);
+  int* mf = reinterpret_cast<int*>(regA + (size_t)kSearchThreads * L * 8);
+  float* out_k = reinterpret_cast<float*>(regA + kMerge);
+  int* out_i = reinterpret_cast<int*>(out_k + QPC * L);
+  float* out_w = reinterpret_cast<float*>(out_i + QPC * L);
+  int* out_f = reinterpret_cast<int*>(out_w + QPC * L);
+
+  bool fl = tie;
+  if (G > 1) {
+    const int slot = split * QPC + lq;
+#pragma unroll
+    for (int s = 0; s < L; ++s) {
+      mk[slot * L + s] = keys[s];
+      mv[slot * L + s] = vals[s];
+    }
+    mf[slot] = tie ? 1 : 0;
+    __syncthreads();
+    if (split == 0) {
+      int h[G];
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        h[g] = KMAX - K;
+        fl = fl || (mf[g * QPC + lq] != 0);
+      }
+      for (int j = 0; j <= K; ++j) {
+        float bk = INFINITY;
+        int bi = -1, bg = 0;
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+          if (h[g] < L) {
+            const float kk = mk[(g * QPC + lq) * L + h[g]];
+            if (bi < 0 && g == 0 || kk < bk) {
+              bk = kk;
+              bi = mv[(g * QPC + lq) * L + h[g]];
+              bg = g;
+            }
+          }
+        }
+#pragma unroll
+        for (int g = 0; g < G; ++g) h[g] += (g == bg) ? 1 : 0;
+        out_k[lq * L + j] = bk;
+        out_i[lq * L + j] = bi;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int s = 0; s < L; ++s) {
+      const int j = s - (KMAX - K);
+      if (j >= 0) {
+        out_k[lq * L + j] = keys[s];
+        out_i[lq * L + j] = vals[s];
+      }
+    }
+  }
+  if (split == 0) {
+    const int nneed = (P > K) ? K + 1 : K;
+    for (int j = 0; j < nneed; ++j)
+      if (out_i[lq * L + j] < 0) fl = true;
+    for (int j = 0; j + 1 < nneed; ++j)
+      if (out_k[lq * L + j] == out_k[lq * L + j + 1]) fl = true;
+    for (int j = 0; j < K; ++j) out_w[lq * L + j] = weight_of(out_k[lq * L + j]);
+    out_f[lq] = (fl || !valid) ? 1 : 0;
+    if (valid && fl) {
+      const int pos = atomicAdd(a.flag_count, 1);
+      a.flag_list[pos] = (int)bq;
+    }
+  }
+  __syncthreads();
+
+  // ---- epilogue: dists / idxs / w_out, then f_out = sum_k w_k f[idx_k]
+  // accumulated in k order with fma, 128-bit gathers of f rows.
+  const int qbase = blockIdx.x * QPC;
+  const int nq = min(QPC, a.Q - qbase);
+  const int64_t q0 = (int64_t)b * a.Q + qbase;
+  for (int it = tid; it < nq * K; it += kSearchThreads) {
+    const int l = it / K, k = it - l * K;
+    if (out_f[l]) continue;
+    const int64_t e = (q0 + l) * K + k;
+    a.dists[e] = out_k[l * L + k];
+    a.idxs[e] = (int64_t)out_i[l * L + k];
+    a.w_out[e] = out_w[l * L + k];
+  }
+  const int F = a.F;
+  const float* fb = a.f + (int64_t)b * P * F;
+  if (a.vec4) {
+    const int C4 = F >> 2;
+    for (int it = tid; it < nq * C4; it += kSearchThreads) {
+      const int l = it / C4, c = it - l * C4;
+      if (out_f[l]) continue;
+      float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int k = 0; k < K; ++k) {
+        const int idx = out_i[l * L + k];
+        const float w = out_w[l * L + k];
+        const float4 v = __ldg(reinterpret_cast<const float4*>(fb + (int64_t)idx * F) + c);
+        acc.x = __fmaf_rn(v.x, w, acc.x);
+        acc.y = __fmaf_rn(v.y, w, acc.y);
+        acc.z = __fmaf_rn(v.z, w, acc.z);
+        acc.w = __fmaf_rn(v.w, w, acc.w);
+      }
+      reinterpret_cast<float4*>(a.f_out + (q0 + l) * F)[c] = acc;
+    }
+  } else {
+    for (int it = tid; it < nq * F; it += kSearchThreads) {
+      const int l = it / F, c = it - l * F;
+      if (out_f[l]) continue;
+      float acc = 0.f;
+      for (int k = 0; k < K; ++k)
+        acc = __fmaf_rn(__ldg(fb + (int64_t)out_i[l * L + k] * F + c), out_w[l * L + k], acc);
+      a.f_out[(q0 + l) * F + c] = acc;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ host
+
+namespace {
+
+int num_sms(int dev) {
+  static int cache[64] = {0};
+  if (dev < 0 || dev >= 64) return 148;
+  if (!cache[dev]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+    cache[dev] = v;
+  }
+  return cache[dev];
+}
+
+template <int KMAX, int G>
+int launch_search_t(const SearchParams& a, cudaStream_t st) {
+  constexpr size_t smem = search_smem_bytes(KMAX, G);
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    if (cudaFuncSetAttribute(search_f32_kernel<KMAX, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+      return KNNAG_ERR_CUDA;
+    attr_set[dev] = true;
+  }
+  constexpr int QPC = 32 * (4 / G);
+  dim3 grid((a.Q + QPC - 1) / QPC, a.B);
+  search_f32_kernel<KMAX, G><<<grid, kSearchThreads, smem, st>>>(a);
+  return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
+}
+
+template <int KMAX>
+int launch_search_k(const SearchParams& a, int G, cudaStream_t st) {
+  if (G == 1) return launch_search_t<KMAX, 1>(a, st);
+  if (G == 2) return launch_search_t<KMAX, 2>(a, st);
+  return launch_search_t<KMAX, 4>(a, st);
+}
+
+template <typename T>
+int launch_exact(const ExactParams<T>& a, cudaStream_t st) {
+  const size_t smem = (size_t)4 * a.K * (sizeof(T) + sizeof(int));
+  if (smem > 48 * 1024) {
+    if (smem > 200 * 1024) return KNNAG_ERR_TOO_LARGE;
+    if (cudaFuncSetAttribute(mink_exact_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+      return KNNAG_ERR_CUDA;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int64_t blocks;
+  if (a.use_list) {
+    blocks = (int64_t)num_sms(dev) * 8;
+  } else {
+    blocks = ((int64_t)a.B * a.Q + 3) / 4;
+    blocks = blocks < (int64_t)num_sms(dev) * 64 ? blocks : (int64_t)num_sms(dev) * 64;
+  }
+  if (blocks < 1) blocks = 1;
+  mink_exact_kernel<T><<<(unsigned)blocks, 128, smem, st>>>(a);
+  return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
+}
+
+// Splits per query group: the fewest that still give ~4 CTAs per SM.
+int choose_splits(int B, int Q, int dev) {
+  const int64_t target = (int64_t)num_sms(dev) * 4;
+  for (int g = 1; g <= 4; g *= 2) {
+    const int qpc = 32 * (4 / g);
+    const int64_t ctas = (int64_t)B * ((Q + qpc - 1) / qpc);
+    if (ctas >= target) return g;
+  }
+  return 4;
+}
+
+inline unsigned grid_for(int64_t n, int threads, int dev) {
+  int64_t b = (n + threads - 1) / threads;
+  const int64_t cap = (int64_t)num_sms(dev) * 32;
+  if (b > cap) b = cap;
+  return (unsigned)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+FwdLayout fwd_layout(int B, int Q, int P, int K, int dtype, bool own_rec) {
+  FwdLayout L{};
+  const size_t esz = dtype == KNNAG_F64 ? 8 : 4;
+  size_t off = 0;
+  L.status = off;
+  off += 256;
+  L.flag_list = off;
+  off += align256((size_t)B * Q * 4);
+  L.rec = off;
+  if (own_rec) off += align256((size_t)B * P * kRecLen * esz);
+  L.P_pad = (int)round_up(P, kTilePoints);
+  L.pairs = off;
+  if (dtype == KNNAG_F32 && K <= 32) off += align256((size_t)B * L.P_pad * kRecLen * 4);
+  L.total = off;
+  return L;
+}
+
+int launch_pack_points(const void* p, const void* sigma, const void* R, int B, int P, int dtype, void* rec,
+                       cudaStream_t st) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const int64_t n = (int64_t)B * P;
+  if (dtype == KNNAG_F64)
+    pack_points_kernel<double><<<grid_for(n, 256, dev), 256, 0, st>>>(
+        (const double*)p, (const double*)sigma, (const double*)R, n, (double*)rec);
+  else
+    pack_points_kernel<float><<<grid_for(n, 256, dev), 256, 0, st>>>((const float*)p, (const float*)sigma,
+                                                                     (const float*)R, n, (float*)rec);
+  return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
+}
+
+template <typename T>
+static int forward_exact_all(const T* q, const T* rec, const T* f, int B, int Q, int P, int F, int K, T* f_out,
+                             T* w_out, T* dists, int64_t* idxs, cudaStream_t st) {
+  ExactParams<T> e{q, rec, f, B, Q, P, F, K, 0, nullptr, nullptr, f_out, w_out, dists, idxs};
+  return launch_exact<T>(e, st);
+}
+
+int forward_impl(const void* q, const void* p, const void* f, const void* sigma, const void* R, int B, int Q,
+                 int P, int F, int K, int dtype, void* f_out, void* w_out, void* dists, int64_t* idxs,
+                 void* points, void* workspace, cudaStream_t st) {
+  const bool own_rec = points == nullptr;
+  const FwdLayout L = fwd_layout(B, Q, P, K, dtype, own_rec);
+  char* ws = static_cast<char*>(workspace);
+  int* status = reinterpret_cast<int*>(ws + L.status);
+  int* flag_count = status + 1;
+  int* flag_list = reinterpret_cast<int*>(ws + L.flag_list);
+  void* rec = own_rec ? (void*)(ws + L.rec) : points;
+  if (cudaMemsetAsync(status, 0, 2 * sizeof(int), st) != cudaSuccess) return KNNAG_ERR_CUDA;
+  int rc = launch_pack_points(p, sigma, R, B, P, dtype, rec, st);
+  if (rc) return rc;
+  if (dtype == KNNAG_F64)
+    return forward_exact_all<double>((const double*)q, (const double*)rec, (const double*)f, B, Q, P, F, K,
+                                     (double*)f_out, (double*)w_out, (double*)dists, idxs, st);
+  if (K > 32)
+    return forward_exact_all<float>((const float*)q, (const float*)rec, (const float*)f, B, Q, P, F, K,
+                                    (float*)f_out, (float*)w_out, (float*)dists, idxs, st);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  float* pairs = reinterpret_cast<float*>(ws + L.pairs);
+  pack_pairs_kernel<<<grid_for((int64_t)B * L.P_pad * kRecLen, 256, dev), 256, 0, st>>>(
+      (const float*)rec, B, P, L.P_pad, pairs);
+  if (cudaGetLastError() != cudaSuccess) return KNNAG_ERR_CUDA;
+  SearchParams sp{};
+  sp.q = (const float*)q;
+  sp.pairs = pairs;
+  sp.rec = (const float*)rec;
+  sp.f = (const float*)f;
+  sp.B = B;
+  sp.Q = Q;
+  sp.P = P;
+  sp.P_pad = L.P_pad;
+  sp.F = F;
+  sp.K = K;
+  sp.vec4 = (F % 4 == 0) && ((uintptr_t)f % 16 == 0) && ((uintptr_t)f_out % 16 == 0);
+  sp.f_out = (float*)f_out;
+  sp.w_out = (float*)w_out;
+  sp.dists = (float*)dists;
+  sp.idxs = idxs;
+  sp.status = status;
+  sp.flag_count = flag_count;
+  sp.flag_list = flag_list;
+  const int G = choose_splits(B, Q, dev);
+  if (K <= 8)
+    rc = launch_search_k<8>(sp, G, st);
+  else if (K <= 16)
+    rc = launch_search_k<16>(sp, G, st);
+  else
+    rc = launch_search_k<32>(sp, G, st);
+  if (rc) return rc;
+  // Exact MinK replay of the flagged queries (count read on the device).
+  ExactParams<float> e{(const float*)q, (const float*)rec, (const float*)f, B, Q, P, F, K, 1, flag_list,
+                       flag_count, (float*)f_out, (float*)w_out, (float*)dists, idxs};
+  return launch_exact<float>(e, st);
+}
+
+}  // namespace knnag

@@ -1,0 +1,266 @@
+// Torch extension `cuda_knn_aggregate._C`: validates tensors, allocates
+// outputs and scratch from torch's caching allocator, and calls the C ABI of
+// libknn_aniso.so on the current CUDA stream.
+//
+// The first three ops keep the names, argument lists and return lists of
+// the reference's pybind module (csrc/knn_aggregate.cpp:26-47, 101-172,
+// 178-185) so code written against it runs unchanged; the *_ex ops expose
+// the reuse of packed points, adjacency and coefficients that the autograd
+// layer uses.
+#include <ATen/cuda/CUDAContext.h>
+#include <c10/cuda/CUDAGuard.h>
+#include <torch/extension.h>
+
+#include <string>
+#include <vector>
+
+#include "knn_aniso.h"
+
+namespace {
+
+#define KNN_CHECK_CUDA(x) TORCH_CHECK((x).is_cuda(), #x " must be a CUDA tensor")
+#define KNN_CHECK_CONTIGUOUS(x) TORCH_CHECK((x).is_contiguous(), #x " must be contiguous")
+#define KNN_CHECK_INPUT(x) \
+  KNN_CHECK_CUDA(x);       \
+  KNN_CHECK_CONTIGUOUS(x)
+
+void check_status(int rc, const char* what) {
+  TORCH_CHECK(rc == KNNAG_OK, what, " failed: ", knnag_status_string(rc));
+}
+
+int dtype_code(const torch::Tensor& t) {
+  if (t.scalar_type() == torch::kFloat32) return KNNAG_F32;
+  if (t.scalar_type() == torch::kFloat64) return KNNAG_F64;
+  TORCH_CHECK(false, "knn_aggregate_aniso supports float32 and float64, got ", t.scalar_type());
+  return -1;
+}
+
+struct Dims {
+  int B, Q, P, F, dtype;
+};
+
+Dims check_inputs(const torch::Tensor& q, const torch::Tensor& p, const torch::Tensor& f,
+                  const torch::Tensor& sigma, const torch::Tensor& R) {
+  KNN_CHECK_INPUT(q);
+  KNN_CHECK_INPUT(p);
+  KNN_CHECK_INPUT(f);
+  KNN_CHECK_INPUT(sigma);
+  KNN_CHECK_INPUT(R);
+  TORCH_CHECK(q.dim() == 3 && q.size(2) == 3, "q must have shape [B, Q, 3]");
+  TORCH_CHECK(p.dim() == 3 && p.size(2) == 3, "p must have shape [B, P, 3]");
+  const int64_t B = q.size(0), P = p.size(1);
+  TORCH_CHECK(p.size(0) == B, "p batch size must match q");
+  TORCH_CHECK(f.dim() == 3 && f.size(0) == B && f.size(1) == P, "f must have shape [B, P, F]");
+  TORCH_CHECK(sigma.dim() == 3 && sigma.size(0) == B && sigma.size(1) == P && sigma.size(2) == 3,
+              "sigma must have shape [B, P, 3]");
+  TORCH_CHECK(R.dim() == 4 && R.size(0) == B && R.size(1) == P && R.size(2) == 3 && R.size(3) == 3,
+              "R must have shape [B, P, 3, 3]");
+  const int dt = dtype_code(q);
+  for (const torch::Tensor* t : {&p, &f, &sigma, &R})
+    TORCH_CHECK(t->scalar_type() == q.scalar_type(), "all floating-point inputs must share q's dtype");
+  for (const torch::Tensor* t : {&p, &f, &sigma, &R})
+    TORCH_CHECK(t->device() == q.device(), "all inputs must be on the same device");
+  TORCH_CHECK(B <= INT32_MAX && q.size(1) <= INT32_MAX && P <= INT32_MAX && f.size(2) <= INT32_MAX,
+              "sizes exceed the 32-bit range");
+  return Dims{(int)B, (int)q.size(1), (int)P, (int)f.size(2), dt};
+}
+
+void check_k(int64_t K, int P) {
+  TORCH_CHECK(K >= 1 && K <= P, "K must satisfy 1 <= K <= P (K=", K, ", P=", P, ")");
+}
+
+torch::Tensor scratch(size_t bytes, const torch::Tensor& like) {
+  return torch::empty({(int64_t)(bytes > 0 ? bytes : 1)}, like.options().dtype(torch::kUInt8));
+}
+
+void* stream_of(const torch::Tensor& t) { return (void*)at::cuda::getCurrentCUDAStream(t.device().index()).stream(); }
+
+void* ptr_or_null(const c10::optional<torch::Tensor>& t) { return (t && t->defined()) ? t->data_ptr() : nullptr; }
+
+std::vector<torch::Tensor> forward_impl(const torch::Tensor& q, const torch::Tensor& p, const torch::Tensor& f,
+                                        const torch::Tensor& sigma, const torch::Tensor& R, int64_t K,
+                                        bool want_points) {
+  const Dims d = check_inputs(q, p, f, sigma, R);
+  check_k(K, d.P);
+  const c10::cuda::CUDAGuard guard(q.device());
+  auto f_out = torch::empty({d.B, d.Q, d.F}, f.options());
+  auto w_out = torch::empty({d.B, d.Q, K}, f.options());
+  auto dists = torch::empty({d.B, d.Q, K}, q.options());
+  auto idxs = torch::empty({d.B, d.Q, K}, q.options().dtype(torch::kInt64));
+  torch::Tensor points;
+  if (want_points) points = torch::empty({d.B, d.P, 16}, p.options());
+  const size_t ws_bytes = knnag_forward_workspace_bytes(d.B, d.Q, d.P, d.F, (int)K, d.dtype);
+  auto ws = scratch(ws_bytes, q);
+  const int rc = knnag_forward(q.data_ptr(), p.data_ptr(), f.data_ptr(), sigma.data_ptr(), R.data_ptr(), d.B, d.Q,
+                               d.P, d.F, (int)K, d.dtype, f_out.data_ptr(), w_out.data_ptr(), dists.data_ptr(),
+                               idxs.data_ptr<int64_t>(), want_points ? points.data_ptr() : nullptr, ws.data_ptr(),
+                               ws_bytes, stream_of(q));
+  check_status(rc, "knn_aggregate_aniso_forward");
+  if (want_points) return {f_out, w_out, dists, idxs, points};
+  return {f_out, w_out, dists, idxs};
+}
+
+void check_idxs(const torch::Tensor& idxs, const Dims& d) {
+  KNN_CHECK_INPUT(idxs);
+  TORCH_CHECK(idxs.scalar_type() == torch::kInt64, "idxs must be int64");
+  TORCH_CHECK(idxs.dim() == 3 && idxs.size(0) == d.B && idxs.size(1) == d.Q, "idxs must have shape [B, Q, K]");
+  check_k(idxs.size(2), d.P);
+}
+
+void check_like(const torch::Tensor& t, const char* name, std::vector<int64_t> shape, const torch::Tensor& ref) {
+  TORCH_CHECK(t.is_cuda(), name, " must be a CUDA tensor");
+  TORCH_CHECK(t.is_contiguous(), name, " must be contiguous");
+  TORCH_CHECK(t.sizes() == c10::IntArrayRef(shape), name, " has the wrong shape");
+  TORCH_CHECK(t.scalar_type() == ref.scalar_type(), name, " must share q's dtype");
+}
+
+// needs bits -> output tensors (undefined tensors for skipped outputs)
+std::vector<torch::Tensor> backward_impl(int order, const c10::optional<torch::Tensor>& ggq, const torch::Tensor& gfo,
+                                         const torch::Tensor& q, const torch::Tensor& p, const torch::Tensor& f,
+                                         const torch::Tensor& sigma, const torch::Tensor& R,
+                                         const c10::optional<torch::Tensor>& w_out, const torch::Tensor& idxs,
+                                         const c10::optional<torch::Tensor>& points,
+                                         const c10::optional<torch::Tensor>& adjacency,
+                                         const c10::optional<torch::Tensor>& coef, int64_t needs, bool want_coef) {
+  const Dims d = check_inputs(q, p, f, sigma, R);
+  check_idxs(idxs, d);
+  const int K = (int)idxs.size(2);
+  check_like(gfo, "grad_f_out", {d.B, d.Q, d.F}, q);
+  if (order == 2) check_like(*ggq, "grad_grad_q", {d.B, d.Q, 3}, q);
+  if (w_out && w_out->defined()) check_like(*w_out, "w_out", {d.B, d.Q, K}, q);
+  if (points && points->defined()) check_like(*points, "points", {d.B, d.P, 16}, q);
+  if (coef && coef->defined()) check_like(*coef, "coef", {d.B, d.Q, K}, q);
+  if (adjacency && adjacency->defined()) {
+    TORCH_CHECK(adjacency->is_cuda() && adjacency->scalar_type() == torch::kUInt8 &&
+                    (size_t)adjacency->numel() >= knnag_adjacency_bytes(d.B, d.Q, d.P, K),
+                "adjacency must be the uint8 CUDA buffer built by build_adjacency");
+  }
+  const c10::cuda::CUDAGuard guard(q.device());
+  torch::Tensor dgfo, dq, dp, df, ds, dR, cf;
+  if (order == 2 && (needs & KNNAG_NEED_DGFO)) dgfo = torch::empty({d.B, d.Q, d.F}, f.options());
+  if (needs & KNNAG_NEED_DQ) dq = torch::empty({d.B, d.Q, 3}, q.options());
+  if (needs & KNNAG_NEED_DP) dp = torch::empty({d.B, d.P, 3}, p.options());
+  if (needs & KNNAG_NEED_DF) df = torch::empty({d.B, d.P, d.F}, f.options());
+  if (needs & KNNAG_NEED_DSIGMA) ds = torch::empty({d.B, d.P, 3}, sigma.options());
+  if (needs & KNNAG_NEED_DR) dR = torch::empty({d.B, d.P, 3, 3}, R.options());
+  if (order == 1 && want_coef) cf = torch::empty({d.B, d.Q, K}, q.options());
+  auto P_ = [](const torch::Tensor& t) -> void* { return t.defined() ? t.data_ptr() : nullptr; };
+  const size_t ws_bytes = knnag_backward_workspace_bytes(d.B, d.Q, d.P, d.F, K, d.dtype);
+  auto ws = scratch(ws_bytes, q);
+  int rc;
+  if (order == 1) {
+    rc = knnag_backward(gfo.data_ptr(), nullptr, q.data_ptr(), p.data_ptr(), f.data_ptr(), sigma.data_ptr(),
+                        R.data_ptr(), ptr_or_null(w_out), idxs.data_ptr<int64_t>(), d.B, d.Q, d.P, d.F, K, d.dtype,
+                        (int)needs, ptr_or_null(points), ptr_or_null(adjacency), P_(dq), P_(dp), P_(df), P_(ds),
+                        P_(dR), P_(cf), ws.data_ptr(), ws_bytes, stream_of(q));
+    check_status(rc, "knn_aggregate_aniso_backward");
+    return {dq, dp, df, ds, dR, cf};
+  }
+  rc = knnag_backward_2nd(ggq->data_ptr(), gfo.data_ptr(), nullptr, q.data_ptr(), p.data_ptr(), f.data_ptr(),
+                          sigma.data_ptr(), R.data_ptr(), ptr_or_null(w_out), idxs.data_ptr<int64_t>(), d.B, d.Q,
+                          d.P, d.F, K, d.dtype, (int)needs, ptr_or_null(points), ptr_or_null(adjacency),
+                          ptr_or_null(coef), P_(dgfo), P_(dq), P_(dp), P_(df), P_(ds), P_(dR), ws.data_ptr(),
+                          ws_bytes, stream_of(q));
+  check_status(rc, "knn_aggregate_aniso_backward_2nd");
+  return {dgfo, dq, dp, df, ds, dR};
+}
+
+// ----------------------------------------------- reference-compatible ops
+
+std::vector<torch::Tensor> knn_aggregate_aniso_forward(torch::Tensor q, torch::Tensor p, torch::Tensor f,
+                                                       torch::Tensor sigma, torch::Tensor R, int64_t K) {
+  return forward_impl(q, p, f, sigma, R, K, false);
+}
+
+std::vector<torch::Tensor> knn_aggregate_aniso_backward(torch::Tensor grad_f_out, torch::Tensor grad_w_out,
+                                                        torch::Tensor q, torch::Tensor p, torch::Tensor f,
+                                                        torch::Tensor sigma, torch::Tensor R, torch::Tensor w_out,
+                                                        torch::Tensor k_idxs) {
+  KNN_CHECK_INPUT(grad_f_out);
+  KNN_CHECK_INPUT(grad_w_out);
+  KNN_CHECK_INPUT(w_out);
+  auto r = backward_impl(1, c10::nullopt, grad_f_out, q, p, f, sigma, R, w_out, k_idxs, c10::nullopt, c10::nullopt,
+                         c10::nullopt, KNNAG_NEED_DQ | KNNAG_NEED_DP | KNNAG_NEED_DF | KNNAG_NEED_DSIGMA |
+                                           KNNAG_NEED_DR,
+                         false);
+  return {r[0], r[1], r[2], r[3], r[4]};
+}
+
+std::vector<torch::Tensor> knn_aggregate_aniso_backward_2nd(torch::Tensor grad_grad_q, torch::Tensor grad_f_out,
+                                                            torch::Tensor grad_w_out, torch::Tensor q, torch::Tensor p,
+                                                            torch::Tensor f, torch::Tensor sigma, torch::Tensor R,
+                                                            torch::Tensor w_out, torch::Tensor k_idxs) {
+  KNN_CHECK_INPUT(grad_grad_q);
+  KNN_CHECK_INPUT(grad_f_out);
+  KNN_CHECK_INPUT(grad_w_out);
+  KNN_CHECK_INPUT(w_out);
+  return backward_impl(2, grad_grad_q, grad_f_out, q, p, f, sigma, R, w_out, k_idxs, c10::nullopt, c10::nullopt,
+                       c10::nullopt, KNNAG_NEED_ALL, false);
+}
+
+// --------------------------------------------------------- extended ops
+
+std::vector<torch::Tensor> forward_ex(torch::Tensor q, torch::Tensor p, torch::Tensor f, torch::Tensor sigma,
+                                      torch::Tensor R, int64_t K) {
+  return forward_impl(q, p, f, sigma, R, K, true);
+}
+
+torch::Tensor build_adjacency(torch::Tensor idxs, int64_t P) {
+  KNN_CHECK_INPUT(idxs);
+  TORCH_CHECK(idxs.scalar_type() == torch::kInt64 && idxs.dim() == 3, "idxs must be int64 [B, Q, K]");
+  const int B = (int)idxs.size(0), Q = (int)idxs.size(1), K = (int)idxs.size(2);
+  check_k(K, (int)P);
+  const c10::cuda::CUDAGuard guard(idxs.device());
+  auto adj = scratch(knnag_adjacency_bytes(B, Q, (int)P, K), idxs);
+  check_status(knnag_build_adjacency(idxs.data_ptr<int64_t>(), B, Q, (int)P, K, adj.data_ptr(), stream_of(idxs)),
+               "build_adjacency");
+  return adj;
+}
+
+// rowptr [B*P+1] and sorted entry ids [B*Q*K] views of an adjacency buffer.
+std::vector<torch::Tensor> adjacency_views(torch::Tensor adj, int64_t B, int64_t Q, int64_t P, int64_t K) {
+  const size_t rows = (size_t)B * P, n = (size_t)B * Q * K;
+  // layout: rowptr | cursor | unsorted | entries, each rounded up to 256 bytes
+  const size_t a0 = ((rows + 1) * 4 + 255) / 256 * 256;
+  const size_t a1 = (rows * 4 + 255) / 256 * 256;
+  const size_t a2 = (n * 4 + 255) / 256 * 256;
+  auto i32 = adj.view(torch::kInt32);
+  auto rowptr = i32.narrow(0, 0, (int64_t)rows + 1);
+  auto entries = i32.narrow(0, (int64_t)((a0 + a1 + a2) / 4), (int64_t)n);
+  return {rowptr, entries};
+}
+
+std::vector<torch::Tensor> backward_ex(torch::Tensor gfo, torch::Tensor q, torch::Tensor p, torch::Tensor f,
+                                       torch::Tensor sigma, torch::Tensor R, torch::Tensor idxs,
+                                       c10::optional<torch::Tensor> points, c10::optional<torch::Tensor> adjacency,
+                                       int64_t needs) {
+  return backward_impl(1, c10::nullopt, gfo, q, p, f, sigma, R, c10::nullopt, idxs, points, adjacency, c10::nullopt,
+                       needs, true);
+}
+
+std::vector<torch::Tensor> backward2_ex(torch::Tensor ggq, torch::Tensor gfo, torch::Tensor q, torch::Tensor p,
+                                        torch::Tensor f, torch::Tensor sigma, torch::Tensor R, torch::Tensor idxs,
+                                        c10::optional<torch::Tensor> points, c10::optional<torch::Tensor> adjacency,
+                                        c10::optional<torch::Tensor> coef, int64_t needs) {
+  return backward_impl(2, ggq, gfo, q, p, f, sigma, R, c10::nullopt, idxs, points, adjacency, coef, needs, false);
+}
+
+}  // namespace
+
+PYBIND11_MODULE(_C, m) {
+  m.def("knn_aggregate_aniso_forward", &knn_aggregate_aniso_forward, "KNN aggregate aniso forward");
+  m.def("knn_aggregate_aniso_backward", &knn_aggregate_aniso_backward, "KNN aggregate aniso backward");
+  m.def("knn_aggregate_aniso_backward_2nd", &knn_aggregate_aniso_backward_2nd,
+        "KNN aggregate aniso second order backward");
+  m.def("forward_ex", &forward_ex, "forward that also returns the packed point records");
+  m.def("build_adjacency", &build_adjacency, "point -> entry adjacency (CSR) of idxs");
+  m.def("adjacency_views", &adjacency_views, "rowptr / entry views of an adjacency buffer");
+  m.def("backward_ex", &backward_ex, "first-order adjoint with selectable outputs; also returns coef");
+  m.def("backward2_ex", &backward2_ex, "second-order adjoint with selectable outputs");
+  m.attr("NEED_DQ") = (int)KNNAG_NEED_DQ;
+  m.attr("NEED_DP") = (int)KNNAG_NEED_DP;
+  m.attr("NEED_DF") = (int)KNNAG_NEED_DF;
+  m.attr("NEED_DSIGMA") = (int)KNNAG_NEED_DSIGMA;
+  m.attr("NEED_DR") = (int)KNNAG_NEED_DR;
+  m.attr("NEED_DGFO") = (int)KNNAG_NEED_DGFO;
+}

@@ -1,0 +1,155 @@
+"""Anisotropic-Gaussian kNN feature aggregation on B200 (sm_100a).
+
+Drop-in for the reference package of the same name
+(LemonATsu/CUDA-kNN-Aniso-Gaussian-Feature-Aggregation,
+``cuda_knn_aggregate/__init__.py``): same function, same autograd classes,
+same argument order and return order, same ``_C`` op names.
+
+    f_out, w_out, dists, idxs = knn_aggregate_aniso(q, p, f, sigma, R, K)
+
+For each query q [B,Q,3] the K points of p [B,P,3] with the smallest
+``s = sum_a sigma[a] * (R[a] . (q - p))^2`` are found (ascending, ties broken
+as the reference breaks them), ``w_out = exp(-s)`` and
+``f_out = sum_k w_out[k] * f[idx_k]``.  Only ``f_out`` carries gradient, as in
+the reference: gradients arriving on ``w_out`` and ``dists`` are ignored.
+Second-order gradients flow through ``dL/dq`` (Eikonal regularisation);
+second-order terms arriving through the point-side first-order gradients are
+ignored, as in the reference.
+
+All compute runs in the hand-written CUDA kernels of ``libknn_aniso.so``;
+there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import torch
+
+try:
+    from . import _C  # noqa: F401
+except ImportError as exc:  # pragma: no cover - exercised only on a broken install
+    raise ImportError(
+        "cuda_knn_aggregate: the CUDA extension (_C / libknn_aniso.so) is not built; "
+        "run `python build.py` in the package's parent directory") from exc
+
+__all__ = [
+    "knn_aggregate_aniso",
+    "KNNAnisotropicAggregate",
+    "KNNAnisotropicAggregateBackward",
+]
+
+_NEED_BITS = (_C.NEED_DQ, _C.NEED_DP, _C.NEED_DF, _C.NEED_DSIGMA, _C.NEED_DR)
+
+
+def knn_aggregate_aniso(q: torch.Tensor, p: torch.Tensor, f: torch.Tensor, sigma: torch.Tensor, R: torch.Tensor,
+                        K: int):
+    """k-NN feature aggregate using anisotropic Gaussian weights.
+
+    Args:
+        q: [B, Q, 3] query point coordinates.
+        p: [B, P, 3] surface point coordinates.
+        f: [B, P, F] features of the surface points.
+        sigma: [B, P, 3] Gaussian precisions along the three axes (multiplies
+            the squared rotated offset).
+        R: [B, P, 3, 3] Gaussian axes (rows), row-major.
+        K: number of nearest neighbours, 1 <= K <= P.
+
+    Returns:
+        f_out [B, Q, F], w_out [B, Q, K], dists [B, Q, K], idxs [B, Q, K] int64.
+        Only f_out is differentiable.
+    """
+    return KNNAnisotropicAggregate.apply(q, p, f, sigma, R, K)
+
+
+class _Aux:
+    """Per-forward state shared with the backward passes: the packed point
+    records written by the forward, which inputs need gradients, and the
+    point -> entry adjacency (built on first use, reused by both orders)."""
+
+    __slots__ = ("points", "P", "needs", "_adj")
+
+    def __init__(self, points, P, needs):
+        self.points = points
+        self.P = P
+        self.needs = needs
+        self._adj = None
+
+    def adjacency(self, idxs):
+        if self._adj is None:
+            self._adj = _C.build_adjacency(idxs, self.P)
+        return self._adj
+
+
+def _mask(flags):
+    m = 0
+    for bit, on in zip(_NEED_BITS, flags):
+        if on:
+            m |= bit
+    return m
+
+
+class KNNAnisotropicAggregate(torch.autograd.Function):
+    """Fused kNN search and aggregation (reference
+    ``cuda_knn_aggregate/__init__.py:64-117``)."""
+
+    @staticmethod
+    def forward(ctx, q, p, f, sigma, R, K):
+        f_out, w_out, dists, idxs, points = _C.forward_ex(q, p, f, sigma, R, int(K))
+        ctx.save_for_backward(q, p, f, sigma, R, idxs)
+        ctx.aux = _Aux(points, p.shape[1], tuple(bool(x) for x in ctx.needs_input_grad[:5]))
+        return f_out, w_out, dists, idxs
+
+    @staticmethod
+    def backward(ctx, grad_f_out, grad_w_out, grad_dists, grad_idxs):
+        q, p, f, sigma, R, idxs = ctx.saved_tensors
+        if grad_f_out is None:
+            return None, None, None, None, None, None
+        grads = KNNAnisotropicAggregateBackward.apply(
+            grad_f_out.contiguous(), grad_w_out, q, p, f, sigma, R, None, idxs, ctx.aux)
+        return (*grads, None)
+
+
+class KNNAnisotropicAggregateBackward(torch.autograd.Function):
+    """First-order adjoint as a differentiable op, so that dL/dq can itself be
+    differentiated (reference ``cuda_knn_aggregate/__init__.py:216-289``).
+
+    ``apply(grad_f_out, grad_w_out, q, p, f, sigma, R, w_out, idxs)`` keeps the
+    reference's argument list; ``grad_w_out`` is ignored and ``w_out`` may be
+    None (weights are then recomputed from ``idxs``, bit-identical to the
+    forward's).  An optional tenth argument carries the forward's state."""
+
+    @staticmethod
+    def forward(ctx, grad_f_out, grad_w_out, q, p, f, sigma, R, w_out, idxs, aux=None):
+        if aux is None:
+            aux = _Aux(None, p.shape[1], (True,) * 5)
+        needs = _mask(aux.needs)
+        point_side = bool(needs & (_C.NEED_DP | _C.NEED_DF | _C.NEED_DSIGMA | _C.NEED_DR))
+        if w_out is not None:
+            # Explicit weights (reference-style call): use them as given.
+            outs = list(_C.knn_aggregate_aniso_backward(grad_f_out.contiguous(), grad_w_out.contiguous(), q, p, f,
+                                                        sigma, R, w_out.contiguous(), idxs))
+            coef = None
+        else:
+            adj = aux.adjacency(idxs) if point_side else None
+            dq, dp, df, ds, dR, coef = _C.backward_ex(grad_f_out, q, p, f, sigma, R, idxs, aux.points, adj, needs)
+            outs = [dq, dp, df, ds, dR]
+        ctx.save_for_backward(grad_f_out, q, p, f, sigma, R, idxs, coef)
+        ctx.aux = aux
+        ctx.has_w = w_out is not None
+        return tuple(outs)
+
+    @staticmethod
+    def backward(ctx, grad_grad_q, grad_grad_p, grad_grad_f, grad_grad_sigma, grad_grad_R):
+        # Only the path through dL/dq is differentiated (Eikonal), as in the
+        # reference (cuda_knn_aggregate/__init__.py:261-289).
+        grad_f_out, q, p, f, sigma, R, idxs, coef = ctx.saved_tensors
+        if grad_grad_q is None:
+            return (None,) * 10
+        ni = ctx.needs_input_grad
+        flags = (ni[2], ni[3], ni[4], ni[5], ni[6])
+        needs = _mask(flags) | (_C.NEED_DGFO if ni[0] else 0)
+        if needs == 0:
+            return (None,) * 10
+        point_side = bool(needs & (_C.NEED_DP | _C.NEED_DF | _C.NEED_DSIGMA | _C.NEED_DR))
+        adj = ctx.aux.adjacency(idxs) if point_side else None
+        dgfo, dq, dp, df, ds, dR = _C.backward2_ex(grad_grad_q.contiguous(), grad_f_out, q, p, f, sigma, R, idxs,
+                                                   ctx.aux.points, adj, coef, needs)
+        return dgfo, None, dq, dp, df, ds, dR, None, None, None

@@ -45,7 +45,7 @@ def random_rotations(n: int, g: torch.Generator, dtype=torch.float32) -> torch.T
     d = torch.sign(torch.diagonal(rm, dim1=-2, dim2=-1))
     d[d == 0] = 1.0
     qm = qm * d.unsqueeze(-2)
-    return qm.to(dtype)
+    return qm.to(dtype).contiguous()
 
 
 def uniform_cloud(shape: Shape, seed: int, dtype=torch.float32):
@@ -58,7 +58,7 @@ def uniform_cloud(shape: Shape, seed: int, dtype=torch.float32):
     f = torch.rand(B, P, F, generator=g, dtype=dtype)
     sigma = 0.05 + 0.15 * torch.rand(B, P, 3, generator=g, dtype=dtype)
     R = random_rotations(B * P, g, dtype).reshape(B, P, 3, 3)
-    return q, p, f, sigma, R
+    return tuple(t.contiguous() for t in (q, p, f, sigma, R))
 
 
 def readme_cloud(B, Q, P, F, seed: int, dtype=torch.float32):

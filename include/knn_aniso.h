@@ -1,0 +1,161 @@
+/*
+ * knn_aniso.h -- C ABI of the B200 (sm_100a) anisotropic-Gaussian kNN feature
+ * aggregation library (libknn_aniso.so).
+ *
+ * Computes, for queries q [B,Q,3] against points p [B,P,3] carrying features
+ * f [B,P,F], precisions sigma [B,P,3] and axes R [B,P,3,3] (row-major, rows
+ * are the axes):
+ *     s(q,i)  = sum_a sigma[i][a] * (R[i][a] . (q - p[i]))^2
+ *     idxs    = the K points with the smallest s, ascending (ties broken
+ *               exactly as the reference's MinK structure breaks them)
+ *     dists   = s at those points;  w_out = exp(-dists)
+ *     f_out   = sum_k w_out[k] * f[idxs[k]]   (accumulated in k order)
+ * and the first- and second-order (Eikonal, through dL/dq) adjoints.
+ *
+ * Conventions shared by every entry point:
+ *   - all tensor pointers are DEVICE pointers to dense row-major arrays;
+ *   - dtype selects float32 (KNNAG_F32) or float64 (KNNAG_F64) for every
+ *     floating-point array; idxs are int64;
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream); every launch
+ *     goes to it, nothing synchronises the host, nothing allocates device
+ *     memory: callers size scratch with the *_bytes() queries and pass it in;
+ *   - the return value is a knnag_status; KNNAG_OK means all kernels were
+ *     enqueued.  Errors detected on the device (a bounded wait that gave up)
+ *     are latched in a status word inside the caller's workspace and read
+ *     back with knnag_read_device_status().
+ *
+ * Each entry point names the reference interface it replaces (paths inside
+ * the LemonATsu/CUDA-kNN-Aniso-Gaussian-Feature-Aggregation project).
+ */
+#ifndef KNN_ANISO_H_
+#define KNN_ANISO_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  KNNAG_OK = 0,
+  KNNAG_ERR_ARG = 1,        /* null pointer, negative or inconsistent size */
+  KNNAG_ERR_K = 2,          /* K < 1 or K > P */
+  KNNAG_ERR_DTYPE = 3,      /* dtype not KNNAG_F32 / KNNAG_F64 */
+  KNNAG_ERR_WORKSPACE = 4,  /* workspace smaller than the *_bytes() query */
+  KNNAG_ERR_TOO_LARGE = 5,  /* B*Q*K or B*P exceeds the 32-bit index range */
+  KNNAG_ERR_CUDA = 6,       /* a launch failed (cudaGetLastError) */
+  KNNAG_ERR_DEVICE = 7      /* latched on the device: a bounded wait gave up */
+} knnag_status;
+
+enum { KNNAG_F32 = 0, KNNAG_F64 = 1 };
+
+/* Bits of the `needs` mask of the backward entry points: which outputs to
+ * write.  Outputs whose bit is clear may be NULL. */
+enum {
+  KNNAG_NEED_DQ = 1,
+  KNNAG_NEED_DP = 2,
+  KNNAG_NEED_DF = 4,
+  KNNAG_NEED_DSIGMA = 8,
+  KNNAG_NEED_DR = 16,
+  KNNAG_NEED_DGFO = 32,
+  KNNAG_NEED_ALL = 63
+};
+
+/* Human-readable text of a status code (static storage). */
+const char* knnag_status_string(int status);
+
+/* Library version, as major*10000 + minor*100 + patch. */
+int knnag_version(void);
+
+/* ------------------------------------------------------------------ forward */
+
+/* Bytes of scratch knnag_forward needs (256-byte aligned base expected). */
+size_t knnag_forward_workspace_bytes(int B, int Q, int P, int F, int K, int dtype);
+
+/*
+ * Fused kNN search + weighted feature aggregation.
+ * Replaces knn_aggregate_aniso_forward (csrc/knn_aggregate.cpp:26-47) and its
+ * launcher knn_aggregate_aniso_forward_cuda (csrc/forward.cu:286-338) with the
+ * kernel csrc/forward.cu:56-110 and csrc/mink.cuh.
+ * Outputs: f_out [B,Q,F], w_out [B,Q,K], dists [B,Q,K] (dtype), idxs [B,Q,K]
+ * int64.  Requires 1 <= K <= P.  `points` (optional, may be NULL) receives the
+ * packed per-point records (knnag_points_bytes) that the backward entry
+ * points can reuse instead of re-packing p, sigma and R.
+ */
+int knnag_forward(const void* q, const void* p, const void* f, const void* sigma, const void* R,
+                  int B, int Q, int P, int F, int K, int dtype,
+                  void* f_out, void* w_out, void* dists, int64_t* idxs,
+                  void* points, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------- adjoint index */
+
+/* Bytes of the packed per-point records (16 values of dtype per point). */
+size_t knnag_points_bytes(int B, int P, int dtype);
+
+/* Pack p, sigma and R into per-point records (what knnag_forward also writes). */
+int knnag_pack_points(const void* p, const void* sigma, const void* R, int B, int P, int dtype,
+                      void* points, void* stream);
+
+/* Bytes of the point->entry adjacency (CSR) built by knnag_build_adjacency. */
+size_t knnag_adjacency_bytes(int B, int Q, int P, int K);
+
+/*
+ * Inverse neighbour lists: for every point (b,i), the entries e = (b*Q+q)*K+k
+ * with idxs[e] == i, in increasing e.  Deterministic.  `adjacency` holds
+ * rowptr [B*P+1] int32 followed by the entry lists [B*Q*K] int32 and scratch.
+ * No reference counterpart: the reference scatters with float atomicAdd
+ * (csrc/backward.cu:91,102-119,291,308-326) instead.
+ */
+int knnag_build_adjacency(const int64_t* idxs, int B, int Q, int P, int K, void* adjacency, void* stream);
+
+/* --------------------------------------------------------------- backward */
+
+/* Bytes of scratch knnag_backward / knnag_backward_2nd need. */
+size_t knnag_backward_workspace_bytes(int B, int Q, int P, int F, int K, int dtype);
+
+/*
+ * First-order adjoint of f_out.
+ * Replaces knn_aggregate_aniso_backward (csrc/knn_aggregate.cpp:101-132) and
+ * knn_aggregate_aniso_backward_cuda (csrc/backward.cu:331-389, kernel
+ * csrc/backward.cu:5-121).  grad_w_out is accepted and ignored, as in the
+ * reference (csrc/backward.cu:93-94).  w_out may be NULL: weights are then
+ * recomputed from idxs (bit-identical to the forward's).  points/adjacency
+ * may be NULL: they are then built in the workspace.  coef_out (optional,
+ * [B,Q,K] dtype) receives c = grad_f_out[q] . f[idx], reusable by
+ * knnag_backward_2nd.  Outputs: dq [B,Q,3], dp [B,P,3], df [B,P,F],
+ * dsigma [B,P,3], dR [B,P,3,3], each written in full when its `needs` bit is set.
+ */
+int knnag_backward(const void* grad_f_out, const void* grad_w_out,
+                   const void* q, const void* p, const void* f, const void* sigma, const void* R,
+                   const void* w_out, const int64_t* idxs,
+                   int B, int Q, int P, int F, int K, int dtype, int needs,
+                   const void* points, const void* adjacency,
+                   void* dq, void* dp, void* df, void* dsigma, void* dR, void* coef_out,
+                   void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Second-order adjoint through dL/dq (Eikonal): gradients of
+ * <grad_grad_q, dq(grad_f_out)> w.r.t. grad_f_out, q, p, f, sigma and R.
+ * Replaces knn_aggregate_aniso_backward_2nd (csrc/knn_aggregate.cpp:135-172)
+ * and knn_aggregate_aniso_backward_2nd_cuda (csrc/backward.cu:392-455, kernel
+ * csrc/backward.cu:124-328).  grad_w_out is ignored.  coef (optional) is the
+ * coef_out of the matching knnag_backward call; NULL recomputes it.
+ * Outputs: dgfo [B,Q,F], dq [B,Q,3], dp, df, dsigma, dR as above.
+ */
+int knnag_backward_2nd(const void* grad_grad_q, const void* grad_f_out, const void* grad_w_out,
+                       const void* q, const void* p, const void* f, const void* sigma, const void* R,
+                       const void* w_out, const int64_t* idxs,
+                       int B, int Q, int P, int F, int K, int dtype, int needs,
+                       const void* points, const void* adjacency, const void* coef,
+                       void* dgfo, void* dq, void* dp, void* df, void* dsigma, void* dR,
+                       void* workspace, size_t workspace_bytes, void* stream);
+
+/* Copy the device status word latched in a forward/backward workspace to the
+ * host (synchronises `stream`) and clear it; returns KNNAG_OK or KNNAG_ERR_DEVICE. */
+int knnag_read_device_status(void* workspace, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KNN_ANISO_H_ */

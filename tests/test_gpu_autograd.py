@@ -1,0 +1,167 @@
+"""The autograd layer on the GPU: the Eikonal training step against the FP64
+oracle, FP64 gradcheck of the first- and second-order kernels against finite
+differences, and the reference-compatible `_C` ops.
+
+Tolerances: forward 1e-5, gradients 1e-4 (relative to each tensor's max).
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_err
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda:0")
+
+
+def make(**kw):
+    from cuda_knn_aggregate import workloads as W
+
+    dtype = kw.pop("dtype", torch.float32)
+    return W.make("small", dtype=dtype, **kw)
+
+
+def test_eikonal_step_vs_fp64_oracle():
+    from cuda_knn_aggregate import knn_aggregate_aniso
+
+    shape, t = make(B=2, Q=1000, P=500, F=32, K=12)
+    K = shape.K
+    ins = [x.to(DEV).requires_grad_(True) for x in t]
+    f_out, w_out, dists, idxs = knn_aggregate_aniso(*ins, K)
+    (gq,) = torch.autograd.grad(f_out.sum(), ins[0], create_graph=True)
+    loss = ((gq.norm(dim=-1) - 1.0) ** 2).mean()
+    loss.backward()
+
+    ref = [x.double().clone().requires_grad_(True) for x in t]
+    fo, _ = O.aggregate64(*ref, idxs.cpu())
+    (g64,) = torch.autograd.grad(fo.sum(), ref[0], create_graph=True)
+    l64 = ((g64.norm(dim=-1) - 1.0) ** 2).mean()
+    l64.backward()
+    assert rel_err(f_out.detach().cpu().numpy(), fo.detach().numpy()) < 1e-5
+    assert rel_err(gq.detach().cpu().numpy(), g64.detach().numpy()) < 1e-4
+    assert abs(loss.item() - l64.item()) <= 1e-4 * abs(l64.item())
+    for a, b in zip(ins, ref):
+        assert rel_err(a.grad.cpu().numpy(), b.grad.numpy()) < 1e-4
+
+
+def test_full_backward_vs_oracle():
+    """loss = <v, f_out>: all first-order gradients through the autograd layer."""
+    from cuda_knn_aggregate import knn_aggregate_aniso
+
+    shape, t = make(B=2, Q=700, P=900, F=20, K=16, seed=3)
+    ins = [x.to(DEV).requires_grad_(True) for x in t]
+    f_out, _, _, idxs = knn_aggregate_aniso(*ins, shape.K)
+    v = torch.randn_like(f_out)
+    (f_out * v).sum().backward()
+    ref = [x.double() for x in t]
+    first, _ = O.grads64(*ref, idxs.cpu(), v.double().cpu())
+    for a, g in zip(ins, first):
+        assert rel_err(a.grad.cpu().numpy(), g.numpy()) < 1e-4
+
+
+def test_gradients_of_w_out_and_dists_are_ignored():
+    """As in the reference, only f_out carries gradient."""
+    from cuda_knn_aggregate import knn_aggregate_aniso
+
+    shape, t = make(B=1, Q=64, P=200, F=4, K=8, seed=4)
+    ins = [x.to(DEV).requires_grad_(True) for x in t]
+    f_out, w_out, dists, _ = knn_aggregate_aniso(*ins, shape.K)
+    (w_out.sum() + dists.sum()).backward()
+    for a in ins:
+        assert a.grad is None or torch.count_nonzero(a.grad) == 0
+
+
+def test_gradcheck_first_and_second_order_fp64():
+    """FP64 finite-difference checks at Q=64, P=128 (F=8, K=4): f_out w.r.t.
+    every input, and dL/dq (the Eikonal path) w.r.t. every input."""
+    from cuda_knn_aggregate import knn_aggregate_aniso
+
+    shape, t = make(B=1, Q=64, P=128, F=8, K=4, seed=11, dtype=torch.float64)
+    K = shape.K
+    ins = tuple(x.to(DEV).requires_grad_(True) for x in t)
+
+    def fwd(q, p, f, sigma, R):
+        return knn_aggregate_aniso(q, p, f, sigma, R, K)[0]
+
+    assert torch.autograd.gradcheck(fwd, ins, eps=1e-6, atol=1e-7, rtol=1e-4)
+
+    g = torch.Generator().manual_seed(0)
+    v = torch.randn(1, 64, 8, generator=g, dtype=torch.float64).to(DEV)
+
+    def dq(q, p, f, sigma, R):
+        out = knn_aggregate_aniso(q, p, f, sigma, R, K)[0]
+        return torch.autograd.grad((out * v).sum(), q, create_graph=True)[0]
+
+    assert torch.autograd.gradcheck(dq, ins, eps=1e-6, atol=1e-7, rtol=1e-4)
+
+
+def test_reference_compatible_ops():
+    """_C keeps the reference's op names, argument lists and return lists."""
+    from cuda_knn_aggregate import _C
+
+    shape, t = make(B=2, Q=100, P=300, F=8, K=6, seed=12)
+    q, p, f, sigma, R = [x.to(DEV) for x in t]
+    f_out, w_out, dists, idxs = _C.knn_aggregate_aniso_forward(q, p, f, sigma, R, 6)
+    gfo = torch.randn_like(f_out)
+    gwo = torch.zeros_like(w_out)
+    ggq = torch.randn_like(q)
+    b1 = _C.knn_aggregate_aniso_backward(gfo, gwo, q, p, f, sigma, R, w_out, idxs)
+    b2 = _C.knn_aggregate_aniso_backward_2nd(ggq, gfo, gwo, q, p, f, sigma, R, w_out, idxs)
+    assert len(b1) == 5 and len(b2) == 6
+    first, second = O.grads64(*[x.double().cpu() for x in (q, p, f, sigma, R)], idxs.cpu(), gfo.double().cpu(),
+                              ggq.double().cpu())
+    for a, r in zip(b1, first):
+        assert rel_err(a.cpu().numpy(), r.numpy()) < 1e-4
+    for a, r in zip(b2, second):
+        assert rel_err(a.cpu().numpy(), r.numpy()) < 1e-4
+
+
+def test_errors_follow_reference_wording():
+    from cuda_knn_aggregate import knn_aggregate_aniso
+
+    _, t = make(B=1, Q=8, P=16, F=4, K=4)
+    q, p, f, sigma, R = [x.to(DEV) for x in t]
+    with pytest.raises(RuntimeError, match="must be a CUDA tensor"):
+        knn_aggregate_aniso(q.cpu(), p, f, sigma, R, 4)
+    with pytest.raises(RuntimeError, match="must be contiguous"):
+        knn_aggregate_aniso(q.transpose(0, 1).contiguous().transpose(0, 1)[:, ::2], p, f, sigma, R, 4)
+    with pytest.raises(RuntimeError, match="K must satisfy"):
+        knn_aggregate_aniso(q, p, f, sigma, R, 17)
+
+
+def test_step_is_capturable_in_a_cuda_graph():
+    """Forward + autograd.grad(create_graph) + backward replays in a graph with
+    the same results as eager execution."""
+    from cuda_knn_aggregate import knn_aggregate_aniso
+
+    shape, t = make(B=2, Q=512, P=700, F=16, K=12, seed=13)
+    ins = [x.to(DEV).requires_grad_(True) for x in t]
+
+    def step():
+        for a in ins:
+            a.grad = None
+        f_out, _, _, _ = knn_aggregate_aniso(*ins, shape.K)
+        (gq,) = torch.autograd.grad(f_out.sum(), ins[0], create_graph=True)
+        loss = ((gq.norm(dim=-1) - 1.0) ** 2).mean()
+        loss.backward()
+        return loss.detach()
+
+    eager = step()
+    eager_grads = [a.grad.clone() for a in ins]
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for _ in range(2):
+            step()
+    torch.cuda.current_stream().wait_stream(s)
+    g = torch.cuda.CUDAGraph()
+    for a in ins:
+        a.grad = None
+    with torch.cuda.graph(g):
+        out = step()
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(out, eager)
+    for a, e in zip(ins, eager_grads):
+        assert torch.equal(a.grad, e)
