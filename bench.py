@@ -1,0 +1,493 @@
+"""Benchmark of the knn_aggregate_aniso training step.
+
+One step = forward (fused kNN search + aggregation), dq = d(sum f_out)/dq
+with create_graph, Eikonal loss mean((|dq| - 1)^2), backward into q, p, f,
+sigma and R -- the forward + first- + second-order path.  Workload: the
+reference README's timing-table shape, B=2, Q=12288, P=4096, F=64, K=16,
+FP32, seeded synthetic uniform-cube inputs.  One unit = one query.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference|reference-ext]
+
+--impl ours (default): the CUDA path, steps replayed from a CUDA graph with
+    inputs resident in HBM, L2 flushed between steps (inputs are smaller than
+    L2).  Prints one JSON line with value, e2e (public API with host buffers
+    and copies in the timed region), roofline of the search kernel, the CPU
+    baseline, clocks and launch counts.
+--impl reference: the reference path on this machine's host cores (the
+    reference ships no CPU implementation, so the plain-PyTorch CPU
+    formulation of the op is timed -- all threads -- on a bounded sample of the
+    same workload).
+--impl reference-ext: the reference CUDA extension, compiled from its own
+    sources, on the same GPU through autograd wiring equivalent to the
+    reference's package (eager; it launches on the legacy default stream).
+
+Under torchrun each rank runs its own batch (independent clouds: no
+collective on the data path, weak scaling); rank 0 prints the line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "cuda-knn-aniso-gaussian-feature-aggregation_b200")
+sys.path.insert(0, PKG_DIR)
+
+METRIC = "fwd+1st+2nd-order queries/s"
+UNIT = "queries/s"
+WORKLOAD = dict(name="table", B=2, Q=12288, P=4096, F=64, K=16)
+FLOP_PER_PAIR = 26          # 3 sub, 3x(1 mul + 2 fma), 3 squares, 1 mul + 2 fma
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def init_dist(ws, local, backend):
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+
+
+def max_over_ranks(x: float, ws: int, device) -> float:
+    if ws == 1:
+        return x
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.2)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        loaded = [x for x in sm if mx and x > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_inputs(rank, device):
+    from cuda_knn_aggregate import workloads as W
+
+    shape, t = W.make(WORKLOAD["name"], seed=1001 + 7919 * rank)
+    return shape, t
+
+
+def eikonal_step_fn(op, ins, K):
+    def step():
+        for a in ins:
+            a.grad = None
+        f_out = op(*ins, K)[0]
+        (gq,) = torch.autograd.grad(f_out.sum(), ins[0], create_graph=True)
+        loss = ((gq.norm(dim=-1) - 1.0) ** 2).mean()
+        loss.backward()
+        return loss.detach()
+
+    return step
+
+# ---------------------------------------------------------------- CPU side
+
+def cpu_step_rate(q_per_batch: int, min_seconds: float = 0.0, iters: int | None = None):
+    """Plain-PyTorch FP32 formulation of the step on the host cores (all
+    threads), on the first q_per_batch queries of each batch element of the
+    workload, for exactly `iters` iterations or, when iters is None, until
+    min_seconds have passed (at least 2); returns (queries/s, iterations,
+    seconds, threads)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    torch.set_num_threads(os.cpu_count() or 1)
+    shape, t = make_inputs(0, "cpu")
+    q = t[0][:, :q_per_batch].contiguous()
+    base = [q] + [x.clone() for x in t[1:]]
+    fwd = lambda *a: O.plain_forward(*a, chunk=256)
+    n, t0 = 0, time.perf_counter()
+    while True:
+        ins = [x.clone().requires_grad_(True) for x in base]
+        O.eikonal_step(*ins, shape.K, forward=fwd)
+        n += 1
+        el = time.perf_counter() - t0
+        if (iters is not None and n >= iters) or (iters is None and el >= min_seconds and n >= 2):
+            break
+    return shape.B * q_per_batch * n / el, n, el, torch.get_num_threads()
+
+
+def cpu_baseline_block(seconds=12.0, q_per_batch=2048):
+    rate, n, el, thr = cpu_step_rate(q_per_batch, seconds)
+    return {"value": rate, "unit": UNIT, "cores": thr, "kind": "port",
+            "sample": f"plain-PyTorch FP32 step (oracle/oracle.py) on {q_per_batch} of 12288 queries per batch "
+                      f"element, full P=4096, {n} iterations in {el:.1f} s"}
+
+
+# ------------------------------------------------------------ reference ext
+
+def load_reference_ext():
+    import importlib.util
+
+    path = os.path.join(ROOT, "oracle", "_ref", "knn_ref_C.so")
+    if not os.path.exists(path):
+        return None, "reference extension not built (python oracle/build_ref.py needs the reference sources)"
+    spec = importlib.util.spec_from_file_location("knn_ref_C", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod, None
+
+
+def reference_ext_op(ref):
+    """The reference package's autograd wiring (cuda_knn_aggregate/__init__.py:
+    64-117 and 216-289 of the reference) around the reference's own ops."""
+
+    class RefBackward(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, gfo, gwo, q, p, f, sigma, R, w_out, idxs):
+            outs = ref.knn_aggregate_aniso_backward(gfo, gwo, q, p, f, sigma, R, w_out, idxs)
+            ctx.save_for_backward(gfo, gwo, q, p, f, sigma, R, w_out, idxs)
+            return tuple(outs)
+
+        @staticmethod
+        def backward(ctx, ggq, ggp, ggf, ggs, ggR):
+            gfo, gwo, q, p, f, sigma, R, w_out, idxs = ctx.saved_tensors
+            o = ref.knn_aggregate_aniso_backward_2nd(ggq.contiguous(), gfo.contiguous(), gwo.contiguous(), q, p, f,
+                                                     sigma, R, w_out, idxs)
+            return o[0], None, o[1], o[2], o[3], o[4], o[5], None, None
+
+    class RefAgg(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, q, p, f, sigma, R, K):
+            f_out, w_out, dists, idxs = ref.knn_aggregate_aniso_forward(q, p, f, sigma, R, K)
+            ctx.save_for_backward(q, p, f, sigma, R, w_out, idxs)
+            return f_out, w_out, dists, idxs
+
+        @staticmethod
+        def backward(ctx, gfo, gwo, gd, gi):
+            q, p, f, sigma, R, w_out, idxs = ctx.saved_tensors
+            g = RefBackward.apply(gfo.contiguous(), gwo.contiguous(), q, p, f, sigma, R, w_out, idxs)
+            return (*g, None)
+
+    return RefAgg.apply
+
+
+def time_reference_ext(device, steps, warmup):
+    ref, why = load_reference_ext()
+    if ref is None:
+        return {"unavailable": why}
+    shape, t = make_inputs(0, device)
+    ins = [x.to(device).requires_grad_(True) for x in t]
+    step = eikonal_step_fn(reference_ext_op(ref), ins, shape.K)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step()
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = statistics.mean(times)
+    return {"value": shape.B * shape.Q / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "steps": steps,
+            "how": "reference extension compiled from its own sources (sm_100), reference autograd wiring, eager"}
+
+
+# ------------------------------------------------------------------- arms
+
+def fp32_peak_tflops(device):
+    from cuda_knn_aggregate import capi
+
+    blocks, iters = 148 * 8, 8192
+    out = torch.empty(blocks * 256, dtype=torch.float32, device=device)
+    for _ in range(2):
+        capi.fp32_peak_probe(out, blocks, iters)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = 0.0
+    for _ in range(3):
+        e0.record()
+        capi.fp32_peak_probe(out, blocks, iters)
+        e1.record()
+        e1.synchronize()
+        best = max(best, blocks * 256 * iters * 32 / (e0.elapsed_time(e1) / 1e3) / 1e12)
+    return best
+
+
+def read_profile_traffic():
+    """Per-launch DRAM bytes of the search kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "search_f32_table.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+def run_ours(args):
+    ws, rank, local = dist_env()
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    init_dist(ws, local, "nccl")
+    from cuda_knn_aggregate import capi, knn_aggregate_aniso
+
+    shape, t = make_inputs(rank, device)
+    K, units = shape.K, shape.B * shape.Q
+    ins = [x.to(device).requires_grad_(True) for x in t]
+    step = eikonal_step_fn(knn_aggregate_aniso, ins, K)
+
+    ev_sb, ev_se = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev_sb.record()
+    ev_se.record()
+    torch.cuda.synchronize()
+    capi.set_profile_events(ev_sb, ev_se)
+
+    c0 = capi.launch_count()
+    step()
+    torch.cuda.synchronize()
+    launches_per_step = capi.launch_count() - c0
+
+    # eager timing (for reference; the headline uses the captured step)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
+    eager = []
+    for _ in range(max(3, args.warmup)):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step()
+        e1.record()
+        e1.synchronize()
+        eager.append(e0.elapsed_time(e1))
+
+    side = torch.cuda.Stream(device)
+    side.wait_stream(torch.cuda.current_stream(device))
+    with torch.cuda.stream(side):
+        for _ in range(3):
+            step()
+    torch.cuda.current_stream(device).wait_stream(side)
+    graph = torch.cuda.CUDAGraph()
+    for a in ins:
+        a.grad = None
+    with torch.cuda.graph(graph):
+        step()
+    for _ in range(args.warmup):
+        flush.zero_()
+        graph.replay()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier(ws)
+    torch.cuda.synchronize()
+    step_ms, search_ms = [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        graph.replay()
+        e1.record()
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        search_ms.append(ev_sb.elapsed_time(ev_se))
+    torch.cuda.synchronize()
+    barrier(ws)
+    clocks = sampler.stop()
+    capi.set_profile_events(None, None)
+
+    ms = max_over_ranks(statistics.mean(step_ms), ws, device)
+    value = ws * units / (ms / 1e3)
+
+    # end to end through the public API: host inputs in pinned memory,
+    # H2D copies + step + D2H of the loss inside the timed region
+    host = [x.detach().cpu().pin_memory() for x in t]
+    loss_h = torch.empty((), dtype=torch.float32).pin_memory()
+    h2d = sum(x.numel() * x.element_size() for x in host)
+    e2e = []
+    for i in range(args.warmup + args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dev_in = [x.to(device, non_blocking=True).requires_grad_(True) for x in host]
+        f_out = knn_aggregate_aniso(*dev_in, K)[0]
+        (gq,) = torch.autograd.grad(f_out.sum(), dev_in[0], create_graph=True)
+        loss = ((gq.norm(dim=-1) - 1.0) ** 2).mean()
+        loss.backward()
+        loss_h.copy_(loss.detach(), non_blocking=True)
+        e1.record()
+        e1.synchronize()
+        if i >= args.warmup:
+            e2e.append(e0.elapsed_time(e1))
+    e2e_ms = max_over_ranks(statistics.mean(e2e), ws, device)
+
+    if rank != 0:
+        barrier(ws)
+        return None
+
+    search_s = statistics.median(search_ms) / 1e3
+    pairs = shape.B * shape.Q * shape.P
+    peak = fp32_peak_tflops(device)
+    achieved = FLOP_PER_PAIR * pairs / search_s / 1e12
+    roofline = {"bound": "fp32", "kernel": "search_f32_kernel", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak,
+                "peak_source": "measured: FFMA-bound probe kernel in bench.py (MEASURED_PEAKS.json has no FP32 figure)",
+                "algorithmic": f"{FLOP_PER_PAIR} FLOP x {pairs} (q,p) pairs per launch",
+                "launch_ms": search_s * 1e3, "traffic": read_profile_traffic()}
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded uniform cube, README timing-table shape)",
+        "config": {"workload": "table: B=2 Q=12288 P=4096 F=64 K=16, fwd + dq(create_graph) + Eikonal backward",
+                   "queries_per_gpu": units, "parallelism": f"independent batches per rank x{ws}",
+                   "l2": "flushed between timed steps (256 MiB write)", "execution": "CUDA graph replay"},
+        "e2e": {"value": ws * units / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": loss_h.element_size(),
+                "how": "public API knn_aggregate_aniso + autograd, eager, pinned host inputs"},
+        "roofline": roofline,
+        "clocks": clocks,
+        "gpu_launches": launches_per_step * args.steps,
+        "gpu_launches_per_step": launches_per_step,
+        "eager_ms_per_step": statistics.mean(eager),
+    }
+    if ws == 1 and not args.no_reference_ext:
+        out["reference_ext"] = time_reference_ext(device, min(args.steps, 10), 2)
+        if "ms_per_step" in out["reference_ext"]:
+            out["reference_ext"]["speedup_value"] = out["reference_ext"]["ms_per_step"] / ms
+            out["reference_ext"]["speedup_e2e"] = out["reference_ext"]["ms_per_step"] / e2e_ms
+    if ws == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_block()
+    print(json.dumps(out), flush=True)
+    barrier(ws)
+    return out
+
+
+def run_reference_cpu(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return None
+    q_per_batch = 2048
+    cpu_step_rate(q_per_batch, iters=args.warmup)
+    rate, n, el, thr = cpu_step_rate(q_per_batch, iters=args.steps)
+    ms = el / n * 1e3
+    block = {"value": rate, "unit": UNIT, "cores": thr, "kind": "port",
+             "sample": f"plain-PyTorch FP32 step (oracle/oracle.py) on {q_per_batch} of 12288 queries per batch "
+                       f"element of the table workload, full P=4096; {n} steps"}
+    out = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "impl": "reference", "data": "synthetic (seeded uniform cube, README timing-table shape)",
+           "config": {"workload": "table: B=2 Q=12288 P=4096 F=64 K=16 (bounded query sample per step)",
+                      "note": "the reference ships no CPU implementation; its op is timed as the plain-PyTorch "
+                              "formulation on all host threads"},
+           "cpu_baseline": block,
+           "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return out
+
+
+def run_reference_ext(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return None
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    r = time_reference_ext(device, args.steps, args.warmup)
+    out = {"metric": METRIC, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "higher_is_better": True, "impl": "reference-ext", "dtype": "f32", **r}
+    print(json.dumps(out), flush=True)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-ext"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-ext", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        run_reference_cpu(args)
+    elif args.impl == "reference-ext":
+        run_reference_ext(args)
+    else:
+        run_ours(args)
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    if ws > 1 and args.impl == "ours":
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -176,6 +176,7 @@ int launch_build_adjacency(const int64_t* idxs, int B, int Q, int P, int K, void
   adj_scan_kernel<<<1, 1024, 0, st>>>(cursor, rows, rowptr);
   adj_fill_kernel<<<blocks_for(n, 256), 256, 0, st>>>(idxs, n, qk, P, rowptr, cursor, unsorted);
   adj_sort_kernel<<<blocks_for(rows * 32, 256), 256, 0, st>>>(rowptr, unsorted, rows, entries);
+  note_launches(4);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 
@@ -522,6 +523,7 @@ int launch_query(const QueryParams<T>& p, int order, bool v4, cudaStream_t st) {
     else
       query_side_kernel<T, 2, false><<<grid, 128, 0, st>>>(p);
   }
+  note_launches(1);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 
@@ -537,6 +539,7 @@ int launch_point_o(const PointParams<T>& p, cudaStream_t st) {
     point_side_kernel<T, ORDER, 4><<<grid, 256, 0, st>>>(p);
   else
     point_side_kernel<T, ORDER, 8><<<grid, 256, 0, st>>>(p);
+  note_launches(1);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 

@@ -3,13 +3,65 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "knn_aniso.h"
 #include "knn_common.cuh"
 #include "knn_internal.h"
 
 using namespace knnag;
 
+namespace knnag {
+
+static std::atomic<long long> g_launches{0};
+static std::atomic<void*> g_ev_begin{nullptr}, g_ev_end{nullptr};
+
+void note_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// Record a profiling event on `st`: as an external event node while the
+// stream is being captured into a graph, as a plain record otherwise.  A
+// failed record is cleared so it cannot be mistaken for a launch error.
+static void record_profile_event(void* e, cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  const cudaError_t rc = (cs == cudaStreamCaptureStatusActive)
+                             ? cudaEventRecordWithFlags(static_cast<cudaEvent_t>(e), st, cudaEventRecordExternal)
+                             : cudaEventRecord(static_cast<cudaEvent_t>(e), st);
+  if (rc != cudaSuccess) cudaGetLastError();
+}
+
+void profile_begin(cudaStream_t st) {
+  void* e = g_ev_begin.load();
+  if (e && g_ev_end.load()) record_profile_event(e, st);
+}
+
+void profile_end(cudaStream_t st) {
+  void* e = g_ev_end.load();
+  if (e && g_ev_begin.load()) record_profile_event(e, st);
+}
+
+}  // namespace knnag
+
 namespace {
+
+// 16 independent FMA chains per thread: FP32-pipe bound.
+__global__ void fp32_peak_kernel(float* out, int iters) {
+  float v[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = threadIdx.x * 1e-3f + i;
+  const float a = 0.999f, b = 1e-4f;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __fmaf_rn(v[i], a, b);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) s += v[i];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
 
 constexpr int64_t kI32Max = 2147483647;
 
@@ -194,6 +246,20 @@ int knnag_read_device_status(void* workspace, void* stream) {
     return KNNAG_ERR_DEVICE;
   }
   return KNNAG_OK;
+}
+
+void knnag_set_profile_events(void* ev_begin, void* ev_end) {
+  g_ev_begin.store(ev_begin);
+  g_ev_end.store(ev_end);
+}
+
+long long knnag_launch_count(void) { return g_launches.load(); }
+
+int knnag_fp32_peak_probe(float* out, int blocks, int iters, void* stream) {
+  if (!out || blocks < 1 || iters < 1) return KNNAG_ERR_ARG;
+  fp32_peak_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(out, iters);
+  note_launches(1);
+  return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 
 }  // extern "C"

@@ -32,10 +32,10 @@ enum RecField {
   kRecLen = 16
 };
 
-// Points per search tile and the pair-interleaved tile layout: a pair of
+// Points per search tile (8 KB) and the pair-interleaved tile layout: a pair of
 // points (2m, 2m+1) is 16 float2 = 128 bytes, field f of the pair at float2
 // slot f, so packed f32x2 arithmetic reads both points' field with one load.
-constexpr int kTilePoints = 256;
+constexpr int kTilePoints = 128;
 constexpr int kPairFloats = 32;
 
 __host__ __device__ inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }

@@ -48,8 +48,8 @@ __host__ __device__ inline constexpr size_t search_merge_bytes(int kmax, int g) 
   return (g > 1) ? (size_t)kSearchThreads * (kmax + 1) * 8 + (size_t)kSearchThreads * 4 : 0;
 }
 __host__ __device__ inline constexpr size_t search_region_a_bytes(int kmax, int g) {
-  // phase 1: two tiles of 128 pairs x 128 B
-  size_t tiles = 2 * 128 * 128;
+  // phase 1: two tiles of 64 pairs x 128 B
+  size_t tiles = 2 * 64 * 128;
   int qpc = 32 * (4 / g);
   int L = kmax + 1;
   size_t merge = (g > 1) ? (size_t)kSearchThreads * L * 8 + (size_t)kSearchThreads * 4 : 0;
@@ -79,6 +79,11 @@ struct AdjLayout {
   size_t rowptr, cursor, unsorted, entries, total;
 };
 AdjLayout adj_layout(int B, int Q, int P, int K);
+
+// Instrumentation shared by the .cu files (defined in knn_capi.cu).
+void note_launches(int n);
+void profile_begin(cudaStream_t st);
+void profile_end(cudaStream_t st);
 
 inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 

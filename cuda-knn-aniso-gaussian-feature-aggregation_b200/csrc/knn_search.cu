@@ -60,111 +60,176 @@ __global__ void pack_pairs_kernel(const float* __restrict__ rec, int B, int P, i
 
 // ------------------------------------------------------------ exact MinK
 //
-// One warp per query.  Keys are computed 32 points at a time (one per lane,
-// same arithmetic as everywhere else); the selection then follows the
-// reference's MinK rules literally (csrc/mink.cuh:60-81):
+// One CTA per query.  All threads compute the query's keys (same arithmetic
+// as everywhere else) into shared memory, chunk by chunk; warp 0 then runs
+// the reference's MinK selection over them in index order
+// (csrc/mink.cuh:60-81):
 //   fill:  the first K points take slots 0..K-1; the tracked maximum moves
 //          only for the very first key or a strictly larger one;
 //   full:  a point is taken only if strictly below the tracked maximum; it
-//          overwrites the maximum's slot, then the maximum is re-found with a
-//          strict '>' scan starting from the new key (the old slot is kept
-//          when no slot is strictly larger);
-//   sort:  bubble sort with a strict '<' swap (csrc/mink.cuh:99-112).
-// A ballot skips 32-point chunks in which no lane is below the maximum;
-// since the maximum only falls, lanes outside the ballot would be rejected
-// anyway.  All lanes hold the same (size, max) state; slot arrays live in
-// shared memory and lane 0 writes them.
+//          overwrites the maximum's slot; the maximum is re-found by a strict
+//          '>' scan that starts from the new key, i.e. it becomes the first
+//          slot holding the largest key strictly above the new key, and stays
+//          on the written slot when there is none;
+//   sort:  bubble sort with a strict '<' swap (csrc/mink.cuh:99-112), which
+//          without NaN keys is the stable sort by key.
+// For K <= 32 slot s lives in lane s, so the re-scan is a warp max plus a
+// ballot and the sort a stable rank; for K > 32, or when a kept key is NaN,
+// lane 0 runs the rules sequentially on shared-memory slots.  A ballot
+// skips keys that are not below the current maximum (it only falls, so they
+// would be rejected anyway).
+
+constexpr int kReplayThreads = 256;
+
 template <typename T>
-__global__ void __launch_bounds__(128) mink_exact_kernel(ExactParams<T> a) {
+__host__ __device__ constexpr int replay_chunk() { return sizeof(T) == 4 ? 8192 : 4096; }
+
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+template <typename T>
+__device__ void bubble_sort_slots(T* sk, int* sv, int size) {
+  for (int x = 0; x < size - 1; ++x)
+    for (int y = 0; y < size - x - 1; ++y)
+      if (sk[y + 1] < sk[y]) {
+        const T tk = sk[y];
+        const int tv = sv[y];
+        sk[y] = sk[y + 1];
+        sv[y] = sv[y + 1];
+        sk[y + 1] = tk;
+        sv[y + 1] = tv;
+      }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams<T> a) {
+  constexpr int CH = replay_chunk<T>();
+  constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  T* sk = reinterpret_cast<T*>(smem_raw) + (size_t)warp * a.K;
-  int* sv = reinterpret_cast<int*>(reinterpret_cast<T*>(smem_raw) + (size_t)4 * a.K) + (size_t)warp * a.K;
-
-  const int64_t n_items = a.use_list ? (int64_t)(*a.list_count) : (int64_t)a.B * a.Q;
-  const int64_t gwarp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  T* skey = reinterpret_cast<T*>(smem_raw);
+  T* slot_k = skey + CH;
+  int* slot_v = reinterpret_cast<int*>(slot_k + a.K);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int K = a.K, P = a.P, F = a.F;
+  const bool in_lanes = K <= 32;
+  const int64_t n_items = a.use_list ? (int64_t)(*a.list_count) : (int64_t)a.B * a.Q;
 
-  for (int64_t item = gwarp; item < n_items; item += nwarps) {
+  for (int64_t item = blockIdx.x; item < n_items; item += gridDim.x) {
     const int64_t bq = a.use_list ? (int64_t)a.list[item] : item;
     const int64_t b = bq / a.Q;
     const T qx = a.q[bq * 3 + 0], qy = a.q[bq * 3 + 1], qz = a.q[bq * 3 + 2];
     const T* recb = a.rec + b * (int64_t)P * kRecLen;
 
-    int size = 0, max_idx = 0;
-    T max_key = T(0);
-    for (int base = 0; base < P; base += 32) {
-      const int i = base + lane;
-      const int nvalid = min(32, P - base);
-      T key = T(0);
-      if (i < P) key = key_rec<T>(qx, qy, qz, recb + (int64_t)i * kRecLen);
-      int j = 0;
-      while (j < nvalid && size < K) {  // fill phase (uniform)
-        const T kj = __shfl_sync(0xffffffffu, key, j);
-        if (lane == 0) {
-          sk[size] = kj;
-          sv[size] = base + j;
-        }
-        if (size == 0 || kj > max_key) {
-          max_key = kj;
-          max_idx = size;
-        }
-        ++size;
-        ++j;
-      }
-      __syncwarp();
-      if (j < nvalid) {
-        unsigned cand = __ballot_sync(0xffffffffu, lane >= j && lane < nvalid && key < max_key);
-        while (cand) {
-          const int l = __ffs(cand) - 1;
-          cand &= cand - 1;
-          const T kl = __shfl_sync(0xffffffffu, key, l);
-          if (kl < max_key) {
-            if (lane == 0) {
-              sk[max_idx] = kl;
-              sv[max_idx] = base + l;
+    int size = 0, max_idx = 0, my_v = -1;
+    T max_key = T(0), my_k = T(0);
+    for (int c0 = 0; c0 < P; c0 += CH) {
+      const int n = min(CH, P - c0);
+      for (int i = tid; i < n; i += kReplayThreads) skey[i] = key_rec<T>(qx, qy, qz, recb + (int64_t)(c0 + i) * kRecLen);
+      __syncthreads();
+      if (warp == 0) {
+        for (int base = 0; base < n; base += 32) {
+          const int nvalid = min(32, n - base);
+          const T key = lane < nvalid ? skey[base + lane] : T(0);
+          int j = 0;
+          while (j < nvalid && size < K) {  // fill phase (uniform across the warp)
+            const T kj = __shfl_sync(FULL, key, j);
+            if (in_lanes) {
+              if (lane == size) {
+                my_k = kj;
+                my_v = c0 + base + j;
+              }
+            } else if (lane == 0) {
+              slot_k[size] = kj;
+              slot_v[size] = c0 + base + j;
             }
-            __syncwarp();
-            max_key = kl;
-            for (int s = 0; s < K; ++s) {
-              const T c = sk[s];
-              if (c > max_key) {
-                max_key = c;
-                max_idx = s;
+            if (size == 0 || kj > max_key) {
+              max_key = kj;
+              max_idx = size;
+            }
+            ++size;
+            ++j;
+          }
+          __syncwarp();
+          if (j < nvalid) {
+            unsigned cand = __ballot_sync(FULL, lane >= j && lane < nvalid && key < max_key);
+            while (cand) {
+              const int l = __ffs(cand) - 1;
+              cand &= cand - 1;
+              const T kl = __shfl_sync(FULL, key, l);
+              if (!(kl < max_key)) continue;
+              if (in_lanes) {
+                if (lane == max_idx) {
+                  my_k = kl;
+                  my_v = c0 + base + l;
+                }
+                const T v = (lane < K && my_k > kl) ? my_k : T(-INFINITY);
+                const T m = warp_max(v);
+                if (m > kl) {
+                  max_key = m;
+                  max_idx = __ffs(__ballot_sync(FULL, lane < K && v == m)) - 1;
+                } else {
+                  max_key = kl;
+                }
+              } else {
+                if (lane == 0) {
+                  slot_k[max_idx] = kl;
+                  slot_v[max_idx] = c0 + base + l;
+                }
+                __syncwarp();
+                max_key = kl;
+                for (int s2 = 0; s2 < K; ++s2) {
+                  const T c = slot_k[s2];
+                  if (c > max_key) {
+                    max_key = c;
+                    max_idx = s2;
+                  }
+                }
+                __syncwarp();
               }
             }
-            __syncwarp();
           }
         }
       }
+      __syncthreads();
     }
-    if (lane == 0) {
-      for (int x = 0; x < size - 1; ++x)
-        for (int y = 0; y < size - x - 1; ++y)
-          if (sk[y + 1] < sk[y]) {
-            const T tk = sk[y];
-            const int tv = sv[y];
-            sk[y] = sk[y + 1];
-            sv[y] = sv[y + 1];
-            sk[y + 1] = tk;
-            sv[y + 1] = tv;
-          }
+    if (warp == 0) {
+      if (in_lanes && !__any_sync(FULL, lane < K && my_k != my_k)) {
+        int rank = 0;
+        for (int t = 0; t < K; ++t) {
+          const T kt = __shfl_sync(FULL, my_k, t);
+          rank += (kt < my_k || (kt == my_k && t < lane)) ? 1 : 0;
+        }
+        if (lane < K) {
+          slot_k[rank] = my_k;
+          slot_v[rank] = my_v;
+        }
+      } else {
+        if (in_lanes && lane < K) {
+          slot_k[lane] = my_k;
+          slot_v[lane] = my_v;
+        }
+        __syncwarp();
+        if (lane == 0) bubble_sort_slots(slot_k, slot_v, size);
+      }
     }
-    __syncwarp();
-    for (int k = lane; k < K; k += 32) {
+    __syncthreads();
+    for (int k = tid; k < K; k += kReplayThreads) {
       const int64_t e = bq * K + k;
-      a.dists[e] = sk[k];
-      a.idxs[e] = (int64_t)sv[k];
-      a.w_out[e] = weight_of(sk[k]);
+      a.dists[e] = slot_k[k];
+      a.idxs[e] = (int64_t)slot_v[k];
+      a.w_out[e] = weight_of(slot_k[k]);
     }
     const T* fb = a.f + b * (int64_t)P * F;
-    for (int c = lane; c < F; c += 32) {
+    for (int c = tid; c < F; c += kReplayThreads) {
       T acc = T(0);
-      for (int k = 0; k < K; ++k) acc = fma_rn(fb[(int64_t)sv[k] * F + c], weight_of(sk[k]), acc);
+      for (int k = 0; k < K; ++k) acc = fma_rn(fb[(int64_t)slot_v[k] * F + c], weight_of(slot_k[k]), acc);
       a.f_out[bq * F + c] = acc;
     }
-    __syncwarp();
+    __syncthreads();
   }
 }
 
@@ -172,7 +237,7 @@ __global__ void __launch_bounds__(128) mink_exact_kernel(ExactParams<T> a) {
 //
 // CTA = 4 warps.  Each thread owns one query; G warps of the CTA share one
 // 32-query group and split every point tile between them (G = 1, 2, 4), so
-// small query counts still fill the GPU.  Point tiles (256 points, 16 KB, in
+// small query counts still fill the GPU.  Point tiles (128 points, 8 KB, in
 // the pair-interleaved layout) are streamed into shared memory by one-
 // dimensional bulk copies (TMA), double-buffered on two mbarriers; all lanes
 // read the same pair at a time (broadcast), and both keys of a pair come out
@@ -184,19 +249,27 @@ __global__ void __launch_bounds__(128) mink_exact_kernel(ExactParams<T> a) {
 // key is a candidate when key <= tau (the tightest list top known to the
 // group); candidates are appended to a per-thread queue in shared memory and
 // folded into the list when any lane's queue is nearly full and at every
-// tile end, when the G splits also exchange their list tops.
+// tile end, when the G splits also exchange their list tops.  After the
+// first kSeedTiles tiles the G lists of a query are merged once: split 0
+// keeps the exact top-(K+1) of those points and the other splits restart
+// from placeholder entries (index -2) at its (K+1)-th key, so they only
+// accept keys below it and no split refills a list from scratch.
 //
 // Exactness.  The result equals the reference's MinK selection whenever the
 // K+1 smallest keys are pairwise distinct (then the top-K set and its order
-// are unique) and no NaN key falls in MinK's fill phase (points 0..K-1).  A
-// query is flagged for the exact replay kernel when its merged top-(K+1)
-// holds equal keys or an empty slot, when a dropped or evicted key equalled
-// the threshold it was compared with, or when a fill-phase key is NaN.
-// Dropped keys are > a threshold that is itself >= the global (K+1)-th key,
-// so they can tie with nothing that matters.
+// are unique) and no NaN key falls in MinK's fill phase (points 0..K-1).
+// Every key that leaves the lists is either strictly above a threshold that
+// is >= the global (K+1)-th key, or equal to the threshold it was compared
+// with; the smallest such "equal" key is tracked (tie_key).  A query is
+// flagged for the exact replay kernel when its merged top-(K+1) holds equal
+// keys or an empty slot, when tie_key <= its merged (K+1)-th key, or when a
+// fill-phase key is NaN.
+
+constexpr int kSeedTiles = 2;
+constexpr unsigned kTileBytes = (kTilePoints / 2) * kPairFloats * 4;
 
 template <int L>
-__device__ __forceinline__ void list_insert(float (&keys)[L], int (&vals)[L], float k, int i, bool& tie) {
+__device__ __forceinline__ void list_insert(float (&keys)[L], int (&vals)[L], float k, int i, float& tie_key) {
 #pragma unroll
   for (int s = 0; s < L; ++s) {
     const bool lt = k < keys[s];
@@ -209,34 +282,72 @@ __device__ __forceinline__ void list_insert(float (&keys)[L], int (&vals)[L], fl
     k = ek;
     i = ei;
   }
-  // (k, i) was evicted from the top: equal to the new top means a tie.
-  if (i >= 0 && k == keys[L - 1]) tie = true;
+  // (k, i) left the list: if it was a real entry equal to the new top, remember it.
+  if (i >= 0 && k == keys[L - 1]) tie_key = fminf(tie_key, k);
 }
 
 template <int L>
-__device__ __forceinline__ void flush_queue(float (&keys)[L], int (&vals)[L], int& qn, bool& tie, float& tau,
+__device__ __forceinline__ void flush_queue(float (&keys)[L], int (&vals)[L], int& qn, float& tie_key, float& tau,
                                             const float* qk, const int* qv, int tid) {
   for (int e = 0; e < qn; ++e) {
     const float k = qk[e * kSearchThreads + tid];
     const int i = qv[e * kSearchThreads + tid];
     const float top = keys[L - 1];
     if (k < top) {
-      list_insert<L>(keys, vals, k, i, tie);
+      list_insert<L>(keys, vals, k, i, tie_key);
     } else if (k == top) {
-      tie = true;
+      tie_key = fminf(tie_key, k);
     }
   }
   qn = 0;
   tau = fminf(tau, keys[L - 1]);
 }
 
+// Merge the sorted lists of the G splits of query lq (slots [start, L) of
+// each; entries with a negative index count as +inf) and write the `count`
+// smallest to ok/oi.  Returns the next key after them (+inf if none).
+template <int G, int L>
+__device__ __forceinline__ float merge_splits(const float* mk, const int* mv, int qpc, int lq, int start, int count,
+                                              float* ok, int* oi) {
+  int h[G];
+#pragma unroll
+  for (int g = 0; g < G; ++g) h[g] = start;
+  float next = INFINITY;
+  for (int j = 0; j <= count; ++j) {
+    float bk = INFINITY;
+    int bi = -1, bg = -1;
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      if (h[g] < L) {
+        const int v = mv[(g * qpc + lq) * L + h[g]];
+        const float kk = v >= 0 ? mk[(g * qpc + lq) * L + h[g]] : INFINITY;
+        if (bg < 0 || kk < bk) {
+          bk = kk;
+          bi = v;
+          bg = g;
+        }
+      }
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g) h[g] += (g == bg) ? 1 : 0;
+    if (j < count) {
+      ok[j] = bk;
+      oi[j] = bi >= 0 ? bi : -1;
+    } else {
+      next = bk;
+    }
+  }
+  return next;
+}
+
 template <int KMAX, int G>
-__global__ void __launch_bounds__(kSearchThreads) search_f32_kernel(SearchParams a) {
+__global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f32_kernel(SearchParams a) {
   constexpr int L = KMAX + 1;
   constexpr int QPC = 32 * (4 / G);
-  constexpr int PPS = 128 / G;  // pairs per split per tile
+  constexpr int PPT = kTilePoints / 2;  // pairs per tile
+  constexpr int PPS = PPT / G;          // pairs per split per tile
   constexpr size_t RA = search_region_a_bytes(KMAX, G);
-  constexpr uint32_t kTileBytes = 128 * kPairFloats * 4;
+  constexpr size_t kMerge = search_merge_bytes(KMAX, G);
 
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned char* regA = smem;
@@ -244,6 +355,14 @@ __global__ void __launch_bounds__(kSearchThreads) search_f32_kernel(SearchParams
   int* qv = reinterpret_cast<int*>(qk + kQueueCap * kSearchThreads);
   float* tau_share = reinterpret_cast<float*>(qv + kQueueCap * kSearchThreads);  // [2][128]
   uint64_t* full = reinterpret_cast<uint64_t*>(tau_share + 2 * kSearchThreads);
+  // phase-2 views of region A
+  float* mk = reinterpret_cast<float*>(regA);
+  int* mv = reinterpret_cast<int*>(regA + (size_t)kSearchThreads * L * 4);
+  float* mf = reinterpret_cast<float*>(regA + (size_t)kSearchThreads * L * 8);
+  float* out_k = reinterpret_cast<float*>(regA + kMerge);
+  int* out_i = reinterpret_cast<int*>(out_k + QPC * L);
+  float* out_w = reinterpret_cast<float*>(out_i + QPC * L);
+  int* out_f = reinterpret_cast<int*>(out_w + QPC * L);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int split = warp % G, grp = warp / G;
@@ -260,11 +379,11 @@ __global__ void __launch_bounds__(kSearchThreads) search_f32_kernel(SearchParams
 
   // MinK's fill phase stores points 0..K-1 whatever their key: a NaN there
   // changes the result in ways only the replay reproduces.
-  bool tie = false;
+  bool nan_fill = false;
   if (split == 0)
     for (int i = 0; i < K; ++i) {
       const float s = key_rec<float>(qx, qy, qz, recb + (int64_t)i * kRecLen);
-      if (s != s) tie = true;
+      if (s != s) nan_fill = true;
     }
 
   float keys[L];
@@ -274,10 +393,11 @@ __global__ void __launch_bounds__(kSearchThreads) search_f32_kernel(SearchParams
     keys[s] = (s < KMAX - K) ? -INFINITY : INFINITY;
     vals[s] = -1;
   }
-  float tau = INFINITY;
+  float tau = INFINITY, tie_key = INFINITY;
   int qn = 0;
 
   const int ntile = a.P_pad / kTilePoints;
+  const bool seed = G > 1 && ntile > kSeedTiles;
   const float* pairs_b = a.pairs + (int64_t)b * (a.P_pad / 2) * kPairFloats;
   if (tid == 0) {
     mbar_init(&full[0], 1);
@@ -285,12 +405,13 @@ __global__ void __launch_bounds__(kSearchThreads) search_f32_kernel(SearchParams
     fence_mbar_init();
   }
   __syncthreads();
-  if (tid == 0) {
-    for (int t = 0; t < 2 && t < ntile; ++t) {
-      mbar_arrive_expect_tx(&full[t], kTileBytes);
-      bulk_copy_g2s(regA + t * kTileBytes, pairs_b + (int64_t)t * 128 * kPairFloats, kTileBytes, &full[t]);
-    }
-  }
+  auto issue = [&](int t) {
+    const int buf = t & 1;
+    mbar_arrive_expect_tx(&full[buf], kTileBytes);
+    bulk_copy_g2s(regA + buf * kTileBytes, pairs_b + (int64_t)t * PPT * kPairFloats, kTileBytes, &full[buf]);
+  };
+  if (tid == 0)
+    for (int t = 0; t < 2 && t < ntile; ++t) issue(t);
 
   for (int t = 0; t < ntile; ++t) {
     const int buf = t & 1;
@@ -318,43 +439,69 @@ __global__ void __launch_bounds__(kSearchThreads) search_f32_kernel(SearchParams
         qv[qn * kSearchThreads + tid] = ia + 1;
         ++qn;
       }
-      if (__any_sync(0xffffffffu, qn > kQueueCap - 2)) flush_queue<L>(keys, vals, qn, tie, tau, qk, qv, tid);
+      if (__any_sync(0xffffffffu, qn > kQueueCap - 2)) flush_queue<L>(keys, vals, qn, tie_key, tau, qk, qv, tid);
     }
-    flush_queue<L>(keys, vals, qn, tie, tau, qk, qv, tid);
+    flush_queue<L>(keys, vals, qn, tie_key, tau, qk, qv, tid);
     tau_share[buf * kSearchThreads + split * QPC + lq] = keys[L - 1];
     const int abort = __syncthreads_or(!ok);
     if (abort) {
       if (tid == 0) {
         atomicOr(a.status, kStatusWaitTimeout);
         mbar_wait_bounded(&full[buf], (t >> 1) & 1);
-        if (t + 1 < ntile) mbar_wait_bounded(&full[buf ^ 1], ((t + 1) >> 1) & 1);
+        if (t + 1 < ntile && !(seed && t + 1 == kSeedTiles)) mbar_wait_bounded(&full[buf ^ 1], ((t + 1) >> 1) & 1);
       }
       return;
+    }
+    if (seed && t == kSeedTiles - 1) {
+      // Both tile buffers are free (the next copies are deferred until now):
+      // merge the G lists of every query into split 0, restart the others.
+      const int slot = split * QPC + lq;
+#pragma unroll
+      for (int s = 0; s < L; ++s) {
+        mk[slot * L + s] = keys[s];
+        mv[slot * L + s] = vals[s];
+      }
+      __syncthreads();
+      float tau0 = INFINITY;
+      if (split == 0) {
+        const float next = merge_splits<G, L>(mk, mv, QPC, lq, KMAX - K, K + 1, out_k + lq * L, out_i + lq * L);
+        tau0 = out_k[lq * L + K];
+        if (next == tau0) tie_key = fminf(tie_key, next);
+        mf[lq] = tau0;
+      }
+      __syncthreads();
+      tau0 = mf[lq];
+#pragma unroll
+      for (int s = 0; s < L; ++s) {
+        const int j = s - (KMAX - K);
+        if (j >= 0) {
+          keys[s] = split == 0 ? out_k[lq * L + j] : tau0;
+          vals[s] = split == 0 ? out_i[lq * L + j] : -2;
+        }
+      }
+      tau = fminf(tau, tau0);
+      __syncthreads();
+      if (tid == 0)
+        for (int t2 = kSeedTiles; t2 < kSeedTiles + 2 && t2 < ntile; ++t2) {
+          fence_proxy_async_smem();
+          issue(t2);
+        }
+      continue;
     }
     float tm = keys[L - 1];
 #pragma unroll
     for (int g = 0; g < G; ++g) tm = fminf(tm, tau_share[buf * kSearchThreads + g * QPC + lq]);
     tau = fminf(tau, tm);
-    if (tid == 0 && t + 2 < ntile) {
+    const bool deferred = seed && t < kSeedTiles - 1;
+    if (tid == 0 && t + 2 < ntile && !deferred) {
       fence_proxy_async_smem();
-      mbar_arrive_expect_tx(&full[buf], kTileBytes);
-      bulk_copy_g2s(regA + buf * kTileBytes, pairs_b + (int64_t)(t + 2) * 128 * kPairFloats, kTileBytes,
-                    &full[buf]);
+      issue(t + 2);
     }
   }
 
   // ---- merge the G split lists; region A is free (no copy in flight, all
   // tile reads ended before the last barrier).
-  constexpr size_t kMerge = search_merge_bytes(KMAX, G);
-  float* mk = reinterpret_cast<float*>(regA);
-  int* mv = reinterpret_cast<int*>(regA + (size_t)kSearchThreads * L * 4);
-  int* mf = reinterpret_cast<int*>(regA + (size_t)kSearchThreads * L * 8);
-  float* out_k = reinterpret_cast<float*>(regA + kMerge);
-  int* out_i = reinterpret_cast<int*>(out_k + QPC * L);
-  float* out_w = reinterpret_cast<float*>(out_i + QPC * L);
-  int* out_f = reinterpret_cast<int*>(out_w + QPC * L);
-
-  bool fl = tie;
+  float fl_tie = tie_key;
   if (G > 1) {
     const int slot = split * QPC + lq;
 #pragma unroll
@@ -362,34 +509,12 @@ __global__ void __launch_bounds__(kSearchThreads) search_f32_kernel(SearchParams
       mk[slot * L + s] = keys[s];
       mv[slot * L + s] = vals[s];
     }
-    mf[slot] = tie ? 1 : 0;
+    mf[slot] = tie_key;
     __syncthreads();
     if (split == 0) {
-      int h[G];
 #pragma unroll
-      for (int g = 0; g < G; ++g) {
-        h[g] = KMAX - K;
-        fl = fl || (mf[g * QPC + lq] != 0);
-      }
-      for (int j = 0; j <= K; ++j) {
-        float bk = INFINITY;
-        int bi = -1, bg = 0;
-#pragma unroll
-        for (int g = 0; g < G; ++g) {
-          if (h[g] < L) {
-            const float kk = mk[(g * QPC + lq) * L + h[g]];
-            if (bi < 0 && g == 0 || kk < bk) {
-              bk = kk;
-              bi = mv[(g * QPC + lq) * L + h[g]];
-              bg = g;
-            }
-          }
-        }
-#pragma unroll
-        for (int g = 0; g < G; ++g) h[g] += (g == bg) ? 1 : 0;
-        out_k[lq * L + j] = bk;
-        out_i[lq * L + j] = bi;
-      }
+      for (int g = 0; g < G; ++g) fl_tie = fminf(fl_tie, mf[g * QPC + lq]);
+      merge_splits<G, L>(mk, mv, QPC, lq, KMAX - K, K + 1, out_k + lq * L, out_i + lq * L);
     }
   } else {
 #pragma unroll
@@ -403,10 +528,13 @@ __global__ void __launch_bounds__(kSearchThreads) search_f32_kernel(SearchParams
   }
   if (split == 0) {
     const int nneed = (P > K) ? K + 1 : K;
+    bool fl = nan_fill;
     for (int j = 0; j < nneed; ++j)
       if (out_i[lq * L + j] < 0) fl = true;
     for (int j = 0; j + 1 < nneed; ++j)
       if (out_k[lq * L + j] == out_k[lq * L + j + 1]) fl = true;
+    const float m = (P > K) ? out_k[lq * L + K] : INFINITY;
+    if (fl_tie <= m) fl = true;
     for (int j = 0; j < K; ++j) out_w[lq * L + j] = weight_of(out_k[lq * L + j]);
     out_f[lq] = (fl || !valid) ? 1 : 0;
     if (valid && fl) {
@@ -489,7 +617,10 @@ int launch_search_t(const SearchParams& a, cudaStream_t st) {
   }
   constexpr int QPC = 32 * (4 / G);
   dim3 grid((a.Q + QPC - 1) / QPC, a.B);
+  profile_begin(st);
   search_f32_kernel<KMAX, G><<<grid, kSearchThreads, smem, st>>>(a);
+  profile_end(st);
+  note_launches(1);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 
@@ -502,24 +633,27 @@ int launch_search_k(const SearchParams& a, int G, cudaStream_t st) {
 
 template <typename T>
 int launch_exact(const ExactParams<T>& a, cudaStream_t st) {
-  const size_t smem = (size_t)4 * a.K * (sizeof(T) + sizeof(int));
-  if (smem > 48 * 1024) {
-    if (smem > 200 * 1024) return KNNAG_ERR_TOO_LARGE;
-    if (cudaFuncSetAttribute(mink_exact_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
-      return KNNAG_ERR_CUDA;
-  }
+  const size_t smem = (size_t)replay_chunk<T>() * sizeof(T) + (size_t)a.K * (sizeof(T) + sizeof(int));
+  if (smem > 200 * 1024) return KNNAG_ERR_TOO_LARGE;
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(mink_replay_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+          cudaSuccess)
+    return KNNAG_ERR_CUDA;
   int dev = 0;
   cudaGetDevice(&dev);
   int64_t blocks;
   if (a.use_list) {
-    blocks = (int64_t)num_sms(dev) * 8;
+    blocks = (int64_t)num_sms(dev) * 2;  // flagged queries are few; each CTA loops over them
   } else {
-    blocks = ((int64_t)a.B * a.Q + 3) / 4;
-    blocks = blocks < (int64_t)num_sms(dev) * 64 ? blocks : (int64_t)num_sms(dev) * 64;
+    blocks = (int64_t)a.B * a.Q;
+    const int64_t cap = (int64_t)num_sms(dev) * 8;
+    if (blocks > cap) blocks = cap;
   }
   if (blocks < 1) blocks = 1;
-  mink_exact_kernel<T><<<(unsigned)blocks, 128, smem, st>>>(a);
+  if (!a.use_list) profile_begin(st);
+  mink_replay_kernel<T><<<(unsigned)blocks, kReplayThreads, smem, st>>>(a);
+  if (!a.use_list) profile_end(st);
+  note_launches(1);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 
@@ -571,6 +705,7 @@ int launch_pack_points(const void* p, const void* sigma, const void* R, int B, i
   else
     pack_points_kernel<float><<<grid_for(n, 256, dev), 256, 0, st>>>((const float*)p, (const float*)sigma,
                                                                      (const float*)R, n, (float*)rec);
+  note_launches(1);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 
@@ -605,6 +740,7 @@ int forward_impl(const void* q, const void* p, const void* f, const void* sigma,
   float* pairs = reinterpret_cast<float*>(ws + L.pairs);
   pack_pairs_kernel<<<grid_for((int64_t)B * L.P_pad * kRecLen, 256, dev), 256, 0, st>>>(
       (const float*)rec, B, P, L.P_pad, pairs);
+  note_launches(1);
   if (cudaGetLastError() != cudaSuccess) return KNNAG_ERR_CUDA;
   SearchParams sp{};
   sp.q = (const float*)q;

@@ -39,6 +39,9 @@ _SIGS = {
     "knnag_backward": ([_V] * 9 + [_I] * 7 + [_V, _V] + [_V] * 6 + [_V, _S, _V], _I),
     "knnag_backward_2nd": ([_V] * 10 + [_I] * 7 + [_V, _V, _V] + [_V] * 6 + [_V, _S, _V], _I),
     "knnag_read_device_status": ([_V, _V], _I),
+    "knnag_set_profile_events": ([_V, _V], None),
+    "knnag_launch_count": ([], ctypes.c_longlong),
+    "knnag_fp32_peak_probe": ([_V, _I, _I, _V], _I),
 }
 
 _lib = None
@@ -62,7 +65,8 @@ def lib():
 def header_functions():
     """Names of the functions declared in include/knn_aniso.h."""
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:const\s+char\*|int|size_t)\s+(knnag_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:const\s+char\*|int|size_t|void|long\s+long)\s+(knnag_\w+)\s*\(",
+                                 text, re.M)))
 
 
 def _p(t):
@@ -161,3 +165,19 @@ def backward_2nd(ggq, gfo, q, p, f, sigma, R, idxs, w_out=None, needs=NEED_ALL, 
                                     _p(dgfo), _p(dq), _p(dp), _p(df), _p(ds), _p(dR), _p(ws), nb,
                                     _stream(q.device)))
     return dgfo, dq, dp, df, ds, dR
+
+
+def set_profile_events(ev_begin, ev_end):
+    """Record torch.cuda.Event pair around every later forward's search kernel
+    (None, None switches it off).  The events must have been recorded once so
+    their CUDA handles exist."""
+    h = lambda e: ctypes.c_void_p(e.cuda_event) if e is not None else None
+    lib().knnag_set_profile_events(h(ev_begin), h(ev_end))
+
+
+def launch_count():
+    return int(lib().knnag_launch_count())
+
+
+def fp32_peak_probe(out, blocks, iters):
+    _check(lib().knnag_fp32_peak_probe(_p(out), blocks, iters, _stream(out.device)))

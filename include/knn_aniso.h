@@ -155,6 +155,25 @@ int knnag_backward_2nd(const void* grad_grad_q, const void* grad_f_out, const vo
  * host (synchronises `stream`) and clear it; returns KNNAG_OK or KNNAG_ERR_DEVICE. */
 int knnag_read_device_status(void* workspace, void* stream);
 
+/* ---------------------------------------------------------- instrumentation
+ * No reference counterpart (the reference has no timing hooks). */
+
+/* Process-wide: when both are non-NULL (cudaEvent_t), every later
+ * knnag_forward records ev_begin just before and ev_end just after its kNN
+ * search kernel on the call's stream -- as external event nodes when the call
+ * is captured into a CUDA graph -- so the search can be timed inside a larger
+ * step.  Pass NULLs to switch off. */
+void knnag_set_profile_events(void* ev_begin, void* ev_end);
+
+/* Process-wide count of kernels this library has launched so far. */
+long long knnag_launch_count(void);
+
+/* Launch an FFMA-bound kernel (blocks x 256 threads, `iters` iterations of 16
+ * independent FMA chains per thread, 32*iters FLOP per thread) writing one
+ * float per thread to `out`; used to measure the FP32 peak the search kernel
+ * is compared against. */
+int knnag_fp32_peak_probe(float* out, int blocks, int iters, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
