@@ -47,13 +47,11 @@ AdjLayout adj_layout(int B, int Q, int P, int K) {
 
 // ----------------------------------------------------------------- CSR
 
-__global__ void adj_count_kernel(const int64_t* __restrict__ idxs, int64_t n, int64_t qk, int P,
-                                 int* __restrict__ count) {
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t b = e / qk;
+__global__ void adj_count_kernel(const int64_t* __restrict__ idxs, int n, int qk, int P, int* __restrict__ count) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
     const int64_t idx = idxs[e];
     if (idx < 0 || idx >= P) continue;  // not a point index: no row holds it
-    atomicAdd(&count[b * P + idx], 1);
+    atomicAdd(&count[(e / qk) * P + (int)idx], 1);
   }
 }
 
@@ -109,28 +107,55 @@ __global__ void __launch_bounds__(1024) adj_scan_kernel(int* __restrict__ count,
   if (tid == 0) rowptr[n] = carry_s;
 }
 
-__global__ void adj_fill_kernel(const int64_t* __restrict__ idxs, int64_t n, int64_t qk, int P,
-                                const int* __restrict__ rowptr, int* __restrict__ cursor, int* __restrict__ unsorted) {
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+__global__ void adj_fill_kernel(const int64_t* __restrict__ idxs, int n, int qk, int P, const int* __restrict__ rowptr,
+                                int* __restrict__ cursor, int* __restrict__ unsorted) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
     const int64_t idx = idxs[e];
     if (idx < 0 || idx >= P) continue;
-    const int64_t row = (e / qk) * P + idx;
-    const int pos = rowptr[row] + atomicAdd(&cursor[row], 1);
-    unsorted[pos] = (int)e;
+    const int row = (e / qk) * P + (int)idx;
+    unsorted[rowptr[row] + atomicAdd(&cursor[row], 1)] = e;
   }
 }
 
-// Sort every row by entry id: one warp per row; an entry's slot is the
-// number of smaller ids in its row (ids in a row are distinct because a
-// query selects a point at most once; equal ids keep their order).
-__global__ void adj_sort_kernel(const int* __restrict__ rowptr, const int* __restrict__ unsorted, int64_t n_rows,
+// Sort every row by entry id, one warp per row.  Rows of up to 64 entries
+// are bitonic-sorted in registers (two per lane); longer rows place each id
+// at the number of smaller ids in the row (ids in a row are distinct because
+// a query selects a point at most once; equal ids keep their order).
+__global__ void adj_sort_kernel(const int* __restrict__ rowptr, const int* __restrict__ unsorted, int n_rows,
                                 int* __restrict__ entries) {
   const int lane = threadIdx.x & 31;
-  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t r = gw; r < n_rows; r += nw) {
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int r = gw; r < n_rows; r += nw) {
     const int start = rowptr[r];
     const int n = rowptr[r + 1] - start;
+    if (n <= 64) {
+      int x[2];
+      x[0] = lane < n ? unsorted[start + lane] : 0x7fffffff;
+      x[1] = lane + 32 < n ? unsorted[start + lane + 32] : 0x7fffffff;
+#pragma unroll
+      for (int k = 2; k <= 64; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+          if (j == 32) {
+            const int lo = min(x[0], x[1]), hi = max(x[0], x[1]);
+            x[0] = lo;
+            x[1] = hi;
+          } else {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int e = lane + 32 * h;
+              const int o = __shfl_xor_sync(0xffffffffu, x[h], j);
+              const bool up = (e & k) == 0, lower = (e & j) == 0;
+              x[h] = (lower == up) ? min(x[h], o) : max(x[h], o);
+            }
+          }
+        }
+      }
+      if (lane < n) entries[start + lane] = x[0];
+      if (lane + 32 < n) entries[start + lane + 32] = x[1];
+      continue;
+    }
     for (int base = 0; base < n; base += 32) {
       const int i = base + lane;
       const int v = (i < n) ? unsorted[start + i] : 0;
@@ -170,12 +195,12 @@ int launch_build_adjacency(const int64_t* idxs, int B, int Q, int P, int K, void
   int* cursor = reinterpret_cast<int*>(base + L.cursor);
   int* unsorted = reinterpret_cast<int*>(base + L.unsorted);
   int* entries = reinterpret_cast<int*>(base + L.entries);
-  const int64_t n = (int64_t)B * Q * K, rows = (int64_t)B * P, qk = (int64_t)Q * K;
+  const int n = B * Q * K, rows = B * P, qk = Q * K;  // sizes checked < 2^31 by the caller
   if (cudaMemsetAsync(cursor, 0, (size_t)rows * 4, st) != cudaSuccess) return KNNAG_ERR_CUDA;
   adj_count_kernel<<<blocks_for(n, 256), 256, 0, st>>>(idxs, n, qk, P, cursor);
   adj_scan_kernel<<<1, 1024, 0, st>>>(cursor, rows, rowptr);
   adj_fill_kernel<<<blocks_for(n, 256), 256, 0, st>>>(idxs, n, qk, P, rowptr, cursor, unsorted);
-  adj_sort_kernel<<<blocks_for(rows * 32, 256), 256, 0, st>>>(rowptr, unsorted, rows, entries);
+  adj_sort_kernel<<<blocks_for((int64_t)rows * 32, 256), 256, 0, st>>>(rowptr, unsorted, rows, entries);
   note_launches(4);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
@@ -242,137 +267,192 @@ __device__ __forceinline__ void rot_back(const T* r, const T* sg, const T* u, T*
   for (int m = 0; m < 3; ++m) v[m] = sg[0] * u[0] * r[m] + sg[1] * u[1] * r[3 + m] + sg[2] * u[2] * r[6 + m];
 }
 
-// Half-warp (16 lanes) per query: dot products c_k = gfo[q] . f[idx_k] are
-// split over the 16 lanes (128-bit loads when V4) and tree-reduced; the
-// geometry of entry k0+l is done by lane l of the half-warp.
-template <typename T, int ORDER, bool V4>
-__global__ void __launch_bounds__(128) query_side_kernel(QueryParams<T> a) {
-  const int hl = threadIdx.x & 15;
-  const unsigned hmask = (threadIdx.x & 16) ? 0xffff0000u : 0x0000ffffu;
-  const int64_t BQ = (int64_t)a.B * a.Q;
-  const int K = a.K, F = a.F, P = a.P;
-  const bool need_dot = (ORDER == 1) || a.coef_in == nullptr;
-  for (int64_t bq = blockIdx.x * 8 + (threadIdx.x >> 4); bq < BQ; bq += (int64_t)gridDim.x * 8) {
-    const int64_t b = bq / a.Q;
-    const T qx = a.q[bq * 3 + 0], qy = a.q[bq * 3 + 1], qz = a.q[bq * 3 + 2];
-    T g[3] = {T(0), T(0), T(0)};
-    if (ORDER == 2) {
-      g[0] = a.ggq[bq * 3 + 0];
-      g[1] = a.ggq[bq * 3 + 1];
-      g[2] = a.ggq[bq * 3 + 2];
-    }
-    const T* grow = a.gfo + bq * F;
-    const T* fb = a.f + b * (int64_t)P * F;
-    T acc[3] = {T(0), T(0), T(0)};
-    for (int k0 = 0; k0 < K; k0 += 16) {
-      const int nk = min(16, K - k0);
-      T c_own = T(0);
-      if (need_dot) {
-        for (int kk = 0; kk < nk; ++kk) {
-          const int64_t idx = a.idxs[bq * K + k0 + kk];
-          const T* frow = fb + idx * F;
-          T part = T(0);
-          if (idx < 0 || idx >= P) {
-            // not a point index: contributes nothing
-          } else if (V4) {
-            const float4* g4 = reinterpret_cast<const float4*>(grow);
-            const float4* f4 = reinterpret_cast<const float4*>(frow);
-            for (int c = hl; c < (F >> 2); c += 16) {
-              const float4 x = __ldg(g4 + c), y = __ldg(f4 + c);
-              part = fma_rn((T)x.x, (T)y.x, part);
-              part = fma_rn((T)x.y, (T)y.y, part);
-              part = fma_rn((T)x.z, (T)y.z, part);
-              part = fma_rn((T)x.w, (T)y.w, part);
-            }
-          } else {
-            for (int c = hl; c < F; c += 16) part = fma_rn(grow[c], frow[c], part);
-          }
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll
-          for (int o = 8; o > 0; o >>= 1) part += __shfl_xor_sync(hmask, part, o, 16);
-          if (hl == kk) c_own = part;
-        }
-      } else if (hl < nk) {
-        c_own = a.coef_in[bq * K + k0 + hl];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// First-order query side: one warp per query.  For each group of 8
+// neighbours the lanes sweep the feature columns (coalesced rows of f, all
+// 8 rows in flight), then a reduce-scatter leaves c_k = gfo[q] . f[idx_k] of
+// neighbour k0 + (lane >> 2) in lanes 4m..4m+3; the first lane of each quad
+// does that neighbour's geometry.  dq = sum_k -2 c_k w_k v_k.
+template <typename T>
+__global__ void __launch_bounds__(256, 3) query_order1_kernel(QueryParams<T> a) {
+  constexpr int NG = 8;
+  const int lane = threadIdx.x & 31;
+  const int BQ = a.B * a.Q, K = a.K, F = a.F, P = a.P;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int bq = gw; bq < BQ; bq += nw) {
+    const int b = bq / a.Q;
+    const T qx = a.q[(int64_t)bq * 3 + 0], qy = a.q[(int64_t)bq * 3 + 1], qz = a.q[(int64_t)bq * 3 + 2];
+    const T* grow = a.gfo + (int64_t)bq * F;
+    const T* fb = a.f + (int64_t)b * P * F;
+    T acc[3] = {T(0), T(0), T(0)};
+    for (int k0 = 0; k0 < K; k0 += NG) {
+      const int nk = min(NG, K - k0);
+      int ik[NG];  // neighbour point index within the batch, -1 if none
+#pragma unroll
+      for (int kk = 0; kk < NG; ++kk) {
+        const int64_t idx = kk < nk ? a.idxs[(int64_t)bq * K + k0 + kk] : -1;
+        ik[kk] = (idx >= 0 && idx < P) ? (int)idx : -1;
       }
-      T a_own = T(0);
-      const int64_t e_own = bq * K + k0 + hl;
-      const int64_t i_own = (hl < nk) ? a.idxs[e_own] : -1;
-      if (hl < nk && a.coef_out) a.coef_out[e_own] = c_own;
-      if (i_own >= 0 && i_own < P) {
-        const int64_t e = e_own;
-        const T* rec = a.rec + (b * P + i_own) * kRecLen;
-        Geo<T> geo;
-        geometry(qx, qy, qz, rec, geo);
-        const T w = a.w_in ? a.w_in[e] : geo.w;
-        const T* r = rec + kR00;
-        const T sg[3] = {rec[kS0], rec[kS1], rec[kS2]};
-        T v[3];
-        rot_back(r, sg, geo.u, v);
-        if (ORDER == 1) {
+      T part[NG];
+#pragma unroll
+      for (int kk = 0; kk < NG; ++kk) part[kk] = T(0);
+      for (int c = lane; c < F; c += 32) {
+        const T g = grow[c];
+#pragma unroll
+        for (int kk = 0; kk < NG; ++kk)
+          if (ik[kk] >= 0) part[kk] = fma_rn(g, fb[(int64_t)ik[kk] * F + c], part[kk]);
+      }
+      // reduce-scatter: 8 values over 32 lanes -> lane holds value (lane >> 2) & 7
+#pragma unroll
+      for (int h = NG / 2, m = 16; h >= 1; h >>= 1, m >>= 1) {
+        const bool upper = (lane & m) != 0;
+#pragma unroll
+        for (int i = 0; i < h; ++i) {
+          const T send = upper ? part[i] : part[i + h];
+          const T keep = upper ? part[i + h] : part[i];
+          part[i] = keep + __shfl_xor_sync(0xffffffffu, send, m);
+        }
+      }
+      T c_own = part[0] + __shfl_xor_sync(0xffffffffu, part[0], 2);
+      c_own += __shfl_xor_sync(0xffffffffu, c_own, 1);
+      const int m_own = lane >> 2;
+      const int64_t e = (int64_t)bq * K + k0 + m_own;
+      if ((lane & 3) == 0 && m_own < nk) {
+        if (a.coef_out) a.coef_out[e] = c_own;
+        const int64_t idx = a.idxs[e];
+        if (idx >= 0 && idx < P) {
+          const T* rec = a.rec + ((int64_t)b * P + idx) * kRecLen;
+          Geo<T> geo;
+          geometry(qx, qy, qz, rec, geo);
+          const T w = a.w_in ? a.w_in[e] : geo.w;
+          const T sg[3] = {rec[kS0], rec[kS1], rec[kS2]};
+          T v[3];
+          rot_back(rec + kR00, sg, geo.u, v);
           const T t = T(-2) * c_own * w;
 #pragma unroll
-          for (int m = 0; m < 3; ++m) acc[m] += t * v[m];
-        } else {
+          for (int mm = 0; mm < 3; ++mm) acc[mm] += t * v[mm];
+        }
+      }
+    }
+#pragma unroll
+    for (int mm = 0; mm < 3; ++mm) acc[mm] = warp_sum(acc[mm]);
+    if (lane == 0 && a.dq) {
+      a.dq[(int64_t)bq * 3 + 0] = acc[0];
+      a.dq[(int64_t)bq * 3 + 1] = acc[1];
+      a.dq[(int64_t)bq * 3 + 2] = acc[2];
+    }
+  }
+}
+
+// Second-order query side: one warp per query, lane = neighbour.  With
+// g = grad_grad_q[q], A = g . v, r_a = R_a . g, Mg = sum_a sigma_a r_a R_a:
+// dq += 2 c w (2 A v - Mg); optionally dgfo[q] = sum_k (-2 w_k A_k) f[idx_k]
+// accumulated in k order, lanes spanning columns, 8 rows in flight.
+template <typename T>
+__global__ void __launch_bounds__(256) query_order2_kernel(QueryParams<T> a) {
+  const int lane = threadIdx.x & 31;
+  const int BQ = a.B * a.Q, K = a.K, F = a.F, P = a.P;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int bq = gw; bq < BQ; bq += nw) {
+    const int b = bq / a.Q;
+    const T qx = a.q[(int64_t)bq * 3 + 0], qy = a.q[(int64_t)bq * 3 + 1], qz = a.q[(int64_t)bq * 3 + 2];
+    const T g[3] = {a.ggq[(int64_t)bq * 3 + 0], a.ggq[(int64_t)bq * 3 + 1], a.ggq[(int64_t)bq * 3 + 2]};
+    const T* fb = a.f + (int64_t)b * P * F;
+    T acc[3] = {T(0), T(0), T(0)};
+    for (int k0 = 0; k0 < K; k0 += 32) {
+      const int k = k0 + lane;
+      const int64_t e = (int64_t)bq * K + k;
+      T a_own = T(0);
+      int64_t row = -1;
+      if (k < K) {
+        const int64_t idx = a.idxs[e];
+        if (idx >= 0 && idx < P) {
+          row = idx * F;
+          const T* rec = a.rec + ((int64_t)b * P + idx) * kRecLen;
+          Geo<T> geo;
+          geometry(qx, qy, qz, rec, geo);
+          const T w = a.w_in ? a.w_in[e] : geo.w;
+          const T* r = rec + kR00;
+          const T sg[3] = {rec[kS0], rec[kS1], rec[kS2]};
+          T v[3];
+          rot_back(r, sg, geo.u, v);
           const T A = g[0] * v[0] + g[1] * v[1] + g[2] * v[2];
-          T rg[3];
-#pragma unroll
-          for (int s = 0; s < 3; ++s) rg[s] = r[3 * s] * g[0] + r[3 * s + 1] * g[1] + r[3 * s + 2] * g[2];
-          const T cw2 = T(2) * c_own * w;
-#pragma unroll
-          for (int m = 0; m < 3; ++m) {
-            const T mg = sg[0] * rg[0] * r[m] + sg[1] * rg[1] * r[3 + m] + sg[2] * rg[2] * r[6 + m];
-            acc[m] += cw2 * (T(2) * A * v[m] - mg);
-          }
           a_own = T(-2) * w * A;
+          if (a.coef_in) {
+            T rg[3];
+#pragma unroll
+            for (int s2 = 0; s2 < 3; ++s2) rg[s2] = r[3 * s2] * g[0] + r[3 * s2 + 1] * g[1] + r[3 * s2 + 2] * g[2];
+            const T cw2 = T(2) * a.coef_in[e] * w;
+#pragma unroll
+            for (int m = 0; m < 3; ++m) {
+              const T mg = sg[0] * rg[0] * r[m] + sg[1] * rg[1] * r[3 + m] + sg[2] * rg[2] * r[6 + m];
+              acc[m] += cw2 * (T(2) * A * v[m] - mg);
+            }
+          }
         }
       }
-      if (ORDER == 2 && a.dgfo) {
-        T ak[16];
-        int64_t ik[16];
+      if (a.dgfo) {
+        const int nk = min(32, K - k0);
+        T* drow = a.dgfo + (int64_t)bq * F;
+        for (int cb = 0; cb < F; cb += 32) {  // warp-uniform: the shuffles below need every lane
+          const int c = cb + lane;
+          const bool col = c < F;
+          T s = (k0 == 0 || !col) ? T(0) : drow[c];
+          for (int j0 = 0; j0 < nk; j0 += 8) {
+            T val[8], ak[8];
 #pragma unroll
-        for (int kk = 0; kk < 16; ++kk) {
-          ak[kk] = __shfl_sync(hmask, a_own, kk, 16);
-          ik[kk] = (kk < nk) ? a.idxs[bq * K + k0 + kk] : -1;
-          if (ik[kk] >= P) ik[kk] = -1;
-        }
-        T* drow = a.dgfo + bq * F;
-        for (int c = hl; c < F; c += 16) {
-          T s = (k0 == 0) ? T(0) : drow[c];
+            for (int jj = 0; jj < 8; ++jj) {
+              const int src = min(j0 + jj, 31);
+              const int64_t rj = __shfl_sync(0xffffffffu, row, src);
+              ak[jj] = __shfl_sync(0xffffffffu, a_own, src);
+              val[jj] = (col && j0 + jj < nk && rj >= 0) ? fb[rj + c] : T(0);
+            }
 #pragma unroll
-          for (int kk = 0; kk < 16; ++kk)
-            if (kk < nk && ik[kk] >= 0) s = fma_rn(ak[kk], fb[ik[kk] * F + c], s);
-          drow[c] = s;
+            for (int jj = 0; jj < 8; ++jj)
+              if (j0 + jj < nk) s = fma_rn(ak[jj], val[jj], s);
+          }
+          if (col) drow[c] = s;
         }
       }
     }
+    if (a.dq) {
 #pragma unroll
-    for (int m = 0; m < 3; ++m) {
-#pragma unroll
-      for (int o = 8; o > 0; o >>= 1) acc[m] += __shfl_xor_sync(hmask, acc[m], o, 16);
-    }
-    if (hl == 0 && a.dq) {
-      a.dq[bq * 3 + 0] = acc[0];
-      a.dq[bq * 3 + 1] = acc[1];
-      a.dq[bq * 3 + 2] = acc[2];
+      for (int m = 0; m < 3; ++m) acc[m] = warp_sum(acc[m]);
+      if (lane == 0) {
+        a.dq[(int64_t)bq * 3 + 0] = acc[0];
+        a.dq[(int64_t)bq * 3 + 1] = acc[1];
+        a.dq[(int64_t)bq * 3 + 2] = acc[2];
+      }
     }
   }
 }
 
 // One warp per point row.  Lane j takes entry j of each 32-entry chunk of
 // the row for the per-entry geometry (15 point-side scalars, reduced over
-// the warp at the end); for df the warp then walks the chunk entry by entry
-// with lanes spanning feature columns (NCOL per lane, coalesced gfo rows).
+// the warp at the end); for df the warp then walks the chunk four entries at
+// a time with lanes spanning feature columns (NCOL per lane, coalesced gfo
+// rows, four rows in flight).  The entry order of a row is fixed (sorted),
+// so every sum has a fixed order.
 template <typename T, int ORDER, int NCOL>
-__global__ void __launch_bounds__(256) point_side_kernel(PointParams<T> a) {
+__global__ void __launch_bounds__(256, 4) point_side_kernel(PointParams<T> a) {
   const int lane = threadIdx.x & 31;
-  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int64_t rows = (int64_t)a.B * a.P;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int rows = a.B * a.P;
   const int F = a.F, K = a.K;
+  const int n_entries = a.B * a.Q * K;
   const bool want_geo = (a.needs & (KNNAG_NEED_DP | KNNAG_NEED_DSIGMA | KNNAG_NEED_DR)) != 0;
   const bool want_df = (a.needs & KNNAG_NEED_DF) != 0;
-  for (int64_t row = gw; row < rows; row += nw) {
-    const T* rec = a.rec + row * kRecLen;
+  for (int row = gw; row < rows; row += nw) {
+    const T* rec = a.rec + (int64_t)row * kRecLen;
     T pr[kRecLen];
 #pragma unroll
     for (int m = 0; m < kRecLen; ++m) pr[m] = rec[m];
@@ -388,13 +468,13 @@ __global__ void __launch_bounds__(256) point_side_kernel(PointParams<T> a) {
       for (int u = 0; u < NCOL; ++u) acc[u] = T(0);
       for (int base = start; base < end; base += 32) {
         const int j = base + lane;
-        int64_t e = (j < end) ? (int64_t)a.entries[j] : -1;
-        const bool valid = e >= 0 && e < (int64_t)a.B * a.Q * K;
+        int e = (j < end) ? a.entries[j] : -1;
+        const bool valid = e >= 0 && e < n_entries;
         if (!valid) e = 0;
-        const int64_t bq = e / K;
+        const int bq = e / K;
         T wgt = T(0);
         if (valid) {
-          const T qx = a.q[bq * 3 + 0], qy = a.q[bq * 3 + 1], qz = a.q[bq * 3 + 2];
+          const T qx = a.q[(int64_t)bq * 3 + 0], qy = a.q[(int64_t)bq * 3 + 1], qz = a.q[(int64_t)bq * 3 + 2];
           Geo<T> geo;
           geometry(qx, qy, qz, pr, geo);
           const T w = a.w_in ? a.w_in[e] : geo.w;
@@ -408,21 +488,21 @@ __global__ void __launch_bounds__(256) point_side_kernel(PointParams<T> a) {
 #pragma unroll
               for (int m = 0; m < 3; ++m) gp[m] += T(2) * cw * v[m];
 #pragma unroll
-              for (int s = 0; s < 3; ++s) {
-                gs[s] -= cw * geo.u[s] * geo.u[s];
-                const T t = T(-2) * cw * sg[s] * geo.u[s];
+              for (int s2 = 0; s2 < 3; ++s2) {
+                gs[s2] -= cw * geo.u[s2] * geo.u[s2];
+                const T t = T(-2) * cw * sg[s2] * geo.u[s2];
 #pragma unroll
-                for (int m = 0; m < 3; ++m) gR[3 * s + m] += t * geo.d[m];
+                for (int m = 0; m < 3; ++m) gR[3 * s2 + m] += t * geo.d[m];
               }
             }
           } else {
-            const T g[3] = {a.ggq[bq * 3 + 0], a.ggq[bq * 3 + 1], a.ggq[bq * 3 + 2]};
+            const T g[3] = {a.ggq[(int64_t)bq * 3 + 0], a.ggq[(int64_t)bq * 3 + 1], a.ggq[(int64_t)bq * 3 + 2]};
             const T A = g[0] * v[0] + g[1] * v[1] + g[2] * v[2];
             wgt = T(-2) * w * A;
             if (want_geo && c0 == 0) {
               T rg[3];
 #pragma unroll
-              for (int s = 0; s < 3; ++s) rg[s] = r[3 * s] * g[0] + r[3 * s + 1] * g[1] + r[3 * s + 2] * g[2];
+              for (int s2 = 0; s2 < 3; ++s2) rg[s2] = r[3 * s2] * g[0] + r[3 * s2 + 1] * g[1] + r[3 * s2 + 2] * g[2];
               const T cw = c * w;
 #pragma unroll
               for (int m = 0; m < 3; ++m) {
@@ -430,35 +510,45 @@ __global__ void __launch_bounds__(256) point_side_kernel(PointParams<T> a) {
                 gp[m] -= T(2) * cw * (T(2) * A * v[m] - mg);
               }
 #pragma unroll
-              for (int s = 0; s < 3; ++s) {
-                gs[s] += T(2) * cw * geo.u[s] * (geo.u[s] * A - rg[s]);
-                const T t = T(-2) * cw * sg[s];
+              for (int s2 = 0; s2 < 3; ++s2) {
+                gs[s2] += T(2) * cw * geo.u[s2] * (geo.u[s2] * A - rg[s2]);
+                const T t = T(-2) * cw * sg[s2];
 #pragma unroll
                 for (int m = 0; m < 3; ++m)
-                  gR[3 * s + m] += t * (T(-2) * geo.u[s] * geo.d[m] * A + geo.d[m] * rg[s] + geo.u[s] * g[m]);
+                  gR[3 * s2 + m] += t * (T(-2) * geo.u[s2] * geo.d[m] * A + geo.d[m] * rg[s2] + geo.u[s2] * g[m]);
               }
             }
           }
         }
         if (want_df) {
           const int nvalid = min(32, end - base);
-          for (int jj = 0; jj < nvalid; ++jj) {
-            const int64_t bqj = __shfl_sync(0xffffffffu, bq, jj);
-            const T wj = __shfl_sync(0xffffffffu, wgt, jj);
-            const T* grow = a.gfo + bqj * F;
+          for (int j0 = 0; j0 < nvalid; j0 += 4) {
+            T val[4][NCOL], wj[4];
 #pragma unroll
-            for (int u = 0; u < NCOL; ++u) {
-              const int c = c0 + lane + 32 * u;
-              if (c < F) acc[u] = fma_rn(wj, grow[c], acc[u]);
+            for (int jj = 0; jj < 4; ++jj) {
+              const int src = min(j0 + jj, 31);
+              const int bqj = __shfl_sync(0xffffffffu, bq, src);
+              wj[jj] = (j0 + jj < nvalid) ? __shfl_sync(0xffffffffu, wgt, src) : T(0);
+              const T* grow = a.gfo + (int64_t)bqj * F;
+#pragma unroll
+              for (int u = 0; u < NCOL; ++u) {
+                const int cc = c0 + lane + 32 * u;
+                val[jj][u] = (cc < F) ? grow[cc] : T(0);
+              }
             }
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+              for (int u = 0; u < NCOL; ++u)
+                if (j0 + jj < nvalid) acc[u] = fma_rn(wj[jj], val[jj][u], acc[u]);
           }
         }
       }
       if (want_df) {
 #pragma unroll
         for (int u = 0; u < NCOL; ++u) {
-          const int c = c0 + lane + 32 * u;
-          if (c < F) a.df[row * F + c] = acc[u];
+          const int cc = c0 + lane + 32 * u;
+          if (cc < F) a.df[(int64_t)row * F + cc] = acc[u];
         }
       }
     }
@@ -472,17 +562,14 @@ __global__ void __launch_bounds__(256) point_side_kernel(PointParams<T> a) {
 #pragma unroll
       for (int m = 0; m < 9; ++m) vals[6 + m] = gR[m];
 #pragma unroll
-      for (int m = 0; m < 15; ++m) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) vals[m] += __shfl_xor_sync(0xffffffffu, vals[m], o);
-      }
+      for (int m = 0; m < 15; ++m) vals[m] = warp_sum(vals[m]);
       if (lane == 0) {
         if (a.needs & KNNAG_NEED_DP)
-          for (int m = 0; m < 3; ++m) a.dp[row * 3 + m] = vals[m];
+          for (int m = 0; m < 3; ++m) a.dp[(int64_t)row * 3 + m] = vals[m];
         if (a.needs & KNNAG_NEED_DSIGMA)
-          for (int m = 0; m < 3; ++m) a.dsigma[row * 3 + m] = vals[3 + m];
+          for (int m = 0; m < 3; ++m) a.dsigma[(int64_t)row * 3 + m] = vals[3 + m];
         if (a.needs & KNNAG_NEED_DR)
-          for (int m = 0; m < 9; ++m) a.dR[row * 9 + m] = vals[6 + m];
+          for (int m = 0; m < 9; ++m) a.dR[(int64_t)row * 9 + m] = vals[6 + m];
       }
     }
   }
@@ -509,20 +596,13 @@ BwdLayout bwd_layout(int B, int Q, int P, int F, int K, int dtype) {
 namespace {
 
 template <typename T>
-int launch_query(const QueryParams<T>& p, int order, bool v4, cudaStream_t st) {
-  const int64_t bq = (int64_t)p.B * p.Q;
-  const unsigned grid = blocks_for(bq * 16, 128);
-  if (order == 1) {
-    if (v4)
-      query_side_kernel<T, 1, true><<<grid, 128, 0, st>>>(p);
-    else
-      query_side_kernel<T, 1, false><<<grid, 128, 0, st>>>(p);
-  } else {
-    if (v4)
-      query_side_kernel<T, 2, true><<<grid, 128, 0, st>>>(p);
-    else
-      query_side_kernel<T, 2, false><<<grid, 128, 0, st>>>(p);
-  }
+int launch_query(const QueryParams<T>& p, int order, cudaStream_t st) {
+  const int64_t warps = (int64_t)p.B * p.Q;
+  const unsigned grid = blocks_for(warps * 32, 256);
+  if (order == 1)
+    query_order1_kernel<T><<<grid, 256, 0, st>>>(p);
+  else
+    query_order2_kernel<T><<<grid, 256, 0, st>>>(p);
   note_launches(1);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
@@ -557,7 +637,6 @@ int backward_t(const BwdArgs& x, cudaStream_t st) {
   }
   const int point_bits = KNNAG_NEED_DP | KNNAG_NEED_DF | KNNAG_NEED_DSIGMA | KNNAG_NEED_DR;
   const int geo_bits = KNNAG_NEED_DP | KNNAG_NEED_DSIGMA | KNNAG_NEED_DR;
-  const bool v4 = sizeof(T) == 4 && x.F % 4 == 0 && (uintptr_t)x.gfo % 16 == 0 && (uintptr_t)x.f % 16 == 0;
 
   const T* coef = static_cast<const T*>(x.coef_in);
   const bool need_coef = (x.order == 1) ? (x.needs & geo_bits) != 0
@@ -584,7 +663,7 @@ int backward_t(const BwdArgs& x, cudaStream_t st) {
     if ((x.needs & KNNAG_NEED_DQ) || cdst) {
       qp.dq = (x.needs & KNNAG_NEED_DQ) ? (T*)x.dq : nullptr;
       qp.coef_out = cdst;
-      rc = launch_query<T>(qp, 1, v4, st);
+      rc = launch_query<T>(qp, 1, st);
       if (rc) return rc;
     }
     coef = cdst;
@@ -593,7 +672,7 @@ int backward_t(const BwdArgs& x, cudaStream_t st) {
       QueryParams<T> cp = qp;
       cp.dq = nullptr;
       cp.coef_out = coef_ws;
-      rc = launch_query<T>(cp, 1, v4, st);
+      rc = launch_query<T>(cp, 1, st);
       if (rc) return rc;
       coef = coef_ws;
     }
@@ -601,7 +680,7 @@ int backward_t(const BwdArgs& x, cudaStream_t st) {
       qp.coef_in = coef;
       qp.dq = (x.needs & KNNAG_NEED_DQ) ? (T*)x.dq : nullptr;
       qp.dgfo = (x.needs & KNNAG_NEED_DGFO) ? (T*)x.dgfo : nullptr;
-      rc = launch_query<T>(qp, 2, v4, st);
+      rc = launch_query<T>(qp, 2, st);
       if (rc) return rc;
     }
   }
