@@ -45,7 +45,8 @@ typedef enum {
   KNNAG_ERR_WORKSPACE = 4,  /* workspace smaller than the *_bytes() query */
   KNNAG_ERR_TOO_LARGE = 5,  /* B*Q*K or B*P exceeds the 32-bit index range */
   KNNAG_ERR_CUDA = 6,       /* a launch failed (cudaGetLastError) */
-  KNNAG_ERR_DEVICE = 7      /* latched on the device: a bounded wait gave up */
+  KNNAG_ERR_DEVICE = 7,     /* latched on the device: a bounded wait gave up */
+  KNNAG_ERR_SCRATCH_LIMIT = 8 /* needs more than knnag_forward_noalloc's fixed scratch */
 } knnag_status;
 
 enum { KNNAG_F32 = 0, KNNAG_F64 = 1 };
@@ -87,6 +88,22 @@ int knnag_forward(const void* q, const void* p, const void* f, const void* sigma
                   int B, int Q, int P, int F, int K, int dtype,
                   void* f_out, void* w_out, void* dists, int64_t* idxs,
                   void* points, void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Same result as knnag_forward, for callers that cannot allocate device
+ * memory (allocator-free sections of a serving loop, plugins whose host
+ * framework owns every device allocation): no workspace argument, no
+ * allocation.  The scratch is one fixed 8 MiB device array inside the
+ * library, held by every GPU that loads it until process exit; sizes whose
+ * scratch would exceed it return KNNAG_ERR_SCRATCH_LIMIT (about B*P <= 60k
+ * points and B*Q <= 500k queries).  The first call on each device looks the
+ * array's address up (cudaGetSymbolAddress) and should come before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race.  No counterpart in the reference.
+ */
+int knnag_forward_noalloc(const void* q, const void* p, const void* f, const void* sigma, const void* R,
+                          int B, int Q, int P, int F, int K, int dtype,
+                          void* f_out, void* w_out, void* dists, int64_t* idxs, void* stream);
 
 /* ---------------------------------------------------------- adjoint index */
 

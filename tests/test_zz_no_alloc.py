@@ -1,0 +1,83 @@
+"""knnag_forward_noalloc: the forward for callers that cannot allocate device
+memory (allocator-free serving sections, plugins whose host framework owns
+all device allocations).  Its scratch is a fixed array inside the library,
+so it must give the same results as knnag_forward -- on consecutive calls,
+whatever the previous call left in that shared array.
+
+Tolerances as in the other parity tests: idxs and dists exact, w_out and
+f_out within 1e-5 relative to the tensor's max.  The file name sorts last so
+a run that stops at the first failure has run every other test first.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_err
+
+FWD_TOL = 1e-5
+
+
+def lib_and_capi():
+    from cuda_knn_aggregate import capi
+
+    L = capi.lib()
+    V, I = ctypes.c_void_p, ctypes.c_int
+    fn = L.knnag_forward_noalloc
+    fn.argtypes = [V] * 5 + [I] * 6 + [V] * 4 + [V]
+    fn.restype = I
+    return fn, capi
+
+
+def run_noalloc(fn, capi, q, p, f, sigma, R, K):
+    B, Q, P, F = q.shape[0], q.shape[1], p.shape[1], f.shape[2]
+    o = dict(dtype=q.dtype, device=q.device)
+    f_out, w_out, dists = torch.empty(B, Q, F, **o), torch.empty(B, Q, K, **o), torch.empty(B, Q, K, **o)
+    idxs = torch.empty(B, Q, K, dtype=torch.int64, device=q.device)
+    rc = fn(*[capi._p(t) for t in (q, p, f, sigma, R)], B, Q, P, F, K, capi._dtype(q),
+            *[capi._p(t) for t in (f_out, w_out, dists, idxs)], capi._stream(q.device))
+    assert rc == 0, capi.lib().knnag_status_string(rc).decode()
+    return f_out, w_out, dists, idxs
+
+
+def assert_same(a, b):
+    f0, w0, d0, i0 = [x.cpu().numpy() for x in a]
+    f1, w1, d1, i1 = [x.cpu().numpy() for x in b]
+    assert np.array_equal(i0, i1)
+    assert np.array_equal(d0.view(np.int32), d1.view(np.int32))
+    assert rel_err(w0, w1) < FWD_TOL
+    assert rel_err(f0, f1) < FWD_TOL
+
+
+@pytest.mark.gpu
+def test_noalloc_matches_forward_on_consecutive_calls():
+    from cuda_knn_aggregate import workloads as W
+
+    fn, capi = lib_and_capi()
+    dev = torch.device("cuda:0")
+    # two different problems back to back: the second call must not see the
+    # first one's leftovers in the shared scratch
+    cases = [W.make("small", B=2, Q=1000, P=500, F=32, K=12, seed=31),
+             W.make("small", B=1, Q=700, P=2300, F=20, K=16, seed=32)]
+    for shape, t in cases + cases:
+        x = [a.to(dev) for a in t]
+        got = run_noalloc(fn, capi, *x, shape.K)
+        want = capi.forward(*x, shape.K)
+        torch.cuda.synchronize()
+        assert_same(got, want)
+
+
+@pytest.mark.gpu
+def test_noalloc_rejects_sizes_beyond_its_scratch():
+    fn, capi = lib_and_capi()
+    dev = torch.device("cuda:0")
+    B, Q, P, F, K = 1, 4, 1 << 20, 4, 8  # records alone would need 64 MiB
+    q = torch.zeros(B, Q, 3, device=dev)
+    small = torch.zeros(16, device=dev)  # never read: the size check comes first
+    ptr = capi._p(small)
+    out = torch.zeros(64, device=dev)
+    rc = fn(capi._p(q), ptr, ptr, ptr, ptr, B, Q, P, F, K, 0, capi._p(out), capi._p(out), capi._p(out),
+            capi._p(out), capi._stream(dev))
+    assert rc == 8
+    assert b"scratch" in capi.lib().knnag_status_string(rc)
