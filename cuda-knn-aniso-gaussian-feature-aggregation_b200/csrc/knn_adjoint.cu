@@ -188,6 +188,12 @@ inline unsigned blocks_for(int64_t n, int threads) {
 }
 }  // namespace
 
+int launch_exclusive_scan(int* count, int n, int* out, cudaStream_t st) {
+  adj_scan_kernel<<<1, 1024, 0, st>>>(count, n, out);
+  note_launches(1);
+  return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
+}
+
 int launch_build_adjacency(const int64_t* idxs, int B, int Q, int P, int K, void* adjacency, cudaStream_t st) {
   const AdjLayout L = adj_layout(B, Q, P, K);
   char* base = static_cast<char*>(adjacency);

@@ -25,6 +25,9 @@ struct ExactParams {
 
 struct SearchParams {
   const float* q;
+  const int* perm_q;   // sorted position -> query index, per batch element
+  const float* tinfo;  // per tile: box (6), key lower-bound factor mu, pad
+  int ntile;
   const float* pairs;  // pair-interleaved tiles [B][P_pad/2][32]
   const float* rec;    // per-point records [B*P*16]
   const float* f;
@@ -64,14 +67,32 @@ __host__ __device__ inline constexpr size_t search_region_b_bytes() {
 __host__ __device__ inline constexpr size_t search_smem_bytes(int kmax, int g) {
   return search_region_a_bytes(kmax, g) + search_region_b_bytes();
 }
+// Tiles per batch element rounded up to a power of two (the visit-order sort).
+__host__ __device__ inline int search_tiles_pow2(int ntile) {
+  int n = 1;
+  while (n < ntile) n <<= 1;
+  return n;
+}
+// Region C: tile bounds + order [NTP x 8 B], original query index [QPC],
+// query boxes [4 x 6 floats], visit counter.
+__host__ __device__ inline size_t search_region_c_bytes(int ntile, int g) {
+  return (size_t)search_tiles_pow2(ntile) * 8 + (size_t)32 * (4 / g) * 4 + 24 * 4 + 16;
+}
 
 // ------------------------------------------------------------- workspace
 // Forward workspace: [status, flag_count] | flag_list [B*Q] | records (when
 // the caller passed no points buffer) | pair tiles (FP32 fast path).
 struct FwdLayout {
   size_t status, flag_list, rec, pairs, total;
-  int P_pad;
+  // spatial index (FP32 search path): bounds [B*8], cell counts / offsets
+  // [B*cells(+1)], point and query permutations, tile boxes [B*ntile*8]
+  size_t bounds, cell_count, cell_offset, perm_p, perm_q, tinfo;
+  int P_pad, bits;
 };
+int spatial_bits(int P);
+int launch_spatial_index(const float* q, const float* rec, int B, int Q, int P, int P_pad, char* ws, const FwdLayout& L,
+                         cudaStream_t st);
+int launch_exclusive_scan(int* count, int n, int* out, cudaStream_t st);
 FwdLayout fwd_layout(int B, int Q, int P, int K, int dtype, bool own_rec);
 
 // Adjacency (CSR) layout: rowptr [B*P+1] | cursor [B*P] | unsorted [N] | entries [N].

@@ -34,30 +34,6 @@ __global__ void pack_points_kernel(const T* __restrict__ p, const T* __restrict_
   }
 }
 
-// Pair-interleaved FP32 tiles: pairs[((b*P_pad/2 + m)*16 + field)*2 + half]
-// holds field `field` of point 2m+half.  Points beyond P are padding whose
-// sigma is NaN, so their key is NaN and never selected.
-__global__ void pack_pairs_kernel(const float* __restrict__ rec, int B, int P, int P_pad,
-                                  float* __restrict__ pairs) {
-  const int64_t total = (int64_t)B * P_pad * kRecLen;
-  for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < total;
-       o += (int64_t)gridDim.x * blockDim.x) {
-    const int half = (int)(o & 1);
-    const int field = (int)((o >> 1) & (kRecLen - 1));
-    const int64_t pair = o >> 5;  // 32 floats per pair
-    const int64_t b = pair / (P_pad / 2);
-    const int64_t m = pair - b * (P_pad / 2);
-    const int64_t i = 2 * m + half;
-    float v;
-    if (i < P) {
-      v = rec[(b * P + i) * kRecLen + field];
-    } else {
-      v = (field == kS0 || field == kS1 || field == kS2) ? __int_as_float(0x7fc00000) : 0.0f;
-    }
-    pairs[o] = v;
-  }
-}
-
 // ------------------------------------------------------------ exact MinK
 //
 // One CTA per query.  All threads compute the query's keys (same arithmetic
@@ -347,6 +323,7 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
   constexpr int PPT = kTilePoints / 2;  // pairs per tile
   constexpr int PPS = PPT / G;          // pairs per split per tile
   constexpr size_t RA = search_region_a_bytes(KMAX, G);
+  constexpr size_t RB = search_region_b_bytes();
   constexpr size_t kMerge = search_merge_bytes(KMAX, G);
 
   extern __shared__ __align__(128) unsigned char smem[];
@@ -355,6 +332,13 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
   int* qv = reinterpret_cast<int*>(qk + kQueueCap * kSearchThreads);
   float* tau_share = reinterpret_cast<float*>(qv + kQueueCap * kSearchThreads);  // [2][128]
   uint64_t* full = reinterpret_cast<uint64_t*>(tau_share + 2 * kSearchThreads);
+  // region C: per-tile lower bounds (sorted), visit order, query bookkeeping
+  const int NTP = search_tiles_pow2(a.ntile);
+  float* lbk = reinterpret_cast<float*>(smem + RA + RB);
+  int* lbt = reinterpret_cast<int*>(lbk + NTP);
+  int* qorig = lbt + NTP;                                    // [QPC] original query index (-1: none)
+  float* qbox = reinterpret_cast<float*>(qorig + QPC);       // [4 warps][6]
+  volatile int* s_nvisit = reinterpret_cast<volatile int*>(qbox + 24);
   // phase-2 views of region A
   float* mk = reinterpret_cast<float*>(regA);
   int* mv = reinterpret_cast<int*>(regA + (size_t)kSearchThreads * L * 4);
@@ -368,14 +352,16 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
   const int split = warp % G, grp = warp / G;
   const int lq = grp * 32 + lane;
   const int b = blockIdx.y;
-  const int qi = blockIdx.x * QPC + lq;
-  const bool valid = qi < a.Q;
-  const int64_t bq = (int64_t)b * a.Q + (valid ? qi : 0);
+  const int sp = blockIdx.x * QPC + lq;  // position in the spatial order
+  const bool valid = sp < a.Q;
+  const int qi = a.perm_q[(int64_t)b * a.Q + (valid ? sp : a.Q - 1)];
+  const int64_t bq = (int64_t)b * a.Q + qi;
   const int K = a.K, P = a.P;
 
   const float qx = a.q[bq * 3 + 0], qy = a.q[bq * 3 + 1], qz = a.q[bq * 3 + 2];
   const float2 qx2 = make_float2(qx, qx), qy2 = make_float2(qy, qy), qz2 = make_float2(qz, qz);
   const float* recb = a.rec + (int64_t)b * P * kRecLen;
+  if (split == 0) qorig[lq] = valid ? qi : -1;
 
   // MinK's fill phase stores points 0..K-1 whatever their key: a NaN there
   // changes the result in ways only the replay reproduces.
@@ -385,6 +371,67 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
       const float s = key_rec<float>(qx, qy, qz, recb + (int64_t)i * kRecLen);
       if (s != s) nan_fill = true;
     }
+
+  // ---- box of this CTA's queries and the tile visit order
+  {
+    float bx[6] = {qx, qy, qz, qx, qy, qz};
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        bx[c] = fminf(bx[c], __shfl_xor_sync(0xffffffffu, bx[c], o));
+        bx[3 + c] = fmaxf(bx[3 + c], __shfl_xor_sync(0xffffffffu, bx[3 + c], o));
+      }
+    }
+    if (lane == 0)
+#pragma unroll
+      for (int c = 0; c < 6; ++c) qbox[warp * 6 + c] = bx[c];
+  }
+  __syncthreads();
+  float bmin[3], bmax[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    bmin[c] = fminf(fminf(qbox[c], qbox[6 + c]), fminf(qbox[12 + c], qbox[18 + c]));
+    bmax[c] = fmaxf(fmaxf(qbox[3 + c], qbox[9 + c]), fmaxf(qbox[15 + c], qbox[21 + c]));
+  }
+  const float* tinfo_b = a.tinfo + (int64_t)b * a.ntile * 8;
+  for (int t = tid; t < NTP; t += kSearchThreads) {
+    float lb = INFINITY;
+    if (t < a.ntile) {
+      const float* ti = tinfo_b + t * 8;
+      float d2 = 0.f;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float g = fmaxf(fmaxf(ti[c] - bmax[c], bmin[c] - ti[3 + c]), 0.f);
+        d2 = __fmaf_rn(g, g, d2);
+      }
+      lb = ti[6] * d2 * 0.99999f;
+      if (!(lb >= 0.f)) lb = 0.f;  // NaN or negative: no bound
+      lb = fminf(lb, 3.4e38f);     // real tiles sort before the +inf padding entries
+    }
+    lbk[t] = lb;
+    lbt[t] = t;
+  }
+  __syncthreads();
+  for (int kk = 2; kk <= NTP; kk <<= 1) {  // bitonic sort of (bound, tile) ascending
+    for (int j = kk >> 1; j > 0; j >>= 1) {
+      for (int i = tid; i < NTP; i += kSearchThreads) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const bool up = (i & kk) == 0;
+          const float ki = lbk[i], kj = lbk[ixj];
+          if ((ki > kj) == up) {
+            lbk[i] = kj;
+            lbk[ixj] = ki;
+            const int ti = lbt[i];
+            lbt[i] = lbt[ixj];
+            lbt[ixj] = ti;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
 
   float keys[L];
   int vals[L];
@@ -396,7 +443,7 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
   float tau = INFINITY, tie_key = INFINITY;
   int qn = 0;
 
-  const int ntile = a.P_pad / kTilePoints;
+  const int ntile = a.ntile;
   const bool seed = G > 1 && ntile > kSeedTiles;
   const float* pairs_b = a.pairs + (int64_t)b * (a.P_pad / 2) * kPairFloats;
   if (tid == 0) {
@@ -405,19 +452,32 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
     fence_mbar_init();
   }
   __syncthreads();
-  auto issue = [&](int t) {
-    const int buf = t & 1;
+  // visit position v reads tile lbt[v] into buffer v & 1
+  auto issue = [&](int v) {
+    const int buf = v & 1;
     mbar_arrive_expect_tx(&full[buf], kTileBytes);
-    bulk_copy_g2s(regA + buf * kTileBytes, pairs_b + (int64_t)t * PPT * kPairFloats, kTileBytes, &full[buf]);
+    bulk_copy_g2s(regA + buf * kTileBytes, pairs_b + (int64_t)lbt[v] * PPT * kPairFloats, kTileBytes, &full[buf]);
   };
-  if (tid == 0)
-    for (int t = 0; t < 2 && t < ntile; ++t) issue(t);
+  // thread 0 only: issue position v unless its bound exceeds every threshold
+  // (the order is ascending, so nothing after it is needed either)
+  auto decide = [&](int v, float tmax) {
+    if (v < ntile && *s_nvisit == v && lbt[v] < ntile && !(lbk[v] > tmax)) {
+      *s_nvisit = v + 1;
+      return true;
+    }
+    return false;
+  };
+  if (tid == 0) {
+    *s_nvisit = 0;
+    for (int v = 0; v < 2; ++v)
+      if (decide(v, INFINITY)) issue(v);
+  }
+  __syncthreads();
 
-  for (int t = 0; t < ntile; ++t) {
+  for (int t = 0; t < *s_nvisit; ++t) {
     const int buf = t & 1;
     const bool ok = mbar_wait_bounded(&full[buf], (t >> 1) & 1);
     const float4* tp = reinterpret_cast<const float4*>(regA + buf * kTileBytes) + split * PPS * 8;
-    const int ibase = t * kTilePoints + split * PPS * 2;
 #pragma unroll 2
     for (int m = 0; m < PPS; ++m) {
       float2 pr[16];
@@ -428,15 +488,14 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
         pr[2 * u + 1] = make_float2(v.z, v.w);
       }
       const float2 s2 = key_pair(qx2, qy2, qz2, pr);
-      const int ia = ibase + 2 * m;
       if (s2.x <= tau) {
         qk[qn * kSearchThreads + tid] = s2.x;
-        qv[qn * kSearchThreads + tid] = ia;
+        qv[qn * kSearchThreads + tid] = __float_as_int(pr[kRecPad].x);
         ++qn;
       }
       if (s2.y <= tau) {
         qk[qn * kSearchThreads + tid] = s2.y;
-        qv[qn * kSearchThreads + tid] = ia + 1;
+        qv[qn * kSearchThreads + tid] = __float_as_int(pr[kRecPad].y);
         ++qn;
       }
       if (__any_sync(0xffffffffu, qn > kQueueCap - 2)) flush_queue<L>(keys, vals, qn, tie_key, tau, qk, qv, tid);
@@ -448,7 +507,7 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
       if (tid == 0) {
         atomicOr(a.status, kStatusWaitTimeout);
         mbar_wait_bounded(&full[buf], (t >> 1) & 1);
-        if (t + 1 < ntile && !(seed && t + 1 == kSeedTiles)) mbar_wait_bounded(&full[buf ^ 1], ((t + 1) >> 1) & 1);
+        if (*s_nvisit > t + 1) mbar_wait_bounded(&full[buf ^ 1], ((t + 1) >> 1) & 1);
       }
       return;
     }
@@ -462,15 +521,14 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
         mv[slot * L + s] = vals[s];
       }
       __syncthreads();
-      float tau0 = INFINITY;
       if (split == 0) {
         const float next = merge_splits<G, L>(mk, mv, QPC, lq, KMAX - K, K + 1, out_k + lq * L, out_i + lq * L);
-        tau0 = out_k[lq * L + K];
+        const float tau0 = out_k[lq * L + K];
         if (next == tau0) tie_key = fminf(tie_key, next);
         mf[lq] = tau0;
       }
       __syncthreads();
-      tau0 = mf[lq];
+      const float tau0 = mf[lq];
 #pragma unroll
       for (int s = 0; s < L; ++s) {
         const int j = s - (KMAX - K);
@@ -480,12 +538,21 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
         }
       }
       tau = fminf(tau, tau0);
-      __syncthreads();
+      float tmax = -INFINITY;
+      if (warp == 0) {
+        for (int i = lane; i < QPC; i += 32) tmax = fmaxf(tmax, mf[i]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
+      }
+      bool go[2] = {false, false};
       if (tid == 0)
-        for (int t2 = kSeedTiles; t2 < kSeedTiles + 2 && t2 < ntile; ++t2) {
-          fence_proxy_async_smem();
-          issue(t2);
-        }
+        for (int v = kSeedTiles; v < kSeedTiles + 2; ++v) go[v - kSeedTiles] = decide(v, tmax);
+      __syncthreads();
+      if (tid == 0) {
+        fence_proxy_async_smem();
+        for (int v = kSeedTiles; v < kSeedTiles + 2; ++v)
+          if (go[v - kSeedTiles]) issue(v);
+      }
       continue;
     }
     float tm = keys[L - 1];
@@ -493,9 +560,16 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
     for (int g = 0; g < G; ++g) tm = fminf(tm, tau_share[buf * kSearchThreads + g * QPC + lq]);
     tau = fminf(tau, tm);
     const bool deferred = seed && t < kSeedTiles - 1;
-    if (tid == 0 && t + 2 < ntile && !deferred) {
-      fence_proxy_async_smem();
-      issue(t + 2);
+    if (warp == 0 && !deferred) {
+      float tmax = -INFINITY;
+#pragma unroll
+      for (int i = 0; i < kSearchThreads / 32; ++i) tmax = fmaxf(tmax, tau_share[buf * kSearchThreads + i * 32 + lane]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
+      if (lane == 0 && decide(t + 2, tmax)) {
+        fence_proxy_async_smem();
+        issue(t + 2);
+      }
     }
   }
 
@@ -545,14 +619,13 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
   __syncthreads();
 
   // ---- epilogue: dists / idxs / w_out, then f_out = sum_k w_k f[idx_k]
-  // accumulated in k order with fma, 128-bit gathers of f rows.
-  const int qbase = blockIdx.x * QPC;
-  const int nq = min(QPC, a.Q - qbase);
-  const int64_t q0 = (int64_t)b * a.Q + qbase;
-  for (int it = tid; it < nq * K; it += kSearchThreads) {
+  // accumulated in k order with fma, 128-bit gathers of f rows.  Rows go to
+  // the queries' original positions.
+  const int64_t qrow0 = (int64_t)b * a.Q;
+  for (int it = tid; it < QPC * K; it += kSearchThreads) {
     const int l = it / K, k = it - l * K;
     if (out_f[l]) continue;
-    const int64_t e = (q0 + l) * K + k;
+    const int64_t e = (qrow0 + qorig[l]) * K + k;
     a.dists[e] = out_k[l * L + k];
     a.idxs[e] = (int64_t)out_i[l * L + k];
     a.w_out[e] = out_w[l * L + k];
@@ -561,7 +634,7 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
   const float* fb = a.f + (int64_t)b * P * F;
   if (a.vec4) {
     const int C4 = F >> 2;
-    for (int it = tid; it < nq * C4; it += kSearchThreads) {
+    for (int it = tid; it < QPC * C4; it += kSearchThreads) {
       const int l = it / C4, c = it - l * C4;
       if (out_f[l]) continue;
       float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -574,16 +647,16 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
         acc.z = __fmaf_rn(v.z, w, acc.z);
         acc.w = __fmaf_rn(v.w, w, acc.w);
       }
-      reinterpret_cast<float4*>(a.f_out + (q0 + l) * F)[c] = acc;
+      reinterpret_cast<float4*>(a.f_out + (qrow0 + qorig[l]) * F)[c] = acc;
     }
   } else {
-    for (int it = tid; it < nq * F; it += kSearchThreads) {
+    for (int it = tid; it < QPC * F; it += kSearchThreads) {
       const int l = it / F, c = it - l * F;
       if (out_f[l]) continue;
       float acc = 0.f;
       for (int k = 0; k < K; ++k)
         acc = __fmaf_rn(__ldg(fb + (int64_t)out_i[l * L + k] * F + c), out_w[l * L + k], acc);
-      a.f_out[(q0 + l) * F + c] = acc;
+      a.f_out[(qrow0 + qorig[l]) * F + c] = acc;
     }
   }
 }
@@ -605,15 +678,16 @@ int num_sms(int dev) {
 
 template <int KMAX, int G>
 int launch_search_t(const SearchParams& a, cudaStream_t st) {
-  constexpr size_t smem = search_smem_bytes(KMAX, G);
-  static bool attr_set[64] = {false};
+  const size_t smem = search_smem_bytes(KMAX, G) + search_region_c_bytes(a.ntile, G);
+  if (smem > 227 * 1024) return KNNAG_ERR_TOO_LARGE;
+  static int attr_set[64] = {0};  // largest size already allowed, per device
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-    if (cudaFuncSetAttribute(search_f32_kernel<KMAX, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
+  if (dev >= 0 && dev < 64 && attr_set[dev] < (int)smem) {
+    if (cudaFuncSetAttribute(search_f32_kernel<KMAX, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
       return KNNAG_ERR_CUDA;
-    attr_set[dev] = true;
+    attr_set[dev] = (int)smem;
   }
   constexpr int QPC = 32 * (4 / G);
   dim3 grid((a.Q + QPC - 1) / QPC, a.B);
@@ -688,8 +762,26 @@ FwdLayout fwd_layout(int B, int Q, int P, int K, int dtype, bool own_rec) {
   L.rec = off;
   if (own_rec) off += align256((size_t)B * P * kRecLen * esz);
   L.P_pad = (int)round_up(P, kTilePoints);
-  L.pairs = off;
-  if (dtype == KNNAG_F32 && K <= 32) off += align256((size_t)B * L.P_pad * kRecLen * 4);
+  L.pairs = L.bounds = L.cell_count = L.cell_offset = L.perm_p = L.perm_q = L.tinfo = off;
+  L.bits = 0;
+  if (dtype == KNNAG_F32 && K <= 32) {
+    L.bits = spatial_bits(P);
+    const size_t cells = (size_t)1 << (3 * L.bits);
+    L.pairs = off;
+    off += align256((size_t)B * L.P_pad * kRecLen * 4);
+    L.bounds = off;
+    off += align256((size_t)B * 8 * 4);
+    L.cell_count = off;
+    off += align256((size_t)B * cells * 4);
+    L.cell_offset = off;
+    off += align256(((size_t)B * cells + 1) * 4);
+    L.perm_p = off;
+    off += align256((size_t)B * P * 4);
+    L.perm_q = off;
+    off += align256((size_t)B * Q * 4);
+    L.tinfo = off;
+    off += align256((size_t)B * (L.P_pad / kTilePoints) * 8 * 4);
+  }
   L.total = off;
   return L;
 }
@@ -738,12 +830,13 @@ int forward_impl(const void* q, const void* p, const void* f, const void* sigma,
   int dev = 0;
   cudaGetDevice(&dev);
   float* pairs = reinterpret_cast<float*>(ws + L.pairs);
-  pack_pairs_kernel<<<grid_for((int64_t)B * L.P_pad * kRecLen, 256, dev), 256, 0, st>>>(
-      (const float*)rec, B, P, L.P_pad, pairs);
-  note_launches(1);
-  if (cudaGetLastError() != cudaSuccess) return KNNAG_ERR_CUDA;
+  rc = launch_spatial_index((const float*)q, (const float*)rec, B, Q, P, L.P_pad, ws, L, st);
+  if (rc) return rc;
   SearchParams sp{};
   sp.q = (const float*)q;
+  sp.perm_q = reinterpret_cast<const int*>(ws + L.perm_q);
+  sp.tinfo = reinterpret_cast<const float*>(ws + L.tinfo);
+  sp.ntile = L.P_pad / kTilePoints;
   sp.pairs = pairs;
   sp.rec = (const float*)rec;
   sp.f = (const float*)f;

@@ -1,0 +1,260 @@
+// Spatial ordering for the search: points and queries of every batch element
+// are counting-sorted by the Morton code of a uniform grid cell, the search
+// tiles are packed in that order (each record keeps its original point
+// index), and every 128-point tile gets an axis-aligned box and a lower bound
+// on the key of any query against any of its points:
+//     key(q, i) >= mu_tile * dist(q, box_tile)^2,
+//     mu_tile = min over the tile's points of  lambda_min(R^T diag(sigma) R)
+//               - 1e-5 * sum_a |sigma_a| |R_a|^2,
+// where lambda_min is computed in double and the second term covers the
+// rounding of the FP32 key (|key_fp32 - key_exact| <= ~12 * 2^-24 *
+// |q - p|^2 * sum_a |sigma_a| |R_a|^2).  Non-finite data give mu = 0 (no bound).
+// The search visits tiles nearest-first by this bound and stops when the
+// bound exceeds every query's threshold; the order of points inside a cell
+// (atomic scatter) never changes a result, only the work done.
+#include <math.h>
+
+#include <algorithm>
+
+#include "knn_common.cuh"
+#include "knn_internal.h"
+
+namespace knnag {
+
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+__device__ __forceinline__ uint32_t cell_of(float x, float y, float z, const float* bnd, int bits) {
+  const float res = (float)(1 << bits);
+  uint32_t c[3];
+  const float v[3] = {x, y, z};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float lo = bnd[a], ext = bnd[3 + a] - bnd[a];
+    float t = ext > 0.f ? (v[a] - lo) / ext * res : 0.f;
+    t = fminf(fmaxf(t, 0.f), res - 1.f);  // NaN -> 0
+    c[a] = (uint32_t)t;
+  }
+  return spread3(c[0]) | (spread3(c[1]) << 1) | (spread3(c[2]) << 2);
+}
+
+// Per batch element: bounding box of its points, bnd[b] = {min xyz, max xyz}.
+__global__ void __launch_bounds__(512) point_bounds_kernel(const float* __restrict__ rec, int P, float* __restrict__ bnd) {
+  __shared__ float red[6][16];
+  const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int i = tid; i < P; i += blockDim.x) {
+    const float* r = rec + ((int64_t)b * P + i) * kRecLen;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float v = -r[kNPX + a];
+      mn[a] = fminf(mn[a], v);
+      mx[a] = fmaxf(mx[a], v);
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mn[a] = fminf(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], o));
+      mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
+    }
+  if (lane == 0)
+    for (int a = 0; a < 3; ++a) {
+      red[a][warp] = mn[a];
+      red[3 + a][warp] = mx[a];
+    }
+  __syncthreads();
+  if (tid < 6) {
+    float v = tid < 3 ? INFINITY : -INFINITY;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v = tid < 3 ? fminf(v, red[tid][w]) : fmaxf(v, red[tid][w]);
+    bnd[b * 8 + tid] = v;
+  }
+}
+
+// Cell histogram of points (from records) or queries (from q).
+__global__ void cell_count_kernel(const float* __restrict__ xyz, int stride, int negate, int n_per_b, int B,
+                                  const float* __restrict__ bnd, int bits, int* __restrict__ count) {
+  const int cells = 1 << (3 * bits);
+  const int n = B * n_per_b;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int b = i / n_per_b;
+    const float* v = xyz + (int64_t)i * stride;
+    const float s = negate ? -1.f : 1.f;
+    const uint32_t c = cell_of(s * v[0], s * v[1], s * v[2], bnd + b * 8, bits);
+    atomicAdd(&count[b * cells + (int)c], 1);
+  }
+}
+
+// perm[offset[cell] + rank] = index within the batch element (positions of
+// batch b lie in [b*n_per_b, (b+1)*n_per_b) because the scan runs over
+// [b][cell]).
+__global__ void cell_scatter_kernel(const float* __restrict__ xyz, int stride, int negate, int n_per_b, int B,
+                                    const float* __restrict__ bnd, int bits, const int* __restrict__ offset,
+                                    int* __restrict__ cursor, int* __restrict__ perm) {
+  const int cells = 1 << (3 * bits);
+  const int n = B * n_per_b;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int b = i / n_per_b;
+    const float* v = xyz + (int64_t)i * stride;
+    const float s = negate ? -1.f : 1.f;
+    const int c = b * cells + (int)cell_of(s * v[0], s * v[1], s * v[2], bnd + b * 8, bits);
+    perm[offset[c] + atomicAdd(&cursor[c], 1)] = i - b * n_per_b;
+  }
+}
+
+// Pair-interleaved tiles in sorted order; field kRecPad carries the original
+// point index (int bits), -1 for padding (whose sigma is NaN).
+__global__ void pack_pairs_sorted_kernel(const float* __restrict__ rec, const int* __restrict__ perm, int B, int P,
+                                         int P_pad, float* __restrict__ pairs) {
+  const int64_t total = (int64_t)B * P_pad * kRecLen;
+  for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < total; o += (int64_t)gridDim.x * blockDim.x) {
+    const int half = (int)(o & 1);
+    const int field = (int)((o >> 1) & (kRecLen - 1));
+    const int64_t pair = o >> 5;
+    const int64_t b = pair / (P_pad / 2);
+    const int64_t pos = 2 * (pair - b * (P_pad / 2)) + half;
+    float v;
+    if (pos < P) {
+      const int i = perm[b * P + pos];
+      v = field == kRecPad ? __int_as_float(i) : rec[(b * P + i) * kRecLen + field];
+    } else if (field == kRecPad) {
+      v = __int_as_float(-1);
+    } else {
+      v = (field == kS0 || field == kS1 || field == kS2) ? __int_as_float(0x7fc00000) : 0.0f;
+    }
+    pairs[o] = v;
+  }
+}
+
+// Smallest eigenvalue of a symmetric 3x3 matrix (closed form), double.
+__device__ double sym3_min_eig(double a00, double a11, double a22, double a01, double a02, double a12) {
+  const double p1 = a01 * a01 + a02 * a02 + a12 * a12;
+  if (p1 == 0.0) return fmin(a00, fmin(a11, a22));
+  const double qm = (a00 + a11 + a22) / 3.0;
+  const double b00 = a00 - qm, b11 = a11 - qm, b22 = a22 - qm;
+  const double p2 = b00 * b00 + b11 * b11 + b22 * b22 + 2.0 * p1;
+  const double p = sqrt(p2 / 6.0);
+  const double ip = 1.0 / p;
+  const double c00 = b00 * ip, c11 = b11 * ip, c22 = b22 * ip, c01 = a01 * ip, c02 = a02 * ip, c12 = a12 * ip;
+  double r = 0.5 * (c00 * (c11 * c22 - c12 * c12) - c01 * (c01 * c22 - c12 * c02) + c02 * (c01 * c12 - c11 * c02));
+  r = fmin(1.0, fmax(-1.0, r));
+  const double phi = acos(r) / 3.0;
+  return qm + 2.0 * p * cos(phi + 2.0943951023931957);  // + 2 pi / 3
+}
+
+// tinfo[(b*ntile + t)*8] = {min xyz, max xyz, mu, 0}; one warp per tile.
+__global__ void tile_info_kernel(const float* __restrict__ rec, const int* __restrict__ perm, int B, int P, int ntile,
+                                 float* __restrict__ tinfo) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int tt = gw; tt < B * ntile; tt += nw) {
+    const int b = tt / ntile, t = tt - b * ntile;
+    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    float mu = INFINITY;
+    bool bad = false;
+    for (int k = lane; k < kTilePoints; k += 32) {
+      const int pos = t * kTilePoints + k;
+      if (pos >= P) continue;
+      const float* r = rec + ((int64_t)b * P + perm[(int64_t)b * P + pos]) * kRecLen;
+      float v[kRecLen];
+#pragma unroll
+      for (int m = 0; m < kRecLen; ++m) v[m] = r[m];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const float c = -v[kNPX + a];
+        mn[a] = fminf(mn[a], c);
+        mx[a] = fmaxf(mx[a], c);
+        if (!isfinite(c)) bad = true;
+      }
+      double M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      double err = 0.0;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const double s = v[kS0 + a];
+        double rn = 0.0;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          const double ra = v[kR00 + 3 * a + m];
+          rn += ra * ra;
+#pragma unroll
+          for (int n2 = 0; n2 < 3; ++n2) M[m][n2] += s * ra * (double)v[kR00 + 3 * a + n2];
+        }
+        err += fabs(s) * rn;
+      }
+      const double lam = sym3_min_eig(M[0][0], M[1][1], M[2][2], M[0][1], M[0][2], M[1][2]);
+      const double scale = fabs(M[0][0]) + fabs(M[1][1]) + fabs(M[2][2]) + fabs(M[0][1]) + fabs(M[0][2]) + fabs(M[1][2]);
+      const double m = lam - 1e-9 * scale - 1e-5 * err;
+      if (!isfinite(m)) bad = true;
+      mu = fminf(mu, (m > 0.0 && isfinite(m)) ? (float)(m * (1.0 - 1e-6)) : 0.0f);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        mn[a] = fminf(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], o));
+        mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
+      }
+      mu = fminf(mu, __shfl_xor_sync(0xffffffffu, mu, o));
+    }
+    bad = __any_sync(0xffffffffu, bad);
+    if (lane == 0) {
+      float* o = tinfo + (int64_t)tt * 8;
+      for (int a = 0; a < 3; ++a) {
+        o[a] = mn[a];
+        o[3 + a] = mx[a];
+      }
+      o[6] = (bad || !(mu < INFINITY)) ? 0.0f : mu;
+      o[7] = 0.0f;
+    }
+  }
+}
+
+int spatial_bits(int P) {
+  int bits = 1;
+  while (bits < 10 && (int64_t(1) << (3 * bits)) * 8 < P) ++bits;
+  return bits;
+}
+
+int launch_spatial_index(const float* q, const float* rec, int B, int Q, int P, int P_pad, char* ws, const FwdLayout& L,
+                         cudaStream_t st) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int bits = L.bits, cells = 1 << (3 * bits);
+  float* bnd = reinterpret_cast<float*>(ws + L.bounds);
+  int* cnt = reinterpret_cast<int*>(ws + L.cell_count);
+  int* off = reinterpret_cast<int*>(ws + L.cell_offset);
+  int* perm_p = reinterpret_cast<int*>(ws + L.perm_p);
+  int* perm_q = reinterpret_cast<int*>(ws + L.perm_q);
+  float* pairs = reinterpret_cast<float*>(ws + L.pairs);
+  float* tinfo = reinterpret_cast<float*>(ws + L.tinfo);
+  auto grid = [&](int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, sms * 16)); };
+  point_bounds_kernel<<<B, 512, 0, st>>>(rec, P, bnd);
+  // points
+  if (cudaMemsetAsync(cnt, 0, (size_t)B * cells * 4, st) != cudaSuccess) return KNNAG_ERR_CUDA;
+  cell_count_kernel<<<grid((int64_t)B * P), 256, 0, st>>>(rec + kNPX, kRecLen, 1, P, B, bnd, bits, cnt);
+  int rc = launch_exclusive_scan(cnt, B * cells, off, st);
+  if (rc) return rc;
+  cell_scatter_kernel<<<grid((int64_t)B * P), 256, 0, st>>>(rec + kNPX, kRecLen, 1, P, B, bnd, bits, off, cnt, perm_p);
+  // queries (the scatter left the point counts in cnt)
+  if (cudaMemsetAsync(cnt, 0, (size_t)B * cells * 4, st) != cudaSuccess) return KNNAG_ERR_CUDA;
+  cell_count_kernel<<<grid((int64_t)B * Q), 256, 0, st>>>(q, 3, 0, Q, B, bnd, bits, cnt);
+  rc = launch_exclusive_scan(cnt, B * cells, off, st);
+  if (rc) return rc;
+  cell_scatter_kernel<<<grid((int64_t)B * Q), 256, 0, st>>>(q, 3, 0, Q, B, bnd, bits, off, cnt, perm_q);
+  pack_pairs_sorted_kernel<<<grid((int64_t)B * P_pad * kRecLen), 256, 0, st>>>(rec, perm_p, B, P, P_pad, pairs);
+  const int ntile = P_pad / kTilePoints;
+  tile_info_kernel<<<grid((int64_t)B * ntile * 32), 256, 0, st>>>(rec, perm_p, B, P, ntile, tinfo);
+  note_launches(7);
+  return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
+}
+
+}  // namespace knnag
