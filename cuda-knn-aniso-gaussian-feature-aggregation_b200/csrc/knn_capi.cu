@@ -236,6 +236,73 @@ int knnag_backward_2nd(const void* grad_grad_q, const void* grad_f_out, const vo
   return backward_common(x, workspace_bytes, stream);
 }
 
+size_t knnag_variant_workspace_bytes(int B, int Q, int P, int dtype) {
+  if (B < 0 || Q < 0 || P < 0) return 0;
+  return 256 + align256((size_t)B * P * kRecLen * (dtype == KNNAG_F64 ? 8 : 4)) + align256((size_t)B * Q * 4);
+}
+
+static int variant_checks(const void* q, const void* p, const void* f, const void* sigma, int B, int Q, int P, int F,
+                          int K, int dtype, const void* f_out, const void* w_out, const void* dists) {
+  if (dtype != KNNAG_F32 && dtype != KNNAG_F64) return KNNAG_ERR_DTYPE;
+  int rc = check_sizes(B, Q, P, F, K);
+  if (rc) return rc;
+  if ((int64_t)B * Q == 0) return -1;  // nothing to do
+  if (!q || !p || !sigma || !w_out || !dists) return KNNAG_ERR_ARG;
+  if (F > 0 && (!f || !f_out)) return KNNAG_ERR_ARG;
+  return KNNAG_OK;
+}
+
+int knnag_forward_precomputed(const void* q, const void* p, const void* f, const void* sigma, const void* R,
+                              const int64_t* knn_idxs, int B, int Q, int P, int F, int K, int dtype, void* f_out,
+                              void* w_out, void* dists, void* workspace, size_t workspace_bytes, void* stream) {
+  int rc = variant_checks(q, p, f, sigma, B, Q, P, F, K, dtype, f_out, w_out, dists);
+  if (rc) return rc < 0 ? KNNAG_OK : rc;
+  if (!R || !knn_idxs || !workspace) return KNNAG_ERR_ARG;
+  if (workspace_bytes < knnag_variant_workspace_bytes(B, Q, P, dtype) || ((uintptr_t)workspace & 15u))
+    return KNNAG_ERR_WORKSPACE;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  void* rec = static_cast<char*>(workspace) + 256;
+  rc = launch_pack_points(p, sigma, R, B, P, dtype, rec, st);
+  if (rc) return rc;
+  return variants_precomputed(q, f, rec, knn_idxs, B, Q, P, F, K, dtype, f_out, w_out, dists, st);
+}
+
+int knnag_forward_lookup(const void* q, const void* p, const void* f, const void* sigma, const void* R,
+                         const int64_t* knn_table, int table_cols, int B, int Q, int P, int F, int K, int dtype,
+                         void* f_out, void* w_out, void* dists, int64_t* idxs, void* workspace,
+                         size_t workspace_bytes, void* stream) {
+  int rc = variant_checks(q, p, f, sigma, B, Q, P, F, K, dtype, f_out, w_out, dists);
+  if (rc) return rc < 0 ? KNNAG_OK : rc;
+  if (!R || !knn_table || !idxs || !workspace || table_cols < K) return KNNAG_ERR_ARG;
+  if (workspace_bytes < knnag_variant_workspace_bytes(B, Q, P, dtype) || ((uintptr_t)workspace & 15u))
+    return KNNAG_ERR_WORKSPACE;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  char* ws = static_cast<char*>(workspace);
+  void* rec = ws + 256;
+  int* nearest = reinterpret_cast<int*>(ws + 256 + align256((size_t)B * P * kRecLen * (dtype == KNNAG_F64 ? 8 : 4)));
+  rc = launch_pack_points(p, sigma, R, B, P, dtype, rec, st);
+  if (rc) return rc;
+  return variants_lookup(q, p, f, rec, knn_table, table_cols, B, Q, P, F, K, dtype, nearest, f_out, w_out, dists, idxs, st);
+}
+
+int knnag_forward_isotropic(const void* q, const void* p, const void* f, const void* sigma, int sigma_cols, int B,
+                            int Q, int P, int F, int K, int dtype, void* f_out, void* w_sum, void* dists,
+                            int64_t* idxs, void* stream) {
+  int rc = variant_checks(q, p, f, sigma, B, Q, P, F, K, dtype, f_out, w_sum, dists);
+  if (rc) return rc < 0 ? KNNAG_OK : rc;
+  if (!idxs || sigma_cols < 1) return KNNAG_ERR_ARG;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dtype == KNNAG_F64) {
+    ExactParams<double> e{(const double*)q, nullptr, (const double*)f, (const double*)p, (const double*)sigma,
+                          sigma_cols, B, Q, P, F, K, 0, nullptr, nullptr, (double*)f_out, (double*)w_sum,
+                          (double*)dists, idxs};
+    return launch_exact<double>(e, st);
+  }
+  ExactParams<float> e{(const float*)q, nullptr, (const float*)f, (const float*)p, (const float*)sigma, sigma_cols,
+                       B, Q, P, F, K, 0, nullptr, nullptr, (float*)f_out, (float*)w_sum, (float*)dists, idxs};
+  return launch_exact<float>(e, st);
+}
+
 int knnag_read_device_status(void* workspace, void* stream) {
   if (!workspace) return KNNAG_ERR_ARG;
   cudaStream_t st = static_cast<cudaStream_t>(stream);

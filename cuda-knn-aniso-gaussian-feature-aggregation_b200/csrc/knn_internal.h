@@ -13,6 +13,12 @@ struct ExactParams {
   const T* q;
   const T* rec;  // per-point records [B*P*16]
   const T* f;
+  // isotropic forward only (key = squared Euclidean distance): raw points,
+  // sigma [B,P,iso_stride] (component 0 scales the key in the weight); the
+  // weight sum goes to w_out[B,Q,1]
+  const T* iso_p;
+  const T* iso_sigma;
+  int iso_stride;
   int B, Q, P, F, K;
   int use_list;            // 1: process list[0 .. *list_count), 0: every query
   const int* list;
@@ -93,6 +99,13 @@ int spatial_bits(int P);
 int launch_spatial_index(const float* q, const float* rec, int B, int Q, int P, int P_pad, char* ws, const FwdLayout& L,
                          cudaStream_t st);
 int launch_exclusive_scan(int* count, int n, int* out, cudaStream_t st);
+template <typename T>
+int launch_exact(const ExactParams<T>& a, cudaStream_t st);
+int variants_precomputed(const void* q, const void* f, const void* rec, const int64_t* idxs, int B, int Q, int P,
+                         int F, int K, int dtype, void* f_out, void* w_out, void* dists, cudaStream_t st);
+int variants_lookup(const void* q, const void* p, const void* f, const void* rec, const int64_t* table, int tstride, int B, int Q,
+                    int P, int F, int K, int dtype, int* nearest, void* f_out, void* w_out, void* dists,
+                    int64_t* idxs, cudaStream_t st);
 FwdLayout fwd_layout(int B, int Q, int P, int K, int dtype, bool own_rec);
 
 // Adjacency (CSR) layout: rowptr [B*P+1] | cursor [B*P] | unsorted [N] | entries [N].

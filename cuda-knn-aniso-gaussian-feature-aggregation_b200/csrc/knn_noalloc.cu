@@ -27,9 +27,10 @@
 
 namespace knnag {
 
-// 8 MiB: enough for B*P up to ~60k points and B*Q up to ~500k queries at the
-// default tile size (the status words, B*Q*4 bytes of flags, 64 bytes per
-// point of records and 64 bytes per padded point of tiles, 256-byte aligned).
+// 8 MiB: the forward's scratch is about 130 bytes per point (records, search
+// tiles, spatial-index keys and permutation, tile bounds) plus 8 bytes per
+// query (flag list, query permutation): up to ~60k points with few queries,
+// or ~40k points with ~300k queries.
 constexpr size_t kNoallocScratchBytes = size_t(8) << 20;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];

@@ -104,7 +104,17 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
     T max_key = T(0), my_k = T(0);
     for (int c0 = 0; c0 < P; c0 += CH) {
       const int n = min(CH, P - c0);
-      for (int i = tid; i < n; i += kReplayThreads) skey[i] = key_rec<T>(qx, qy, qz, recb + (int64_t)(c0 + i) * kRecLen);
+      if (a.iso_p) {
+        // squared Euclidean distance, accumulated as d = 0; d += c*c (csrc/forward.cu:32-36)
+        const T* pb = a.iso_p + b * (int64_t)P * 3;
+        for (int i = tid; i < n; i += kReplayThreads) {
+          const T* pp = pb + (int64_t)(c0 + i) * 3;
+          const T x = qx - pp[0], y = qy - pp[1], z = qz - pp[2];
+          skey[i] = fma_rn(z, z, fma_rn(y, y, mul_rn(x, x)));
+        }
+      } else {
+        for (int i = tid; i < n; i += kReplayThreads) skey[i] = key_rec<T>(qx, qy, qz, recb + (int64_t)(c0 + i) * kRecLen);
+      }
       __syncthreads();
       if (warp == 0) {
         for (int base = 0; base < n; base += 32) {
@@ -193,16 +203,39 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
       }
     }
     __syncthreads();
-    for (int k = tid; k < K; k += kReplayThreads) {
-      const int64_t e = bq * K + k;
-      a.dists[e] = slot_k[k];
-      a.idxs[e] = (int64_t)slot_v[k];
-      a.w_out[e] = weight_of(slot_k[k]);
+    if (a.iso_p) {
+      // isotropic weights w_k = exp(-(d_k * sigma[idx_k][0])) and their sum
+      // in k order (csrc/forward.cu:43-52); keep w_k in slot_k
+      const T* sg = a.iso_sigma + b * (int64_t)P * a.iso_stride;
+      for (int k = tid; k < K; k += kReplayThreads) {
+        const int64_t e = bq * K + k;
+        a.dists[e] = slot_k[k];
+        a.idxs[e] = (int64_t)slot_v[k];
+      }
+      __syncthreads();
+      for (int k = tid; k < K; k += kReplayThreads)
+        slot_k[k] = weight_of(mul_rn(slot_k[k], sg[(int64_t)slot_v[k] * a.iso_stride]));
+      __syncthreads();
+      if (tid == 0) {
+        T ws = T(0);
+        for (int k = 0; k < K; ++k) ws = add_rn(ws, slot_k[k]);
+        a.w_out[bq] = ws;
+      }
+    } else {
+      for (int k = tid; k < K; k += kReplayThreads) {
+        const int64_t e = bq * K + k;
+        a.dists[e] = slot_k[k];
+        a.idxs[e] = (int64_t)slot_v[k];
+        a.w_out[e] = weight_of(slot_k[k]);
+      }
+      __syncthreads();
+      for (int k = tid; k < K; k += kReplayThreads) slot_k[k] = weight_of(slot_k[k]);
+      __syncthreads();
     }
     const T* fb = a.f + b * (int64_t)P * F;
     for (int c = tid; c < F; c += kReplayThreads) {
       T acc = T(0);
-      for (int k = 0; k < K; ++k) acc = fma_rn(fb[(int64_t)slot_v[k] * F + c], weight_of(slot_k[k]), acc);
+      for (int k = 0; k < K; ++k) acc = fma_rn(fb[(int64_t)slot_v[k] * F + c], slot_k[k], acc);
       a.f_out[bq * F + c] = acc;
     }
     __syncthreads();
@@ -705,6 +738,26 @@ int launch_search_k(const SearchParams& a, int G, cudaStream_t st) {
   return launch_search_t<KMAX, 4>(a, st);
 }
 
+// Splits per query group: the fewest that still give ~4 CTAs per SM.
+int choose_splits(int B, int Q, int dev) {
+  const int64_t target = (int64_t)num_sms(dev) * 4;
+  for (int g = 1; g <= 4; g *= 2) {
+    const int qpc = 32 * (4 / g);
+    const int64_t ctas = (int64_t)B * ((Q + qpc - 1) / qpc);
+    if (ctas >= target) return g;
+  }
+  return 4;
+}
+
+inline unsigned grid_for(int64_t n, int threads, int dev) {
+  int64_t b = (n + threads - 1) / threads;
+  const int64_t cap = (int64_t)num_sms(dev) * 32;
+  if (b > cap) b = cap;
+  return (unsigned)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
 template <typename T>
 int launch_exact(const ExactParams<T>& a, cudaStream_t st) {
   const size_t smem = (size_t)replay_chunk<T>() * sizeof(T) + (size_t)a.K * (sizeof(T) + sizeof(int));
@@ -731,25 +784,8 @@ int launch_exact(const ExactParams<T>& a, cudaStream_t st) {
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 
-// Splits per query group: the fewest that still give ~4 CTAs per SM.
-int choose_splits(int B, int Q, int dev) {
-  const int64_t target = (int64_t)num_sms(dev) * 4;
-  for (int g = 1; g <= 4; g *= 2) {
-    const int qpc = 32 * (4 / g);
-    const int64_t ctas = (int64_t)B * ((Q + qpc - 1) / qpc);
-    if (ctas >= target) return g;
-  }
-  return 4;
-}
-
-inline unsigned grid_for(int64_t n, int threads, int dev) {
-  int64_t b = (n + threads - 1) / threads;
-  const int64_t cap = (int64_t)num_sms(dev) * 32;
-  if (b > cap) b = cap;
-  return (unsigned)(b < 1 ? 1 : b);
-}
-
-}  // namespace
+template int launch_exact<float>(const ExactParams<float>&, cudaStream_t);
+template int launch_exact<double>(const ExactParams<double>&, cudaStream_t);
 
 FwdLayout fwd_layout(int B, int Q, int P, int K, int dtype, bool own_rec) {
   FwdLayout L{};
@@ -804,7 +840,7 @@ int launch_pack_points(const void* p, const void* sigma, const void* R, int B, i
 template <typename T>
 static int forward_exact_all(const T* q, const T* rec, const T* f, int B, int Q, int P, int F, int K, T* f_out,
                              T* w_out, T* dists, int64_t* idxs, cudaStream_t st) {
-  ExactParams<T> e{q, rec, f, B, Q, P, F, K, 0, nullptr, nullptr, f_out, w_out, dists, idxs};
+  ExactParams<T> e{q, rec, f, nullptr, nullptr, 0, B, Q, P, F, K, 0, nullptr, nullptr, f_out, w_out, dists, idxs};
   return launch_exact<T>(e, st);
 }
 
@@ -863,8 +899,8 @@ int forward_impl(const void* q, const void* p, const void* f, const void* sigma,
     rc = launch_search_k<32>(sp, G, st);
   if (rc) return rc;
   // Exact MinK replay of the flagged queries (count read on the device).
-  ExactParams<float> e{(const float*)q, (const float*)rec, (const float*)f, B, Q, P, F, K, 1, flag_list,
-                       flag_count, (float*)f_out, (float*)w_out, (float*)dists, idxs};
+  ExactParams<float> e{(const float*)q, (const float*)rec, (const float*)f, nullptr, nullptr, 0, B, Q, P, F, K, 1,
+                       flag_list, flag_count, (float*)f_out, (float*)w_out, (float*)dists, idxs};
   return launch_exact<float>(e, st);
 }
 

@@ -198,6 +198,84 @@ std::vector<torch::Tensor> knn_aggregate_aniso_backward_2nd(torch::Tensor grad_g
                        c10::nullopt, KNNAG_NEED_ALL, false);
 }
 
+// ------------------------------------------------- other reference ops
+
+std::vector<torch::Tensor> knn_precomputed_aggregate_aniso_forward(torch::Tensor q, torch::Tensor p, torch::Tensor f,
+                                                                   torch::Tensor sigma, torch::Tensor R,
+                                                                   torch::Tensor knn_idxs, int64_t K) {
+  const Dims d = check_inputs(q, p, f, sigma, R);
+  KNN_CHECK_INPUT(knn_idxs);
+  TORCH_CHECK(knn_idxs.scalar_type() == torch::kInt64 && knn_idxs.dim() == 3 && knn_idxs.size(0) == d.B &&
+                  knn_idxs.size(1) == d.Q && knn_idxs.size(2) == K,
+              "knn_idxs must be int64 [B, Q, K]");
+  check_k(K, d.P);
+  const c10::cuda::CUDAGuard guard(q.device());
+  auto f_out = torch::empty({d.B, d.Q, d.F}, f.options());
+  auto w_out = torch::empty({d.B, d.Q, K}, f.options());
+  auto dists = torch::empty({d.B, d.Q, K}, q.options());
+  const size_t nb = knnag_variant_workspace_bytes(d.B, d.Q, d.P, d.dtype);
+  auto ws = scratch(nb, q);
+  check_status(knnag_forward_precomputed(q.data_ptr(), p.data_ptr(), f.data_ptr(), sigma.data_ptr(), R.data_ptr(),
+                                         knn_idxs.data_ptr<int64_t>(), d.B, d.Q, d.P, d.F, (int)K, d.dtype,
+                                         f_out.data_ptr(), w_out.data_ptr(), dists.data_ptr(), ws.data_ptr(), nb,
+                                         stream_of(q)),
+               "knn_precomputed_aggregate_aniso_forward");
+  return {f_out, w_out, dists};
+}
+
+std::vector<torch::Tensor> knn_lookup_aggregate_aniso_forward(torch::Tensor q, torch::Tensor p, torch::Tensor f,
+                                                              torch::Tensor sigma, torch::Tensor R,
+                                                              torch::Tensor knn_table, int64_t K) {
+  const Dims d = check_inputs(q, p, f, sigma, R);
+  KNN_CHECK_INPUT(knn_table);
+  TORCH_CHECK(knn_table.scalar_type() == torch::kInt64 && knn_table.dim() == 2 && knn_table.size(0) >= d.P &&
+                  knn_table.size(1) >= K,
+              "knn_table must be int64 [P, >= K]");
+  check_k(K, d.P);
+  const c10::cuda::CUDAGuard guard(q.device());
+  auto f_out = torch::empty({d.B, d.Q, d.F}, f.options());
+  auto w_out = torch::empty({d.B, d.Q, K}, f.options());
+  auto dists = torch::empty({d.B, d.Q, K}, q.options());
+  auto idxs = torch::empty({d.B, d.Q, K}, q.options().dtype(torch::kInt64));
+  const size_t nb = knnag_variant_workspace_bytes(d.B, d.Q, d.P, d.dtype);
+  auto ws = scratch(nb, q);
+  check_status(knnag_forward_lookup(q.data_ptr(), p.data_ptr(), f.data_ptr(), sigma.data_ptr(), R.data_ptr(),
+                                    knn_table.data_ptr<int64_t>(), (int)knn_table.size(1), d.B, d.Q, d.P, d.F, (int)K,
+                                    d.dtype, f_out.data_ptr(), w_out.data_ptr(), dists.data_ptr(),
+                                    idxs.data_ptr<int64_t>(), ws.data_ptr(), nb, stream_of(q)),
+               "knn_lookup_aggregate_aniso_forward");
+  return {f_out, w_out, dists, idxs};
+}
+
+std::vector<torch::Tensor> knn_aggregate_forward(torch::Tensor q, torch::Tensor p, torch::Tensor f,
+                                                 torch::Tensor sigma, int64_t K) {
+  KNN_CHECK_INPUT(q);
+  KNN_CHECK_INPUT(p);
+  KNN_CHECK_INPUT(f);
+  KNN_CHECK_INPUT(sigma);
+  TORCH_CHECK(q.dim() == 3 && q.size(2) == 3 && p.dim() == 3 && p.size(2) == 3 && p.size(0) == q.size(0),
+              "q and p must have shapes [B, Q, 3] and [B, P, 3]");
+  const int B = (int)q.size(0), Q = (int)q.size(1), P = (int)p.size(1);
+  TORCH_CHECK(f.dim() == 3 && f.size(0) == B && f.size(1) == P, "f must have shape [B, P, F]");
+  TORCH_CHECK(sigma.dim() == 3 && sigma.size(0) == B && sigma.size(1) == P && sigma.size(2) >= 1,
+              "sigma must have shape [B, P, S] (component 0 is used)");
+  const int dt = dtype_code(q);
+  for (const torch::Tensor* t : {&p, &f, &sigma})
+    TORCH_CHECK(t->scalar_type() == q.scalar_type(), "all floating-point inputs must share q's dtype");
+  check_k(K, P);
+  const int F = (int)f.size(2);
+  const c10::cuda::CUDAGuard guard(q.device());
+  auto f_out = torch::empty({B, Q, F}, f.options());
+  auto w_out = torch::empty({B, Q, 1}, f.options());
+  auto dists = torch::empty({B, Q, K}, q.options());
+  auto idxs = torch::empty({B, Q, K}, q.options().dtype(torch::kInt64));
+  check_status(knnag_forward_isotropic(q.data_ptr(), p.data_ptr(), f.data_ptr(), sigma.data_ptr(), (int)sigma.size(2),
+                                       B, Q, P, F, (int)K, dt, f_out.data_ptr(), w_out.data_ptr(), dists.data_ptr(),
+                                       idxs.data_ptr<int64_t>(), stream_of(q)),
+               "knn_aggregate_forward");
+  return {f_out, w_out, dists, idxs};
+}
+
 // --------------------------------------------------------- extended ops
 
 std::vector<torch::Tensor> forward_ex(torch::Tensor q, torch::Tensor p, torch::Tensor f, torch::Tensor sigma,
@@ -252,6 +330,10 @@ PYBIND11_MODULE(_C, m) {
   m.def("knn_aggregate_aniso_backward", &knn_aggregate_aniso_backward, "KNN aggregate aniso backward");
   m.def("knn_aggregate_aniso_backward_2nd", &knn_aggregate_aniso_backward_2nd,
         "KNN aggregate aniso second order backward");
+  m.def("knn_aggregate_forward", &knn_aggregate_forward, "KNN aggregate forward");
+  m.def("knn_lookup_aggregate_aniso_forward", &knn_lookup_aggregate_aniso_forward, "KNN lookup aggregate aniso forward");
+  m.def("knn_precomputed_aggregate_aniso_forward", &knn_precomputed_aggregate_aniso_forward,
+        "KNN precomputed aggregate aniso forward");
   m.def("forward_ex", &forward_ex, "forward that also returns the packed point records");
   m.def("build_adjacency", &build_adjacency, "point -> entry adjacency (CSR) of idxs");
   m.def("adjacency_views", &adjacency_views, "rowptr / entry views of an adjacency buffer");

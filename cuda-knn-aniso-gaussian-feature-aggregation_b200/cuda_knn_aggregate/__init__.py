@@ -32,7 +32,10 @@ except ImportError as exc:  # pragma: no cover - exercised only on a broken inst
 
 __all__ = [
     "knn_aggregate_aniso",
+    "knn_aggregate_aniso_lookup",
     "KNNAnisotropicAggregate",
+    "KNNLookupAnisotropicAggregate",
+    "KNNPrecomputedAnisotropicAggregate",
     "KNNAnisotropicAggregateBackward",
 ]
 
@@ -57,6 +60,16 @@ def knn_aggregate_aniso(q: torch.Tensor, p: torch.Tensor, f: torch.Tensor, sigma
         Only f_out is differentiable.
     """
     return KNNAnisotropicAggregate.apply(q, p, f, sigma, R, K)
+
+
+def knn_aggregate_aniso_lookup(q: torch.Tensor, p: torch.Tensor, f: torch.Tensor, sigma: torch.Tensor,
+                               R: torch.Tensor, knn_table: torch.Tensor, K: int):
+    """k-NN feature aggregate with anisotropic Gaussian weights through a
+    neighbour table (reference ``__init__.py:34-62``): the Euclidean nearest
+    point of each query selects row ``knn_table[nearest, :K]`` ([P, >=K] int64,
+    shared by the batch); weights and features as knn_aggregate_aniso, in
+    table order (unsorted).  Returns f_out, w_out, dists, idxs."""
+    return KNNLookupAnisotropicAggregate.apply(q, p, f, sigma, R, knn_table, K)
 
 
 class _Aux:
@@ -105,6 +118,41 @@ class KNNAnisotropicAggregate(torch.autograd.Function):
         grads = KNNAnisotropicAggregateBackward.apply(
             grad_f_out.contiguous(), grad_w_out, q, p, f, sigma, R, None, idxs, ctx.aux)
         return (*grads, None)
+
+
+class KNNLookupAnisotropicAggregate(KNNAnisotropicAggregate):
+    """Lookup variant (reference ``__init__.py:120-165``); gradients as
+    KNNAnisotropicAggregate at the looked-up indices, none for the table."""
+
+    @staticmethod
+    def forward(ctx, q, p, f, sigma, R, knn_table, K):
+        f_out, w_out, dists, idxs = _C.knn_lookup_aggregate_aniso_forward(q, p, f, sigma, R, knn_table, int(K))
+        ctx.save_for_backward(q, p, f, sigma, R, idxs)
+        ctx.aux = _Aux(None, p.shape[1], tuple(bool(x) for x in ctx.needs_input_grad[:5]))
+        return f_out, w_out, dists, idxs
+
+    @staticmethod
+    def backward(ctx, grad_f_out, grad_w_out, grad_dists, grad_idxs):
+        return KNNAnisotropicAggregate.backward(ctx, grad_f_out, grad_w_out, grad_dists, grad_idxs) + (None,)
+
+
+class KNNPrecomputedAnisotropicAggregate(KNNAnisotropicAggregate):
+    """Aggregation at caller-given neighbour indices (reference
+    ``__init__.py:167-213``): returns f_out, w_out, dists; gradients as
+    KNNAnisotropicAggregate, none for the indices.  (The reference's backward
+    also writes grad_f_out to 'grad_f.pt'; that debug side effect is not
+    reproduced.)"""
+
+    @staticmethod
+    def forward(ctx, q, p, f, sigma, R, knn_idxs, K):
+        f_out, w_out, dists = _C.knn_precomputed_aggregate_aniso_forward(q, p, f, sigma, R, knn_idxs, int(K))
+        ctx.save_for_backward(q, p, f, sigma, R, knn_idxs)
+        ctx.aux = _Aux(None, p.shape[1], tuple(bool(x) for x in ctx.needs_input_grad[:5]))
+        return f_out, w_out, dists
+
+    @staticmethod
+    def backward(ctx, grad_f_out, grad_w_out, grad_dists):
+        return KNNAnisotropicAggregate.backward(ctx, grad_f_out, grad_w_out, grad_dists, None) + (None,)
 
 
 class KNNAnisotropicAggregateBackward(torch.autograd.Function):

@@ -31,6 +31,10 @@ _SIGS = {
     "knnag_version": ([], _I),
     "knnag_forward_workspace_bytes": ([_I, _I, _I, _I, _I, _I], _S),
     "knnag_forward": ([_V] * 5 + [_I] * 6 + [_V] * 4 + [_V, _V, _S, _V], _I),
+    "knnag_variant_workspace_bytes": ([_I, _I, _I, _I], _S),
+    "knnag_forward_precomputed": ([_V] * 6 + [_I] * 6 + [_V] * 3 + [_V, _S, _V], _I),
+    "knnag_forward_lookup": ([_V] * 6 + [_I] * 7 + [_V] * 4 + [_V, _S, _V], _I),
+    "knnag_forward_isotropic": ([_V] * 4 + [_I] * 7 + [_V] * 4 + [_V], _I),
     "knnag_points_bytes": ([_I, _I, _I], _S),
     "knnag_pack_points": ([_V, _V, _V, _I, _I, _I, _V, _V], _I),
     "knnag_adjacency_bytes": ([_I, _I, _I, _I], _S),
@@ -107,6 +111,46 @@ def forward(q, p, f, sigma, R, K, points=None):
     _check(lib().knnag_forward(_p(q), _p(p), _p(f), _p(sigma), _p(R), B, Q, P, F, K, dt, _p(f_out), _p(w_out),
                                _p(dists), _p(idxs), _p(points), _p(ws), nb, _stream(q.device)))
     return f_out, w_out, dists, idxs
+
+
+def forward_precomputed(q, p, f, sigma, R, knn_idxs):
+    """knnag_forward_precomputed: returns (f_out, w_out, dists)."""
+    B, Q, P, F, K = q.shape[0], q.shape[1], p.shape[1], f.shape[2], knn_idxs.shape[2]
+    dt = _dtype(q)
+    o = dict(dtype=q.dtype, device=q.device)
+    f_out, w_out, dists = torch.empty(B, Q, F, **o), torch.empty(B, Q, K, **o), torch.empty(B, Q, K, **o)
+    nb = lib().knnag_variant_workspace_bytes(B, Q, P, dt)
+    ws = torch.empty(max(nb, 1), dtype=torch.uint8, device=q.device)
+    _check(lib().knnag_forward_precomputed(_p(q), _p(p), _p(f), _p(sigma), _p(R), _p(knn_idxs), B, Q, P, F, K, dt,
+                                           _p(f_out), _p(w_out), _p(dists), _p(ws), nb, _stream(q.device)))
+    return f_out, w_out, dists
+
+
+def forward_lookup(q, p, f, sigma, R, knn_table, K):
+    """knnag_forward_lookup: returns (f_out, w_out, dists, idxs)."""
+    B, Q, P, F = q.shape[0], q.shape[1], p.shape[1], f.shape[2]
+    dt = _dtype(q)
+    o = dict(dtype=q.dtype, device=q.device)
+    f_out, w_out, dists = torch.empty(B, Q, F, **o), torch.empty(B, Q, K, **o), torch.empty(B, Q, K, **o)
+    idxs = torch.empty(B, Q, K, dtype=torch.int64, device=q.device)
+    nb = lib().knnag_variant_workspace_bytes(B, Q, P, dt)
+    ws = torch.empty(max(nb, 1), dtype=torch.uint8, device=q.device)
+    _check(lib().knnag_forward_lookup(_p(q), _p(p), _p(f), _p(sigma), _p(R), _p(knn_table), knn_table.shape[1], B, Q,
+                                      P, F, K, dt, _p(f_out), _p(w_out), _p(dists), _p(idxs), _p(ws), nb,
+                                      _stream(q.device)))
+    return f_out, w_out, dists, idxs
+
+
+def forward_isotropic(q, p, f, sigma, K):
+    """knnag_forward_isotropic: returns (f_out, w_sum [B,Q,1], dists, idxs)."""
+    B, Q, P, F = q.shape[0], q.shape[1], p.shape[1], f.shape[2]
+    dt = _dtype(q)
+    o = dict(dtype=q.dtype, device=q.device)
+    f_out, w_sum, dists = torch.empty(B, Q, F, **o), torch.empty(B, Q, 1, **o), torch.empty(B, Q, K, **o)
+    idxs = torch.empty(B, Q, K, dtype=torch.int64, device=q.device)
+    _check(lib().knnag_forward_isotropic(_p(q), _p(p), _p(f), _p(sigma), sigma.shape[2], B, Q, P, F, K, dt,
+                                         _p(f_out), _p(w_sum), _p(dists), _p(idxs), _stream(q.device)))
+    return f_out, w_sum, dists, idxs
 
 
 def pack_points(p, sigma, R):

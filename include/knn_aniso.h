@@ -95,8 +95,9 @@ int knnag_forward(const void* q, const void* p, const void* f, const void* sigma
  * framework owns every device allocation): no workspace argument, no
  * allocation.  The scratch is one fixed 8 MiB device array inside the
  * library, held by every GPU that loads it until process exit; sizes whose
- * scratch would exceed it return KNNAG_ERR_SCRATCH_LIMIT (about B*P <= 60k
- * points and B*Q <= 500k queries).  The first call on each device looks the
+ * scratch would exceed it return KNNAG_ERR_SCRATCH_LIMIT (the scratch is
+ * about 130 bytes per point plus 8 bytes per query: up to ~60k points with
+ * few queries, or ~40k points with ~300k queries).  The first call on each device looks the
  * array's address up (cudaGetSymbolAddress) and should come before any
  * stream capture.  All calls share the array: calls that overlap on the GPU
  * race.  No counterpart in the reference.
@@ -104,6 +105,47 @@ int knnag_forward(const void* q, const void* p, const void* f, const void* sigma
 int knnag_forward_noalloc(const void* q, const void* p, const void* f, const void* sigma, const void* R,
                           int B, int Q, int P, int F, int K, int dtype,
                           void* f_out, void* w_out, void* dists, int64_t* idxs, void* stream);
+
+/* ----------------------------------------------------- forward variants */
+
+/* Bytes of scratch the variant entry points below need. */
+size_t knnag_variant_workspace_bytes(int B, int Q, int P, int dtype);
+
+/*
+ * Aggregation at caller-given neighbour indices knn_idxs [B,Q,K] int64
+ * (no search, no sorting): dists = key, w_out = exp(-key), f_out = sum_k
+ * w_k f[idx_k].  Replaces knn_precomputed_aggregate_aniso_forward
+ * (csrc/knn_aggregate.cpp:76-99, csrc/forward.cu:186-230, 398-450).  An index
+ * outside [0, P) contributes nothing (w = 0, dist = +inf).
+ */
+int knnag_forward_precomputed(const void* q, const void* p, const void* f, const void* sigma, const void* R,
+                              const int64_t* knn_idxs, int B, int Q, int P, int F, int K, int dtype,
+                              void* f_out, void* w_out, void* dists,
+                              void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Lookup variant: the Euclidean nearest point of each query (strict '<'
+ * scan, first index wins), then row `nearest` of knn_table [P, table_cols]
+ * int64 (shared by all batch elements; its first K entries, in table order,
+ * unsorted) with anisotropic weights.  Outputs as knnag_forward.
+ * Replaces knn_lookup_aggregate_aniso_forward (csrc/knn_aggregate.cpp:50-73,
+ * csrc/forward.cu:113-183, 341-395).
+ */
+int knnag_forward_lookup(const void* q, const void* p, const void* f, const void* sigma, const void* R,
+                         const int64_t* knn_table, int table_cols, int B, int Q, int P, int F, int K, int dtype,
+                         void* f_out, void* w_out, void* dists, int64_t* idxs,
+                         void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Isotropic forward: K nearest points by squared Euclidean distance (MinK
+ * rules), w_k = exp(-d_k * sigma[idx_k][0]) with sigma [B,P,sigma_cols],
+ * f_out = sum_k w_k f[idx_k], w_sum [B,Q,1] = sum_k w_k.  Replaces
+ * knn_aggregate_forward (csrc/knn_aggregate.cpp:5-23, csrc/forward.cu:5-53,
+ * 233-283).  Needs no workspace.
+ */
+int knnag_forward_isotropic(const void* q, const void* p, const void* f, const void* sigma, int sigma_cols,
+                            int B, int Q, int P, int F, int K, int dtype,
+                            void* f_out, void* w_sum, void* dists, int64_t* idxs, void* stream);
 
 /* ---------------------------------------------------------- adjoint index */
 

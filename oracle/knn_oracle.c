@@ -179,3 +179,118 @@ int oracle_num_threads(void) {
   return 1;
 #endif
 }
+
+/* ---------------------------------------------------------------- variants */
+
+/* Squared Euclidean distance of (x, y, z) in one of the candidate roundings:
+ *   0: fma(z,z, fma(x,x, y*y))   -- `x*x + y*y + z*z` (forward.cu:154)
+ *   1: fma(z,z, fma(y,y, x*x))   -- `d = 0; d += c*c` for c = x, y, z (forward.cu:32-36)
+ *   2: no contraction. */
+static inline float sq_dist3(int mode, float x, float y, float z) {
+  switch (mode) {
+    case 0: { float t = y * y; return fmaf(z, z, fmaf(x, x, t)); }
+    case 1: { float t = x * x; return fmaf(z, z, fmaf(y, y, t)); }
+    default: { float a = x * x, b = y * y, c = z * z; float ab = a + b; return ab + c; }
+  }
+}
+
+/* Aggregation at given neighbour indices (forward.cu:212-229): dists = key,
+ * w64 = exp(-key) in double, fout64 = sum_k w64 * f[idx] in k order.  An
+ * index outside [0, P) gives dist = +inf, w = 0. */
+void oracle_precomputed_f32(const float* q, const float* p, const float* f, const float* sigma, const float* R,
+                            const int64_t* idxs, int B, int Q, int P, int F, int K, float* dists, double* w64,
+                            double* fout64) {
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int b = 0; b < B; ++b)
+    for (int iq = 0; iq < Q; ++iq) {
+      int64_t bq = (int64_t)b * Q + iq;
+      const float* qv = q + bq * 3;
+      const float* pb = p + (int64_t)b * P * 3;
+      const float* sb = sigma + (int64_t)b * P * 3;
+      const float* Rb = R + (int64_t)b * P * 9;
+      const float* fb = f + (int64_t)b * P * F;
+      double* fo = fout64 + bq * F;
+      memset(fo, 0, sizeof(double) * (size_t)F);
+      for (int k = 0; k < K; ++k) {
+        int64_t i = idxs[bq * K + k];
+        if (i < 0 || i >= P) {
+          dists[bq * K + k] = INFINITY;
+          w64[bq * K + k] = 0.0;
+          continue;
+        }
+        float s = aniso_key(0, 0, qv, pb, sb, Rb, i);
+        double w = exp(-(double)s);
+        dists[bq * K + k] = s;
+        w64[bq * K + k] = w;
+        for (int c = 0; c < F; ++c) fo[c] += w * (double)fb[i * F + c];
+      }
+    }
+}
+
+/* Lookup variant (forward.cu:137-182): Euclidean nearest point with a strict
+ * '<' scan from 1e10 (first index wins ties; 0 when nothing is below 1e10),
+ * then the K neighbours table[nearest][k] (table [P,K], shared by all batch
+ * elements) in table order with the anisotropic key and weight. */
+void oracle_lookup_f32(const float* q, const float* p, const float* f, const float* sigma, const float* R,
+                       const int64_t* table, int B, int Q, int P, int F, int K, int sqmode, int64_t* idxs,
+                       float* dists, double* w64, double* fout64) {
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int b = 0; b < B; ++b)
+    for (int iq = 0; iq < Q; ++iq) {
+      int64_t bq = (int64_t)b * Q + iq;
+      const float* qv = q + bq * 3;
+      const float* pb = p + (int64_t)b * P * 3;
+      float best = 1e10f;
+      int64_t arg = 0;
+      for (int64_t i = 0; i < P; ++i) {
+        float x = qv[0] - pb[i * 3 + 0], y = qv[1] - pb[i * 3 + 1], z = qv[2] - pb[i * 3 + 2];
+        float d = sq_dist3(sqmode, x, y, z);
+        if (d < best) {
+          best = d;
+          arg = i;
+        }
+      }
+      for (int k = 0; k < K; ++k) idxs[bq * K + k] = table[arg * K + k];
+    }
+  oracle_precomputed_f32(q, p, f, sigma, R, idxs, B, Q, P, F, K, dists, w64, fout64);
+}
+
+/* Isotropic forward (forward.cu:18-52): MinK over squared Euclidean
+ * distances, then w = exp(-d * sigma[idx][0]) (sigma row stride S),
+ * f_out = sum w f[idx] in k order, wsum64 = sum of the weights. */
+void oracle_iso_f32(const float* q, const float* p, const float* f, const float* sigma, int B, int Q, int P, int F,
+                    int K, int S, int sqmode, int64_t* idxs, float* dists, double* wsum64, double* fout64) {
+#pragma omp parallel
+  {
+    float* keyrow = (float*)malloc(sizeof(float) * (size_t)P);
+    float* kk = (float*)malloc(sizeof(float) * (size_t)K);
+    int64_t* vv = (int64_t*)malloc(sizeof(int64_t) * (size_t)K);
+#pragma omp for collapse(2) schedule(dynamic, 16)
+    for (int b = 0; b < B; ++b)
+      for (int iq = 0; iq < Q; ++iq) {
+        int64_t bq = (int64_t)b * Q + iq;
+        const float* qv = q + bq * 3;
+        const float* pb = p + (int64_t)b * P * 3;
+        const float* fb = f + (int64_t)b * P * F;
+        for (int64_t i = 0; i < P; ++i) {
+          float x = qv[0] - pb[i * 3 + 0], y = qv[1] - pb[i * 3 + 1], z = qv[2] - pb[i * 3 + 2];
+          keyrow[i] = sq_dist3(sqmode, x, y, z);
+        }
+        int n = mink_select(keyrow, P, K, kk, vv);
+        double* fo = fout64 + bq * F;
+        memset(fo, 0, sizeof(double) * (size_t)F);
+        double ws = 0.0;
+        for (int k = 0; k < n; ++k) {
+          idxs[bq * K + k] = vv[k];
+          dists[bq * K + k] = kk[k];
+          double w = exp(-(double)kk[k] * (double)sigma[((int64_t)b * P + vv[k]) * S]);
+          ws += w;
+          for (int c = 0; c < F; ++c) fo[c] += w * (double)fb[vv[k] * F + c];
+        }
+        wsum64[bq] = ws;
+      }
+    free(keyrow);
+    free(kk);
+    free(vv);
+  }
+}

@@ -182,3 +182,68 @@ def eikonal_step(q, p, f, sigma, R, K, forward=plain_forward):
     loss = ((gq.norm(dim=-1) - 1.0) ** 2).mean()
     loss.backward()
     return loss.detach(), f_out.detach(), idxs
+
+
+# ----------------------------------------------------------------------------
+# Variants of the forward (reference csrc/forward.cu:5-53, 113-183, 186-230)
+# ----------------------------------------------------------------------------
+
+# Contraction order of the squared Euclidean distances of the lookup and
+# isotropic kernels (knn_oracle.c sq_dist3), pinned by tests/test_oracle_golden.py.
+LOOKUP_SQ_MODE = 0
+ISO_SQ_MODE = 1
+
+
+def _variant_lib():
+    L = lib()
+    if not hasattr(L, "_variants_ready"):
+        P = ctypes.c_void_p
+        I = ctypes.c_int
+        L.oracle_precomputed_f32.argtypes = [P] * 6 + [I] * 5 + [P, P, P]
+        L.oracle_lookup_f32.argtypes = [P] * 6 + [I] * 6 + [P, P, P, P]
+        L.oracle_iso_f32.argtypes = [P] * 4 + [I] * 7 + [P, P, P, P]
+        L._variants_ready = True
+    return L
+
+
+def precomputed_f32(q, p, f, sigma, R, idxs):
+    """(fout64, w64, dists f32) at given neighbour indices [B,Q,K]."""
+    q, p, f, sigma, R = map(_np32, (q, p, f, sigma, R))
+    idxs = np.ascontiguousarray(idxs.cpu().numpy() if isinstance(idxs, torch.Tensor) else idxs, dtype=np.int64)
+    B, Q, P, F = q.shape[0], q.shape[1], p.shape[1], f.shape[2]
+    K = idxs.shape[2]
+    d = np.empty((B, Q, K), np.float32)
+    w = np.empty((B, Q, K), np.float64)
+    fo = np.empty((B, Q, F), np.float64)
+    _variant_lib().oracle_precomputed_f32(_ptr(q), _ptr(p), _ptr(f), _ptr(sigma), _ptr(R), _ptr(idxs), B, Q, P, F, K,
+                                          _ptr(d), _ptr(w), _ptr(fo))
+    return fo, w, d
+
+
+def lookup_f32(q, p, f, sigma, R, table, mode=None):
+    """(fout64, w64, dists f32, idxs int64) of the lookup variant."""
+    q, p, f, sigma, R = map(_np32, (q, p, f, sigma, R))
+    table = np.ascontiguousarray(table.cpu().numpy() if isinstance(table, torch.Tensor) else table, dtype=np.int64)
+    B, Q, P, F = q.shape[0], q.shape[1], p.shape[1], f.shape[2]
+    K = table.shape[1]
+    idxs = np.empty((B, Q, K), np.int64)
+    d = np.empty((B, Q, K), np.float32)
+    w = np.empty((B, Q, K), np.float64)
+    fo = np.empty((B, Q, F), np.float64)
+    _variant_lib().oracle_lookup_f32(_ptr(q), _ptr(p), _ptr(f), _ptr(sigma), _ptr(R), _ptr(table), B, Q, P, F, K,
+                                     LOOKUP_SQ_MODE if mode is None else mode, _ptr(idxs), _ptr(d), _ptr(w), _ptr(fo))
+    return fo, w, d, idxs
+
+
+def iso_f32(q, p, f, sigma, K, mode=None):
+    """(fout64, wsum64 [B,Q,1], dists f32, idxs int64) of the isotropic forward;
+    sigma [B,P,S], component 0 is used."""
+    q, p, f, sigma = map(_np32, (q, p, f, sigma))
+    B, Q, P, F, S = q.shape[0], q.shape[1], p.shape[1], f.shape[2], sigma.shape[2]
+    idxs = np.empty((B, Q, K), np.int64)
+    d = np.empty((B, Q, K), np.float32)
+    ws = np.empty((B, Q, 1), np.float64)
+    fo = np.empty((B, Q, F), np.float64)
+    _variant_lib().oracle_iso_f32(_ptr(q), _ptr(p), _ptr(f), _ptr(sigma), B, Q, P, F, K, S,
+                                  ISO_SQ_MODE if mode is None else mode, _ptr(idxs), _ptr(d), _ptr(ws), _ptr(fo))
+    return fo, ws, d, idxs

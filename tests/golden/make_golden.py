@@ -80,17 +80,71 @@ def run_case(ref, tensors, K, seed):
     return rec
 
 
+def variant_cases():
+    """Fixtures of the reference's other forward ops (csrc/forward.cu:5-53,
+    113-183, 186-230): isotropic kNN, lookup through a neighbour table, and
+    aggregation at precomputed indices."""
+    out = []
+    g = torch.Generator().manual_seed(600)
+    _, t = W.make("small", B=2, Q=300, P=400, F=12, seed=41)
+    q, p, f, sigma, R = t
+    # precomputed: indices of the aniso kNN of another query set plus random ones
+    idx = torch.randint(0, 400, (2, 300, 9), generator=g)
+    out.append(("pre", dict(q=q, p=p, f=f, sigma=sigma, R=R, knn_idxs=idx, K=9)))
+    # lookup: table = the 10 Euclidean nearest points of every point of batch 0
+    d = ((p[0][:, None, :] - p[0][None, :, :]) ** 2).sum(-1)
+    table = torch.topk(d, 10, dim=-1, largest=False).indices
+    out.append(("lookup", dict(q=q, p=p, f=f, sigma=sigma, R=R, knn_table=table, K=10)))
+    # isotropic: sigma [B,P,1]
+    s1 = 0.5 + torch.rand(2, 400, 1, generator=g)
+    out.append(("iso", dict(q=q, p=p, f=f, sigma=s1.contiguous(), K=12)))
+    _, t = W.make("small", B=1, Q=200, P=64, F=4, seed=42)
+    q, p, f, sigma, R = t
+    out.append(("iso_kp", dict(q=q, p=p, f=f, sigma=sigma[..., :1].contiguous(), K=64)))
+    lt = W.lattice_ties(B=1, n_side=4, Q=64, F=4, seed=8)
+    out.append(("iso_ties", dict(q=lt[0], p=lt[1], f=lt[2], sigma=lt[3][..., :1].contiguous(), K=8)))
+    return out
+
+
+def run_variant(ref, name, c):
+    dev = lambda x: x.cuda().contiguous()
+    rec = {k: (v.numpy() if isinstance(v, torch.Tensor) else np.int64(v)) for k, v in c.items()}
+    if name == "pre":
+        o = ref.knn_precomputed_aggregate_aniso_forward(*[dev(c[k]) for k in ("q", "p", "f", "sigma", "R", "knn_idxs")],
+                                                        c["K"])
+        names = ("f_out", "w_out", "dists")
+    elif name == "lookup":
+        o = ref.knn_lookup_aggregate_aniso_forward(*[dev(c[k]) for k in ("q", "p", "f", "sigma", "R", "knn_table")],
+                                                   c["K"])
+        names = ("f_out", "w_out", "dists", "idxs")
+    else:
+        o = ref.knn_aggregate_forward(*[dev(c[k]) for k in ("q", "p", "f", "sigma")], c["K"])
+        names = ("f_out", "w_out", "dists", "idxs")
+    torch.cuda.synchronize()
+    for n, v in zip(names, o):
+        rec[n] = v.detach().cpu().numpy()
+    return rec
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.dirname(os.path.abspath(__file__)))
+    ap.add_argument("--only-variants", action="store_true")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
     ref = load_ref()
     for i, (name, t, K) in enumerate(cases()):
+        if a.only_variants:
+            break
         rec = run_case(ref, t, K, seed=500 + i)
         path = os.path.join(a.out, f"ref_{name}.npz")
         np.savez_compressed(path, **rec)
         print(f"{name}: {os.path.getsize(path)} bytes")
+    for name, c in variant_cases():
+        rec = run_variant(ref, name, c)
+        path = os.path.join(a.out, f"ref_var_{name}.npz")
+        np.savez_compressed(path, **rec)
+        print(f"var_{name}: {os.path.getsize(path)} bytes")
 
 
 if __name__ == "__main__":
