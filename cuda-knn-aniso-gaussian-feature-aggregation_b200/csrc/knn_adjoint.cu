@@ -246,6 +246,12 @@ struct QueryParams {
   T* dq;             // optional
   T* coef_out;       // optional (first order)
   T* dgfo;           // optional (second order)
+  // ragged first order (FP32): sizes and offsets from the segment table,
+  // records from the cloud set; gfo may be null (all ones).  Nothing is done
+  // when *status is nonzero (a table that failed validation).
+  const char* cs;
+  const void* segs;
+  const int* status;
 };
 
 template <typename T>
@@ -289,28 +295,52 @@ template <typename T>
 __global__ void __launch_bounds__(256, 3) query_order1_kernel(QueryParams<T> a) {
   constexpr int NG = 8;
   const int lane = threadIdx.x & 31;
-  const int BQ = a.B * a.Q, K = a.K, F = a.F, P = a.P;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
-  for (int bq = gw; bq < BQ; bq += nw) {
-    const int b = bq / a.Q;
-    const T qx = a.q[(int64_t)bq * 3 + 0], qy = a.q[(int64_t)bq * 3 + 1], qz = a.q[(int64_t)bq * 3 + 2];
-    const T* grow = a.gfo + (int64_t)bq * F;
-    const T* fb = a.f + (int64_t)b * P * F;
+  const int F = a.F;
+  const SegHeader* sh = static_cast<const SegHeader*>(a.segs);
+  if (sh && *a.status) return;
+  const int64_t BQ = sh ? sh->grad_rows : (int64_t)a.B * a.Q;
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (gridDim.x * (int64_t)blockDim.x) >> 5;
+  for (int64_t bq = gw; bq < BQ; bq += nw) {
+    // the query's cloud: records, features, sizes and first entry
+    int K, P;
+    int64_t e0;
+    const T* recb;
+    const T* fb;
+    if (sh) {
+      const SegDesc* sd = seg_descs(a.segs);
+      const SegDesc g = sd[seg_of_row(sd, sh->nseg, bq)];
+      const CloudDesc c = cloud_descs(a.cs)[g.cloud];
+      K = g.K;
+      P = c.P;
+      e0 = g.e_off + (bq - g.q_off) * K;
+      recb = reinterpret_cast<const T*>(a.cs + reinterpret_cast<const CloudSetHeader*>(a.cs)->rec_off) +
+             c.p_off * kRecLen;
+      fb = a.f + c.p_off * F;
+    } else {
+      const int64_t b = bq / a.Q;
+      K = a.K;
+      P = a.P;
+      e0 = bq * K;
+      recb = a.rec + b * a.P * kRecLen;
+      fb = a.f + b * a.P * F;
+    }
+    const T qx = a.q[bq * 3 + 0], qy = a.q[bq * 3 + 1], qz = a.q[bq * 3 + 2];
+    const T* grow = a.gfo ? a.gfo + bq * F : nullptr;
     T acc[3] = {T(0), T(0), T(0)};
     for (int k0 = 0; k0 < K; k0 += NG) {
       const int nk = min(NG, K - k0);
       int ik[NG];  // neighbour point index within the batch, -1 if none
 #pragma unroll
       for (int kk = 0; kk < NG; ++kk) {
-        const int64_t idx = kk < nk ? a.idxs[(int64_t)bq * K + k0 + kk] : -1;
+        const int64_t idx = kk < nk ? a.idxs[e0 + k0 + kk] : -1;
         ik[kk] = (idx >= 0 && idx < P) ? (int)idx : -1;
       }
       T part[NG];
 #pragma unroll
       for (int kk = 0; kk < NG; ++kk) part[kk] = T(0);
       for (int c = lane; c < F; c += 32) {
-        const T g = grow[c];
+        const T g = grow ? grow[c] : T(1);
 #pragma unroll
         for (int kk = 0; kk < NG; ++kk)
           if (ik[kk] >= 0) part[kk] = fma_rn(g, fb[(int64_t)ik[kk] * F + c], part[kk]);
@@ -329,12 +359,12 @@ __global__ void __launch_bounds__(256, 3) query_order1_kernel(QueryParams<T> a) 
       T c_own = part[0] + __shfl_xor_sync(0xffffffffu, part[0], 2);
       c_own += __shfl_xor_sync(0xffffffffu, c_own, 1);
       const int m_own = lane >> 2;
-      const int64_t e = (int64_t)bq * K + k0 + m_own;
+      const int64_t e = e0 + k0 + m_own;
       if ((lane & 3) == 0 && m_own < nk) {
         if (a.coef_out) a.coef_out[e] = c_own;
         const int64_t idx = a.idxs[e];
         if (idx >= 0 && idx < P) {
-          const T* rec = a.rec + ((int64_t)b * P + idx) * kRecLen;
+          const T* rec = recb + idx * kRecLen;
           Geo<T> geo;
           geometry(qx, qy, qz, rec, geo);
           const T w = a.w_in ? a.w_in[e] : geo.w;
@@ -350,9 +380,9 @@ __global__ void __launch_bounds__(256, 3) query_order1_kernel(QueryParams<T> a) 
 #pragma unroll
     for (int mm = 0; mm < 3; ++mm) acc[mm] = warp_sum(acc[mm]);
     if (lane == 0 && a.dq) {
-      a.dq[(int64_t)bq * 3 + 0] = acc[0];
-      a.dq[(int64_t)bq * 3 + 1] = acc[1];
-      a.dq[(int64_t)bq * 3 + 2] = acc[2];
+      a.dq[bq * 3 + 0] = acc[0];
+      a.dq[bq * 3 + 1] = acc[1];
+      a.dq[bq * 3 + 2] = acc[2];
     }
   }
 }
@@ -612,6 +642,29 @@ int launch_query(const QueryParams<T>& p, int order, cudaStream_t st) {
   note_launches(1);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
+
+}  // namespace
+
+// d(<gfo, f_out>)/dq of a ragged call (gfo null: all ones), weights
+// recomputed from idxs.  One warp per query row up to the table's total.
+int ragged_grad_q_impl(const char* cs, const void* segs, const float* q, const float* f, int F, const float* gfo,
+                       const int64_t* idxs, int64_t cap_q, float* dq, const int* status, cudaStream_t st) {
+  QueryParams<float> p{};
+  p.status = status;
+  p.gfo = gfo;
+  p.q = q;
+  p.f = f;
+  p.idxs = idxs;
+  p.F = F;
+  p.dq = dq;
+  p.cs = cs;
+  p.segs = segs;
+  query_order1_kernel<float><<<blocks_for(cap_q * 32, 256), 256, 0, st>>>(p);
+  note_launches(1);
+  return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
+}
+
+namespace {
 
 template <typename T, int ORDER>
 int launch_point_o(const PointParams<T>& p, cudaStream_t st) {

@@ -89,7 +89,8 @@ const char* knnag_status_string(int status) {
     case KNNAG_ERR_WORKSPACE: return "workspace too small or not 16-byte aligned";
     case KNNAG_ERR_TOO_LARGE: return "problem exceeds the 32-bit entry index range";
     case KNNAG_ERR_CUDA: return "CUDA launch failed";
-    case KNNAG_ERR_DEVICE: return "device-side error latched (a bounded wait gave up)";
+    case KNNAG_ERR_DEVICE:
+      return "device-side error latched (a bounded wait gave up, or a segment table failed validation)";
     case KNNAG_ERR_SCRATCH_LIMIT: return "problem needs more scratch than knnag_forward_noalloc's fixed 8 MiB array";
     default: return "unknown status";
   }

@@ -6,6 +6,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "knn_ragged.h"
+
 namespace knnag {
 
 template <typename T>
@@ -27,13 +29,20 @@ struct ExactParams {
   T* w_out;
   T* dists;
   int64_t* idxs;
+  // ragged calls (FP32): per-query sizes and offsets from the segment table,
+  // records from the cloud set.  List items are global query rows; without a
+  // list the kernel serves the queries of segments with K > 32.  Nothing is
+  // done when *status is nonzero (a table that failed validation).
+  const char* cs;
+  const void* segs;
+  const int* status;
 };
 
 struct SearchParams {
   const float* q;
   const int* perm_q;   // sorted position -> query index, per batch element
   const float* tinfo;  // per tile: box (6), key lower-bound factor mu, pad
-  int ntile;
+  int ntile;           // tiles per batch element (ragged: the most of any cloud)
   const float* pairs;  // pair-interleaved tiles [B][P_pad/2][32]
   const float* rec;    // per-point records [B*P*16]
   const float* f;
@@ -45,7 +54,13 @@ struct SearchParams {
   int64_t* idxs;
   int* status;
   int* flag_count;
-  int* flag_list;
+  int* flag_list;      // flagged queries: global query rows
+  // ragged calls: records, tiles and boxes come from the cloud set, sizes
+  // and offsets from the segment table; work items are taken in order from
+  // item_counter
+  const char* cs;
+  const void* segs;
+  int* item_counter;
 };
 
 // Search CTA: 4 warps; G warps split the points of one 32-query group.
@@ -99,6 +114,27 @@ int spatial_bits(int P);
 int launch_spatial_index(const float* q, const float* rec, int B, int Q, int P, int P_pad, char* ws, const FwdLayout& L,
                          cudaStream_t st);
 int launch_exclusive_scan(int* count, int n, int* out, cudaStream_t st);
+int launch_cloudset_index(char* cs, const CloudSetHeader& h, const CloudDesc* cd_dev, int max_p, int max_ntile,
+                          int* cnt, int* off, int* perm_p, cudaStream_t st);
+int launch_query_order(const float* q, const char* cs, const void* segs_dev, int cap_segs, int64_t cap_q,
+                       int cap_cells, int* cnt, int* off, int* perm_q, const int* status, cudaStream_t st);
+
+// Ragged forward workspace: [status, flag_count, item_counter] | flag_list
+// [cap_q] | perm_q [cap_q] | query cell counts / offsets [cap_cells (+1)],
+// cap_cells = cap_q + 8 * cap_segs (a segment of Q queries has at most
+// max(Q, 8) cells).
+struct RaggedLayout {
+  size_t status, flag_list, perm_q, cell_count, cell_offset, total;
+  int64_t cap_cells;
+};
+RaggedLayout ragged_layout(int cap_segs, int64_t cap_q);
+int launch_validate_segments(const char* cs, const void* segs, int cap_segs, int64_t cap_q, int64_t cap_e, int max_k,
+                             int ntile_cap, int qpc, int* status, cudaStream_t st);
+int ragged_forward_impl(const char* cs, const void* segs, const float* q, const float* f, int F, int cap_segs,
+                        int64_t cap_q, int64_t cap_e, int max_k, int ntile_cap, int splits, float* f_out, float* w_out,
+                        float* dists, int64_t* idxs, void* workspace, cudaStream_t st);
+int ragged_grad_q_impl(const char* cs, const void* segs, const float* q, const float* f, int F, const float* gfo,
+                       const int64_t* idxs, int64_t cap_q, float* dq, const int* status, cudaStream_t st);
 template <typename T>
 int launch_exact(const ExactParams<T>& a, cudaStream_t st);
 int variants_precomputed(const void* q, const void* f, const void* rec, const int64_t* idxs, int B, int Q, int P,

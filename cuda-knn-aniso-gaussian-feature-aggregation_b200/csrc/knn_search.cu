@@ -90,15 +90,49 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
   T* slot_k = skey + CH;
   int* slot_v = reinterpret_cast<int*>(slot_k + a.K);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int K = a.K, P = a.P, F = a.F;
-  const bool in_lanes = K <= 32;
-  const int64_t n_items = a.use_list ? (int64_t)(*a.list_count) : (int64_t)a.B * a.Q;
+  const int F = a.F;
+  const SegHeader* sh = static_cast<const SegHeader*>(a.segs);
+  if (sh && *a.status) return;
+  const int64_t n_items = a.use_list ? (int64_t)(*a.list_count)
+                                     : (sh ? sh->bigk_q : (int64_t)a.B * a.Q);
 
   for (int64_t item = blockIdx.x; item < n_items; item += gridDim.x) {
-    const int64_t bq = a.use_list ? (int64_t)a.list[item] : item;
-    const int64_t b = bq / a.Q;
+    // bq: the query's global row; e0: its first entry; b: batch element
+    // (uniform) -- records, features and sizes of its cloud
+    int64_t bq, e0, b = 0;
+    int K, P;
+    const T* recb;
+    const T* fb;
+    if (sh) {
+      const SegDesc* sd = seg_descs(a.segs);
+      int s;
+      if (a.use_list) {
+        bq = a.list[item];
+        s = seg_of_row(sd, sh->nseg, bq);
+      } else {
+        s = seg_of_bigk(sd, sh->nseg, item);
+        bq = sd[s].q_off + (item - sd[s].bigk_off);
+      }
+      const SegDesc g = sd[s];
+      const CloudDesc c = cloud_descs(a.cs)[g.cloud];
+      K = g.K;
+      P = c.P;
+      e0 = g.e_off + (bq - g.q_off) * K;
+      recb = reinterpret_cast<const T*>(a.cs + reinterpret_cast<const CloudSetHeader*>(a.cs)->rec_off) +
+             c.p_off * kRecLen;
+      fb = a.f + c.p_off * F;
+      if (K > a.K || K > P) continue;  // the host checked the table; never reached
+    } else {
+      bq = a.use_list ? (int64_t)a.list[item] : item;
+      b = bq / a.Q;
+      K = a.K;
+      P = a.P;
+      e0 = bq * K;
+      recb = a.rec + b * (int64_t)P * kRecLen;
+      fb = a.f + b * (int64_t)P * F;
+    }
+    const bool in_lanes = K <= 32;
     const T qx = a.q[bq * 3 + 0], qy = a.q[bq * 3 + 1], qz = a.q[bq * 3 + 2];
-    const T* recb = a.rec + b * (int64_t)P * kRecLen;
 
     int size = 0, max_idx = 0, my_v = -1;
     T max_key = T(0), my_k = T(0);
@@ -208,7 +242,7 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
       // in k order (csrc/forward.cu:43-52); keep w_k in slot_k
       const T* sg = a.iso_sigma + b * (int64_t)P * a.iso_stride;
       for (int k = tid; k < K; k += kReplayThreads) {
-        const int64_t e = bq * K + k;
+        const int64_t e = e0 + k;
         a.dists[e] = slot_k[k];
         a.idxs[e] = (int64_t)slot_v[k];
       }
@@ -223,7 +257,7 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
       }
     } else {
       for (int k = tid; k < K; k += kReplayThreads) {
-        const int64_t e = bq * K + k;
+        const int64_t e = e0 + k;
         a.dists[e] = slot_k[k];
         a.idxs[e] = (int64_t)slot_v[k];
         a.w_out[e] = weight_of(slot_k[k]);
@@ -232,7 +266,6 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
       for (int k = tid; k < K; k += kReplayThreads) slot_k[k] = weight_of(slot_k[k]);
       __syncthreads();
     }
-    const T* fb = a.f + b * (int64_t)P * F;
     for (int c = tid; c < F; c += kReplayThreads) {
       T acc = T(0);
       for (int k = 0; k < K; ++k) acc = fma_rn(fb[(int64_t)slot_v[k] * F + c], slot_k[k], acc);
@@ -349,8 +382,36 @@ __device__ __forceinline__ float merge_splits(const float* mk, const int* mv, in
   return next;
 }
 
+// One search work item: up to QPC queries of one batch element or segment,
+// all against one cloud.  Pointers are offset to the group already.
+struct SearchItem {
+  const float* q;      // query rows (group-local index)
+  const int* perm_q;   // sorted position -> group-local query index
+  const float* rec;    // the cloud's records
+  const float* pairs;  // the cloud's search tiles
+  const float* tinfo;  // the cloud's tile boxes
+  const float* f;      // the cloud's feature rows
+  float* f_out;        // rows of the group's queries
+  float* w_out;        // entries of the group's queries (K per query)
+  float* dists;
+  int64_t* idxs;
+  int64_t row0;        // global query row of group-local query 0
+  int Q, P, K, ntile, qblock;
+};
+
+// The two tile-buffer mbarriers of a search CTA.
+__device__ __forceinline__ uint64_t* search_barriers(unsigned char* smem, size_t region_a) {
+  return reinterpret_cast<uint64_t*>(smem + region_a + (size_t)kQueueCap * kSearchThreads * 8 +
+                                     2 * (size_t)kSearchThreads * 4);
+}
+
+// Search + aggregation of one work item.  The mbarriers are initialised by
+// the kernel; uses[buf] counts the phases buffer buf has completed so far
+// (a persistent CTA runs many items on the same barriers).  Returns false
+// when a tile copy timed out (status flagged; the CTA must stop).
 template <int KMAX, int G>
-__global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f32_kernel(SearchParams a) {
+__device__ __forceinline__ bool search_item(const SearchParams& a, const SearchItem& it, unsigned char* smem,
+                                            int ntp_cap, uint32_t (&uses)[2]) {
   constexpr int L = KMAX + 1;
   constexpr int QPC = 32 * (4 / G);
   constexpr int PPT = kTilePoints / 2;  // pairs per tile
@@ -359,17 +420,16 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
   constexpr size_t RB = search_region_b_bytes();
   constexpr size_t kMerge = search_merge_bytes(KMAX, G);
 
-  extern __shared__ __align__(128) unsigned char smem[];
   unsigned char* regA = smem;
   float* qk = reinterpret_cast<float*>(smem + RA);
   int* qv = reinterpret_cast<int*>(qk + kQueueCap * kSearchThreads);
   float* tau_share = reinterpret_cast<float*>(qv + kQueueCap * kSearchThreads);  // [2][128]
   uint64_t* full = reinterpret_cast<uint64_t*>(tau_share + 2 * kSearchThreads);
   // region C: per-tile lower bounds (sorted), visit order, query bookkeeping
-  const int NTP = search_tiles_pow2(a.ntile);
+  const int NTP = search_tiles_pow2(it.ntile);
   float* lbk = reinterpret_cast<float*>(smem + RA + RB);
-  int* lbt = reinterpret_cast<int*>(lbk + NTP);
-  int* qorig = lbt + NTP;                                    // [QPC] original query index (-1: none)
+  int* lbt = reinterpret_cast<int*>(lbk + ntp_cap);
+  int* qorig = lbt + ntp_cap;                                // [QPC] original query index (-1: none)
   float* qbox = reinterpret_cast<float*>(qorig + QPC);       // [4 warps][6]
   volatile int* s_nvisit = reinterpret_cast<volatile int*>(qbox + 24);
   // phase-2 views of region A
@@ -384,16 +444,14 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int split = warp % G, grp = warp / G;
   const int lq = grp * 32 + lane;
-  const int b = blockIdx.y;
-  const int sp = blockIdx.x * QPC + lq;  // position in the spatial order
-  const bool valid = sp < a.Q;
-  const int qi = a.perm_q[(int64_t)b * a.Q + (valid ? sp : a.Q - 1)];
-  const int64_t bq = (int64_t)b * a.Q + qi;
-  const int K = a.K, P = a.P;
+  const int sp = it.qblock * QPC + lq;  // position in the spatial order
+  const bool valid = sp < it.Q;
+  const int qi = it.perm_q[valid ? sp : it.Q - 1];
+  const int K = it.K, P = it.P;
 
-  const float qx = a.q[bq * 3 + 0], qy = a.q[bq * 3 + 1], qz = a.q[bq * 3 + 2];
+  const float qx = it.q[(int64_t)qi * 3 + 0], qy = it.q[(int64_t)qi * 3 + 1], qz = it.q[(int64_t)qi * 3 + 2];
   const float2 qx2 = make_float2(qx, qx), qy2 = make_float2(qy, qy), qz2 = make_float2(qz, qz);
-  const float* recb = a.rec + (int64_t)b * P * kRecLen;
+  const float* recb = it.rec;
   if (split == 0) qorig[lq] = valid ? qi : -1;
 
   // MinK's fill phase stores points 0..K-1 whatever their key: a NaN there
@@ -427,10 +485,10 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
     bmin[c] = fminf(fminf(qbox[c], qbox[6 + c]), fminf(qbox[12 + c], qbox[18 + c]));
     bmax[c] = fmaxf(fmaxf(qbox[3 + c], qbox[9 + c]), fmaxf(qbox[15 + c], qbox[21 + c]));
   }
-  const float* tinfo_b = a.tinfo + (int64_t)b * a.ntile * 8;
+  const float* tinfo_b = it.tinfo;
   for (int t = tid; t < NTP; t += kSearchThreads) {
     float lb = INFINITY;
-    if (t < a.ntile) {
+    if (t < it.ntile) {
       const float* ti = tinfo_b + t * 8;
       float d2 = 0.f;
 #pragma unroll
@@ -476,15 +534,9 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
   float tau = INFINITY, tie_key = INFINITY;
   int qn = 0;
 
-  const int ntile = a.ntile;
+  const int ntile = it.ntile;
   const bool seed = G > 1 && ntile > kSeedTiles;
-  const float* pairs_b = a.pairs + (int64_t)b * (a.P_pad / 2) * kPairFloats;
-  if (tid == 0) {
-    mbar_init(&full[0], 1);
-    mbar_init(&full[1], 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
+  const float* pairs_b = it.pairs;
   // visit position v reads tile lbt[v] into buffer v & 1
   auto issue = [&](int v) {
     const int buf = v & 1;
@@ -502,14 +554,16 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
   };
   if (tid == 0) {
     *s_nvisit = 0;
+    fence_proxy_async_smem();  // region A was last written by generic stores
     for (int v = 0; v < 2; ++v)
       if (decide(v, INFINITY)) issue(v);
   }
   __syncthreads();
 
-  for (int t = 0; t < *s_nvisit; ++t) {
+  int t = 0;
+  for (; t < *s_nvisit; ++t) {
     const int buf = t & 1;
-    const bool ok = mbar_wait_bounded(&full[buf], (t >> 1) & 1);
+    const bool ok = mbar_wait_bounded(&full[buf], (uses[buf] + (t >> 1)) & 1);
     const float4* tp = reinterpret_cast<const float4*>(regA + buf * kTileBytes) + split * PPS * 8;
 #pragma unroll 2
     for (int m = 0; m < PPS; ++m) {
@@ -539,10 +593,10 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
     if (abort) {
       if (tid == 0) {
         atomicOr(a.status, kStatusWaitTimeout);
-        mbar_wait_bounded(&full[buf], (t >> 1) & 1);
-        if (*s_nvisit > t + 1) mbar_wait_bounded(&full[buf ^ 1], ((t + 1) >> 1) & 1);
+        mbar_wait_bounded(&full[buf], (uses[buf] + (t >> 1)) & 1);
+        if (*s_nvisit > t + 1) mbar_wait_bounded(&full[buf ^ 1], (uses[buf ^ 1] + ((t + 1) >> 1)) & 1);
       }
-      return;
+      return false;
     }
     if (seed && t == kSeedTiles - 1) {
       // Both tile buffers are free (the next copies are deferred until now):
@@ -606,6 +660,9 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
     }
   }
 
+  uses[0] += (t + 1) >> 1;
+  uses[1] += t >> 1;
+
   // ---- merge the G split lists; region A is free (no copy in flight, all
   // tile reads ended before the last barrier).
   float fl_tie = tie_key;
@@ -646,7 +703,7 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
     out_f[lq] = (fl || !valid) ? 1 : 0;
     if (valid && fl) {
       const int pos = atomicAdd(a.flag_count, 1);
-      a.flag_list[pos] = (int)bq;
+      a.flag_list[pos] = (int)(it.row0 + qi);
     }
   }
   __syncthreads();
@@ -654,21 +711,20 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
   // ---- epilogue: dists / idxs / w_out, then f_out = sum_k w_k f[idx_k]
   // accumulated in k order with fma, 128-bit gathers of f rows.  Rows go to
   // the queries' original positions.
-  const int64_t qrow0 = (int64_t)b * a.Q;
-  for (int it = tid; it < QPC * K; it += kSearchThreads) {
-    const int l = it / K, k = it - l * K;
+  for (int x = tid; x < QPC * K; x += kSearchThreads) {
+    const int l = x / K, k = x - l * K;
     if (out_f[l]) continue;
-    const int64_t e = (qrow0 + qorig[l]) * K + k;
-    a.dists[e] = out_k[l * L + k];
-    a.idxs[e] = (int64_t)out_i[l * L + k];
-    a.w_out[e] = out_w[l * L + k];
+    const int64_t e = (int64_t)qorig[l] * K + k;
+    it.dists[e] = out_k[l * L + k];
+    it.idxs[e] = (int64_t)out_i[l * L + k];
+    it.w_out[e] = out_w[l * L + k];
   }
   const int F = a.F;
-  const float* fb = a.f + (int64_t)b * P * F;
+  const float* fb = it.f;
   if (a.vec4) {
     const int C4 = F >> 2;
-    for (int it = tid; it < QPC * C4; it += kSearchThreads) {
-      const int l = it / C4, c = it - l * C4;
+    for (int x = tid; x < QPC * C4; x += kSearchThreads) {
+      const int l = x / C4, c = x - l * C4;
       if (out_f[l]) continue;
       float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
       for (int k = 0; k < K; ++k) {
@@ -680,17 +736,110 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
         acc.z = __fmaf_rn(v.z, w, acc.z);
         acc.w = __fmaf_rn(v.w, w, acc.w);
       }
-      reinterpret_cast<float4*>(a.f_out + (qrow0 + qorig[l]) * F)[c] = acc;
+      reinterpret_cast<float4*>(it.f_out + (int64_t)qorig[l] * F)[c] = acc;
     }
   } else {
-    for (int it = tid; it < QPC * F; it += kSearchThreads) {
-      const int l = it / F, c = it - l * F;
+    for (int x = tid; x < QPC * F; x += kSearchThreads) {
+      const int l = x / F, c = x - l * F;
       if (out_f[l]) continue;
       float acc = 0.f;
       for (int k = 0; k < K; ++k)
         acc = __fmaf_rn(__ldg(fb + (int64_t)out_i[l * L + k] * F + c), out_w[l * L + k], acc);
-      a.f_out[(qrow0 + qorig[l]) * F + c] = acc;
+      it.f_out[(int64_t)qorig[l] * F + c] = acc;
     }
+  }
+  return true;
+}
+
+template <int KMAX, int G>
+__global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f32_kernel(SearchParams a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* full = search_barriers(smem, search_region_a_bytes(KMAX, G));
+  if (threadIdx.x == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const int64_t b = blockIdx.y;
+  SearchItem it;
+  it.q = a.q + b * a.Q * 3;
+  it.perm_q = a.perm_q + b * a.Q;
+  it.rec = a.rec + b * a.P * kRecLen;
+  it.pairs = a.pairs + b * (a.P_pad / 2) * kPairFloats;
+  it.tinfo = a.tinfo + b * a.ntile * 8;
+  it.f = a.f + b * a.P * a.F;
+  it.f_out = a.f_out + b * a.Q * a.F;
+  it.w_out = a.w_out + b * a.Q * a.K;
+  it.dists = a.dists + b * a.Q * a.K;
+  it.idxs = a.idxs + b * a.Q * a.K;
+  it.row0 = b * a.Q;
+  it.Q = a.Q;
+  it.P = a.P;
+  it.K = a.K;
+  it.ntile = a.ntile;
+  it.qblock = blockIdx.x;
+  uint32_t uses[2] = {0u, 0u};
+  search_item<KMAX, G>(a, it, smem, search_tiles_pow2(a.ntile), uses);
+}
+
+// Ragged search: a persistent CTA takes work items in order from a counter
+// until the segment table's items run out.  Item i belongs to the last
+// segment whose item_off <= i; its queries are that segment's sorted
+// positions [(i - item_off) * QPC, ...).
+template <int KMAX, int G>
+__global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_ragged_kernel(SearchParams a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ int s_item;
+  if (*a.status) return;  // the table failed validation
+  uint64_t* full = search_barriers(smem, search_region_a_bytes(KMAX, G));
+  if (threadIdx.x == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const SegHeader* sh = static_cast<const SegHeader*>(a.segs);
+  const SegDesc* sd = seg_descs(a.segs);
+  const CloudSetHeader* ch = reinterpret_cast<const CloudSetHeader*>(a.cs);
+  const CloudDesc* cd = cloud_descs(a.cs);
+  const float* crec = reinterpret_cast<const float*>(a.cs + ch->rec_off);
+  const float* cpairs = reinterpret_cast<const float*>(a.cs + ch->pairs_off);
+  const float* ctinfo = reinterpret_cast<const float*>(a.cs + ch->tinfo_off);
+  const int nseg = sh->nseg, n_items = sh->n_items;
+  const int ntp_cap = search_tiles_pow2(a.ntile);
+  constexpr int QPC = 32 * (4 / G);
+  uint32_t uses[2] = {0u, 0u};
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(a.item_counter, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= n_items) break;
+    const SegDesc g = sd[seg_of_item(sd, nseg, item)];
+    const CloudDesc c = cd[g.cloud];
+    if (g.K < 1 || g.K > KMAX || g.K > c.P || c.ntile > a.ntile || sh->qpc != QPC) {
+      if (threadIdx.x == 0) atomicOr(a.status, kStatusBadTable);
+    } else {
+      SearchItem it;
+      it.q = a.q + g.q_off * 3;
+      it.perm_q = a.perm_q + g.q_off;
+      it.rec = crec + c.p_off * kRecLen;
+      it.pairs = cpairs + c.tile_off * (kTilePoints / 2) * kPairFloats;
+      it.tinfo = ctinfo + c.tile_off * 8;
+      it.f = a.f + c.p_off * a.F;
+      it.f_out = a.f_out + g.q_off * a.F;
+      it.w_out = a.w_out + g.e_off;
+      it.dists = a.dists + g.e_off;
+      it.idxs = a.idxs + g.e_off;
+      it.row0 = g.q_off;
+      it.Q = g.Q;
+      it.P = c.P;
+      it.K = g.K;
+      it.ntile = c.ntile;
+      it.qblock = item - g.item_off;
+      if (!search_item<KMAX, G>(a, it, smem, ntp_cap, uses)) break;
+    }
+    __syncthreads();  // the next item reuses shared memory (and s_item)
   }
 }
 
@@ -729,6 +878,41 @@ int launch_search_t(const SearchParams& a, cudaStream_t st) {
   profile_end(st);
   note_launches(1);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
+}
+
+template <int KMAX, int G>
+int launch_search_ragged_t(const SearchParams& a, int64_t cap_items, cudaStream_t st) {
+  const size_t smem = search_smem_bytes(KMAX, G) + search_region_c_bytes(a.ntile, G);
+  if (smem > 227 * 1024) return KNNAG_ERR_TOO_LARGE;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  static int attr_set[64] = {0};
+  if (dev >= 0 && dev < 64 && attr_set[dev] < (int)smem) {
+    if (cudaFuncSetAttribute(search_ragged_kernel<KMAX, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+      return KNNAG_ERR_CUDA;
+    attr_set[dev] = (int)smem;
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_ragged_kernel<KMAX, G>, kSearchThreads, smem) !=
+          cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  int64_t grid = (int64_t)num_sms(dev) * per_sm;
+  if (grid > cap_items) grid = cap_items;
+  if (grid < 1) grid = 1;
+  profile_begin(st);
+  search_ragged_kernel<KMAX, G><<<(unsigned)grid, kSearchThreads, smem, st>>>(a);
+  profile_end(st);
+  note_launches(1);
+  return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
+}
+
+template <int KMAX>
+int launch_search_ragged_k(const SearchParams& a, int G, int64_t cap_items, cudaStream_t st) {
+  if (G == 1) return launch_search_ragged_t<KMAX, 1>(a, cap_items, st);
+  if (G == 2) return launch_search_ragged_t<KMAX, 2>(a, cap_items, st);
+  return launch_search_ragged_t<KMAX, 4>(a, cap_items, st);
 }
 
 template <int KMAX>
@@ -901,6 +1085,97 @@ int forward_impl(const void* q, const void* p, const void* f, const void* sigma,
   // Exact MinK replay of the flagged queries (count read on the device).
   ExactParams<float> e{(const float*)q, (const float*)rec, (const float*)f, nullptr, nullptr, 0, B, Q, P, F, K, 1,
                        flag_list, flag_count, (float*)f_out, (float*)w_out, (float*)dists, idxs};
+  return launch_exact<float>(e, st);
+}
+
+RaggedLayout ragged_layout(int cap_segs, int64_t cap_q) {
+  RaggedLayout L{};
+  L.cap_cells = cap_q + 8 * (int64_t)cap_segs;
+  size_t off = 0;
+  L.status = off;
+  off += 256;
+  L.flag_list = off;
+  off += align256((size_t)cap_q * 4);
+  L.perm_q = off;
+  off += align256((size_t)cap_q * 4);
+  L.cell_count = off;
+  off += align256((size_t)L.cap_cells * 4);
+  L.cell_offset = off;
+  off += align256(((size_t)L.cap_cells + 1) * 4);
+  L.total = off;
+  return L;
+}
+
+// Ragged forward: validate the table, sort every segment's queries, one
+// persistent search launch over all segments with K <= 32, exact replay of
+// the flagged queries, and the exact kernel for segments with K > 32.
+int ragged_forward_impl(const char* cs, const void* segs, const float* q, const float* f, int F, int cap_segs,
+                        int64_t cap_q, int64_t cap_e, int max_k, int ntile_cap, int splits, float* f_out, float* w_out,
+                        float* dists, int64_t* idxs, void* workspace, cudaStream_t st) {
+  const RaggedLayout L = ragged_layout(cap_segs, cap_q);
+  char* ws = static_cast<char*>(workspace);
+  int* status = reinterpret_cast<int*>(ws + L.status);
+  int* flag_count = status + 1;
+  int* item_counter = status + 2;
+  int* flag_list = reinterpret_cast<int*>(ws + L.flag_list);
+  int* perm_q = reinterpret_cast<int*>(ws + L.perm_q);
+  const int G = splits;
+  const int qpc = 32 * (4 / G);
+  if (cudaMemsetAsync(status, 0, 4 * sizeof(int), st) != cudaSuccess) return KNNAG_ERR_CUDA;
+  int rc = launch_validate_segments(cs, segs, cap_segs, cap_q, cap_e, max_k, ntile_cap, qpc, status, st);
+  if (rc) return rc;
+  rc = launch_query_order(q, cs, segs, cap_segs, cap_q, (int)L.cap_cells, reinterpret_cast<int*>(ws + L.cell_count),
+                          reinterpret_cast<int*>(ws + L.cell_offset), perm_q, status, st);
+  if (rc) return rc;
+  const int ks = max_k < 32 ? max_k : 32;
+  SearchParams sp{};
+  sp.q = q;
+  sp.perm_q = perm_q;
+  sp.ntile = ntile_cap;
+  sp.f = f;
+  sp.B = 1;
+  sp.F = F;
+  sp.K = ks;
+  sp.vec4 = (F % 4 == 0) && ((uintptr_t)f % 16 == 0) && ((uintptr_t)f_out % 16 == 0);
+  sp.f_out = f_out;
+  sp.w_out = w_out;
+  sp.dists = dists;
+  sp.idxs = idxs;
+  sp.status = status;
+  sp.flag_count = flag_count;
+  sp.flag_list = flag_list;
+  sp.cs = cs;
+  sp.segs = segs;
+  sp.item_counter = item_counter;
+  const int64_t cap_items = cap_q / qpc + cap_segs;
+  if (ks <= 8)
+    rc = launch_search_ragged_k<8>(sp, G, cap_items, st);
+  else if (ks <= 16)
+    rc = launch_search_ragged_k<16>(sp, G, cap_items, st);
+  else
+    rc = launch_search_ragged_k<32>(sp, G, cap_items, st);
+  if (rc) return rc;
+  ExactParams<float> e{};
+  e.q = q;
+  e.f = f;
+  e.B = 1;
+  e.Q = (int)(cap_q < (1 << 30) ? cap_q : (1 << 30));
+  e.F = F;
+  e.K = ks;
+  e.use_list = 1;
+  e.list = flag_list;
+  e.list_count = flag_count;
+  e.f_out = f_out;
+  e.w_out = w_out;
+  e.dists = dists;
+  e.idxs = idxs;
+  e.cs = cs;
+  e.segs = segs;
+  e.status = status;
+  rc = launch_exact<float>(e, st);
+  if (rc || max_k <= 32) return rc;
+  e.K = max_k;
+  e.use_list = 0;
   return launch_exact<float>(e, st);
 }
 

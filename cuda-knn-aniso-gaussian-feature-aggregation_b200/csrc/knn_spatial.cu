@@ -44,16 +44,54 @@ __device__ __forceinline__ uint32_t cell_of(float x, float y, float z, const flo
   return spread3(c[0]) | (spread3(c[1]) << 1) | (spread3(c[2]) << 2);
 }
 
-// Per batch element: bounding box of its points, bnd[b] = {min xyz, max xyz}.
-__global__ void __launch_bounds__(512) point_bounds_kernel(const float* __restrict__ rec, int P, float* __restrict__ bnd) {
+// Element groups of a counting sort: the batch elements of a uniform batch
+// (group g = elements [g*n, (g+1)*n), cells [g*8^bits, ...)), the clouds of
+// a cloud set, or the segments of a segment table (whose bounds are their
+// cloud's).  Positions of group g in the sorted order start where its first
+// element does, because the scan runs over [group][cell].
+struct GroupRange {
+  int64_t start;
+  int n, cell_off, bits, bnd;
+};
+struct GroupMap {
+  int n, bits;               // uniform batches
+  const CloudDesc* clouds;   // cloud set (points)
+  const SegDesc* segs;       // segment table (queries)
+  const SegHeader* seg_hdr;  // live segment count
+  const char* cs;            // cloud set whose bounds the segments use
+  const int* status;         // segments: nothing is done once this is nonzero
+};
+// Bounds array of a map: the cloud set's own for segments, else `bnd`.
+__device__ __forceinline__ const float* group_bounds(const GroupMap& m, const float* bnd) {
+  return m.cs ? reinterpret_cast<const float*>(m.cs + reinterpret_cast<const CloudSetHeader*>(m.cs)->bnd_off) : bnd;
+}
+__device__ __forceinline__ bool group_range(const GroupMap& m, int g, GroupRange& r) {
+  if (m.segs) {
+    if ((m.status && *m.status) || g >= m.seg_hdr->nseg) return false;
+    const SegDesc& s = m.segs[g];
+    r = GroupRange{s.q_off, s.Q, s.qcell_off, s.qbits, s.cloud};
+  } else if (m.clouds) {
+    const CloudDesc& c = m.clouds[g];
+    r = GroupRange{c.p_off, c.P, c.cell_off, c.bits, g};
+  } else {
+    r = GroupRange{(int64_t)g * m.n, m.n, g << (3 * m.bits), m.bits, g};
+  }
+  return true;
+}
+
+// Per group of points: bounding box, bnd[g] = {min xyz, max xyz}.
+__global__ void __launch_bounds__(512) point_bounds_kernel(const float* __restrict__ rec, GroupMap m,
+                                                           float* __restrict__ bnd) {
   __shared__ float red[6][16];
   const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  GroupRange r;
+  group_range(m, b, r);
   float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-  for (int i = tid; i < P; i += blockDim.x) {
-    const float* r = rec + ((int64_t)b * P + i) * kRecLen;
+  for (int i = tid; i < r.n; i += blockDim.x) {
+    const float* rr = rec + (r.start + i) * kRecLen;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const float v = -r[kNPX + a];
+      const float v = -rr[kNPX + a];
       mn[a] = fminf(mn[a], v);
       mx[a] = fmaxf(mx[a], v);
     }
@@ -78,58 +116,70 @@ __global__ void __launch_bounds__(512) point_bounds_kernel(const float* __restri
   }
 }
 
-// Cell histogram of points (from records) or queries (from q).
-__global__ void cell_count_kernel(const float* __restrict__ xyz, int stride, int negate, int n_per_b, int B,
-                                  const float* __restrict__ bnd, int bits, int* __restrict__ count) {
-  const int cells = 1 << (3 * bits);
-  const int n = B * n_per_b;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int b = i / n_per_b;
-    const float* v = xyz + (int64_t)i * stride;
-    const float s = negate ? -1.f : 1.f;
-    const uint32_t c = cell_of(s * v[0], s * v[1], s * v[2], bnd + b * 8, bits);
-    atomicAdd(&count[b * cells + (int)c], 1);
+// Cell histogram of the elements of group blockIdx.y (points from records,
+// queries from q).
+__global__ void cell_count_kernel(const float* __restrict__ xyz, int stride, int negate, GroupMap m,
+                                  const float* __restrict__ bnd, int* __restrict__ count) {
+  GroupRange r;
+  if (!group_range(m, blockIdx.y, r)) return;
+  const float s = negate ? -1.f : 1.f;
+  const float* gb = group_bounds(m, bnd) + r.bnd * 8;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n; i += gridDim.x * blockDim.x) {
+    const float* v = xyz + (r.start + i) * stride;
+    const uint32_t c = cell_of(s * v[0], s * v[1], s * v[2], gb, r.bits);
+    atomicAdd(&count[r.cell_off + (int)c], 1);
   }
 }
 
-// perm[offset[cell] + rank] = index within the batch element (positions of
-// batch b lie in [b*n_per_b, (b+1)*n_per_b) because the scan runs over
-// [b][cell]).
-__global__ void cell_scatter_kernel(const float* __restrict__ xyz, int stride, int negate, int n_per_b, int B,
-                                    const float* __restrict__ bnd, int bits, const int* __restrict__ offset,
+// perm[offset[cell] + rank] = index within the group.
+__global__ void cell_scatter_kernel(const float* __restrict__ xyz, int stride, int negate, GroupMap m,
+                                    const float* __restrict__ bnd, const int* __restrict__ offset,
                                     int* __restrict__ cursor, int* __restrict__ perm) {
-  const int cells = 1 << (3 * bits);
-  const int n = B * n_per_b;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int b = i / n_per_b;
-    const float* v = xyz + (int64_t)i * stride;
-    const float s = negate ? -1.f : 1.f;
-    const int c = b * cells + (int)cell_of(s * v[0], s * v[1], s * v[2], bnd + b * 8, bits);
-    perm[offset[c] + atomicAdd(&cursor[c], 1)] = i - b * n_per_b;
+  GroupRange r;
+  if (!group_range(m, blockIdx.y, r)) return;
+  const float s = negate ? -1.f : 1.f;
+  const float* gb = group_bounds(m, bnd) + r.bnd * 8;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n; i += gridDim.x * blockDim.x) {
+    const float* v = xyz + (r.start + i) * stride;
+    const int c = r.cell_off + (int)cell_of(s * v[0], s * v[1], s * v[2], gb, r.bits);
+    perm[offset[c] + atomicAdd(&cursor[c], 1)] = i;
   }
 }
 
-// Pair-interleaved tiles in sorted order; field kRecPad carries the original
-// point index (int bits), -1 for padding (whose sigma is NaN).
-__global__ void pack_pairs_sorted_kernel(const float* __restrict__ rec, const int* __restrict__ perm, int B, int P,
-                                         int P_pad, float* __restrict__ pairs) {
-  const int64_t total = (int64_t)B * P_pad * kRecLen;
+// Point groups of the tile kernels: uniform (group b: records [b*P, ...),
+// tiles [b*ntile, ...)) or the clouds of a cloud set.
+struct TileGroup {
+  int64_t p0, t0;
+  int P, ntile;
+};
+__device__ __forceinline__ TileGroup tile_group(const CloudDesc* cd, int b, int P, int ntile) {
+  if (cd) return TileGroup{cd[b].p_off, cd[b].tile_off, cd[b].P, cd[b].ntile};
+  return TileGroup{(int64_t)b * P, (int64_t)b * ntile, P, ntile};
+}
+
+// Pair-interleaved tiles of group blockIdx.y in sorted order; field kRecPad
+// carries the original point index (int bits), -1 for padding (whose sigma
+// is NaN).
+__global__ void pack_pairs_sorted_kernel(const float* __restrict__ rec, const int* __restrict__ perm,
+                                         const CloudDesc* __restrict__ cd, int P, int ntile,
+                                         float* __restrict__ pairs) {
+  const TileGroup g = tile_group(cd, blockIdx.y, P, ntile);
+  const int64_t total = (int64_t)g.ntile * kTilePoints * kRecLen;
+  float* out = pairs + g.t0 * kTilePoints * kRecLen;
   for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < total; o += (int64_t)gridDim.x * blockDim.x) {
     const int half = (int)(o & 1);
     const int field = (int)((o >> 1) & (kRecLen - 1));
-    const int64_t pair = o >> 5;
-    const int64_t b = pair / (P_pad / 2);
-    const int64_t pos = 2 * (pair - b * (P_pad / 2)) + half;
+    const int64_t pos = 2 * (o >> 5) + half;
     float v;
-    if (pos < P) {
-      const int i = perm[b * P + pos];
-      v = field == kRecPad ? __int_as_float(i) : rec[(b * P + i) * kRecLen + field];
+    if (pos < g.P) {
+      const int i = perm[g.p0 + pos];
+      v = field == kRecPad ? __int_as_float(i) : rec[(g.p0 + i) * kRecLen + field];
     } else if (field == kRecPad) {
       v = __int_as_float(-1);
     } else {
       v = (field == kS0 || field == kS1 || field == kS2) ? __int_as_float(0x7fc00000) : 0.0f;
     }
-    pairs[o] = v;
+    out[o] = v;
   }
 }
 
@@ -149,21 +199,22 @@ __device__ double sym3_min_eig(double a00, double a11, double a22, double a01, d
   return qm + 2.0 * p * cos(phi + 2.0943951023931957);  // + 2 pi / 3
 }
 
-// tinfo[(b*ntile + t)*8] = {min xyz, max xyz, mu, 0}; one warp per tile.
-__global__ void tile_info_kernel(const float* __restrict__ rec, const int* __restrict__ perm, int B, int P, int ntile,
-                                 float* __restrict__ tinfo) {
+// tinfo[(tile of group blockIdx.y)*8] = {min xyz, max xyz, mu, 0}; one warp
+// per tile.
+__global__ void tile_info_kernel(const float* __restrict__ rec, const int* __restrict__ perm,
+                                 const CloudDesc* __restrict__ cd, int P, int ntile, float* __restrict__ tinfo) {
+  const TileGroup g = tile_group(cd, blockIdx.y, P, ntile);
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
-  for (int tt = gw; tt < B * ntile; tt += nw) {
-    const int b = tt / ntile, t = tt - b * ntile;
+  for (int t = gw; t < g.ntile; t += nw) {
     float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
     float mu = INFINITY;
     bool bad = false;
     for (int k = lane; k < kTilePoints; k += 32) {
       const int pos = t * kTilePoints + k;
-      if (pos >= P) continue;
-      const float* r = rec + ((int64_t)b * P + perm[(int64_t)b * P + pos]) * kRecLen;
+      if (pos >= g.P) continue;
+      const float* r = rec + (g.p0 + perm[g.p0 + pos]) * kRecLen;
       float v[kRecLen];
 #pragma unroll
       for (int m = 0; m < kRecLen; ++m) v[m] = r[m];
@@ -206,7 +257,7 @@ __global__ void tile_info_kernel(const float* __restrict__ rec, const int* __res
     }
     bad = __any_sync(0xffffffffu, bad);
     if (lane == 0) {
-      float* o = tinfo + (int64_t)tt * 8;
+      float* o = tinfo + (g.t0 + t) * 8;
       for (int a = 0; a < 3; ++a) {
         o[a] = mn[a];
         o[3 + a] = mx[a];
@@ -223,6 +274,13 @@ int spatial_bits(int P) {
   return bits;
 }
 
+namespace {
+unsigned grid_x(int64_t n, int sms, int groups) {
+  const int64_t cap = std::max<int64_t>(1, (int64_t)sms * 16 / std::max(1, groups));
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, cap));
+}
+}  // namespace
+
 int launch_spatial_index(const float* q, const float* rec, int B, int Q, int P, int P_pad, char* ws, const FwdLayout& L,
                          cudaStream_t st) {
   int dev = 0, sms = 148;
@@ -236,24 +294,76 @@ int launch_spatial_index(const float* q, const float* rec, int B, int Q, int P, 
   int* perm_q = reinterpret_cast<int*>(ws + L.perm_q);
   float* pairs = reinterpret_cast<float*>(ws + L.pairs);
   float* tinfo = reinterpret_cast<float*>(ws + L.tinfo);
-  auto grid = [&](int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, sms * 16)); };
-  point_bounds_kernel<<<B, 512, 0, st>>>(rec, P, bnd);
+  const int ntile = P_pad / kTilePoints;
+  GroupMap pm{P, bits, nullptr, nullptr, nullptr, nullptr, nullptr};
+  GroupMap qm{Q, bits, nullptr, nullptr, nullptr, nullptr, nullptr};
+  point_bounds_kernel<<<B, 512, 0, st>>>(rec, pm, bnd);
   // points
   if (cudaMemsetAsync(cnt, 0, (size_t)B * cells * 4, st) != cudaSuccess) return KNNAG_ERR_CUDA;
-  cell_count_kernel<<<grid((int64_t)B * P), 256, 0, st>>>(rec + kNPX, kRecLen, 1, P, B, bnd, bits, cnt);
+  cell_count_kernel<<<dim3(grid_x(P, sms, B), B), 256, 0, st>>>(rec + kNPX, kRecLen, 1, pm, bnd, cnt);
   int rc = launch_exclusive_scan(cnt, B * cells, off, st);
   if (rc) return rc;
-  cell_scatter_kernel<<<grid((int64_t)B * P), 256, 0, st>>>(rec + kNPX, kRecLen, 1, P, B, bnd, bits, off, cnt, perm_p);
+  cell_scatter_kernel<<<dim3(grid_x(P, sms, B), B), 256, 0, st>>>(rec + kNPX, kRecLen, 1, pm, bnd, off, cnt, perm_p);
   // queries (the scatter left the point counts in cnt)
   if (cudaMemsetAsync(cnt, 0, (size_t)B * cells * 4, st) != cudaSuccess) return KNNAG_ERR_CUDA;
-  cell_count_kernel<<<grid((int64_t)B * Q), 256, 0, st>>>(q, 3, 0, Q, B, bnd, bits, cnt);
+  cell_count_kernel<<<dim3(grid_x(Q, sms, B), B), 256, 0, st>>>(q, 3, 0, qm, bnd, cnt);
   rc = launch_exclusive_scan(cnt, B * cells, off, st);
   if (rc) return rc;
-  cell_scatter_kernel<<<grid((int64_t)B * Q), 256, 0, st>>>(q, 3, 0, Q, B, bnd, bits, off, cnt, perm_q);
-  pack_pairs_sorted_kernel<<<grid((int64_t)B * P_pad * kRecLen), 256, 0, st>>>(rec, perm_p, B, P, P_pad, pairs);
-  const int ntile = P_pad / kTilePoints;
-  tile_info_kernel<<<grid((int64_t)B * ntile * 32), 256, 0, st>>>(rec, perm_p, B, P, ntile, tinfo);
-  note_launches(7);
+  cell_scatter_kernel<<<dim3(grid_x(Q, sms, B), B), 256, 0, st>>>(q, 3, 0, qm, bnd, off, cnt, perm_q);
+  pack_pairs_sorted_kernel<<<dim3(grid_x((int64_t)P_pad * kRecLen, sms, B), B), 256, 0, st>>>(rec, perm_p, nullptr, P,
+                                                                                               ntile, pairs);
+  tile_info_kernel<<<dim3(grid_x((int64_t)ntile * 32, sms, B), B), 256, 0, st>>>(rec, perm_p, nullptr, P, ntile, tinfo);
+  note_launches(7);  // + 2 scans, counted by launch_exclusive_scan
+  return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
+}
+
+// Cloud-set index: bounds, Morton order, sorted tiles and tile boxes of
+// every cloud (records already packed).  Scratch: cell counts and offsets
+// [total_cells (+1)], point permutation [total_p].
+int launch_cloudset_index(char* cs, const CloudSetHeader& h, const CloudDesc* cd_dev, int max_p, int max_ntile,
+                          int* cnt, int* off, int* perm_p, cudaStream_t st) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int C = h.C;
+  const float* rec = reinterpret_cast<const float*>(cs + h.rec_off);
+  float* bnd = reinterpret_cast<float*>(cs + h.bnd_off);
+  float* pairs = reinterpret_cast<float*>(cs + h.pairs_off);
+  float* tinfo = reinterpret_cast<float*>(cs + h.tinfo_off);
+  GroupMap pm{0, 0, cd_dev, nullptr, nullptr, nullptr, nullptr};
+  point_bounds_kernel<<<C, 512, 0, st>>>(rec, pm, bnd);
+  if (cudaMemsetAsync(cnt, 0, (size_t)h.total_cells * 4, st) != cudaSuccess) return KNNAG_ERR_CUDA;
+  cell_count_kernel<<<dim3(grid_x(max_p, sms, C), C), 256, 0, st>>>(rec + kNPX, kRecLen, 1, pm, bnd, cnt);
+  int rc = launch_exclusive_scan(cnt, h.total_cells, off, st);
+  if (rc) return rc;
+  cell_scatter_kernel<<<dim3(grid_x(max_p, sms, C), C), 256, 0, st>>>(rec + kNPX, kRecLen, 1, pm, bnd, off, cnt,
+                                                                       perm_p);
+  pack_pairs_sorted_kernel<<<dim3(grid_x((int64_t)max_ntile * kTilePoints * kRecLen, sms, C), C), 256, 0, st>>>(
+      rec, perm_p, cd_dev, 0, 0, pairs);
+  tile_info_kernel<<<dim3(grid_x((int64_t)max_ntile * 32, sms, C), C), 256, 0, st>>>(rec, perm_p, cd_dev, 0, 0, tinfo);
+  note_launches(5);  // + 1 scan
+  return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
+}
+
+// Query order of a segment table: every segment's queries counting-sorted by
+// the Morton code of a grid over its cloud's box.  cnt/off hold cap_cells
+// (+1) cells (the encoded total is at most that); perm_q gets, at each
+// segment's rows, the segment-local query indices in sorted order.  Sizes
+// come from the device copy of the table, so the launches replay on new
+// tables of the same capacity.
+int launch_query_order(const float* q, const char* cs, const void* segs_dev, int cap_segs, int64_t cap_q,
+                       int cap_cells, int* cnt, int* off, int* perm_q, const int* status, cudaStream_t st) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  GroupMap qm{0, 0, nullptr, seg_descs(segs_dev), static_cast<const SegHeader*>(segs_dev), cs, status};
+  if (cudaMemsetAsync(cnt, 0, (size_t)cap_cells * 4, st) != cudaSuccess) return KNNAG_ERR_CUDA;
+  const dim3 grid(grid_x(cap_q, sms, cap_segs), cap_segs);
+  cell_count_kernel<<<grid, 256, 0, st>>>(q, 3, 0, qm, nullptr, cnt);
+  int rc = launch_exclusive_scan(cnt, cap_cells, off, st);
+  if (rc) return rc;
+  cell_scatter_kernel<<<grid, 256, 0, st>>>(q, 3, 0, qm, nullptr, off, cnt, perm_q);
+  note_launches(2);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 

@@ -35,6 +35,17 @@ _SIGS = {
     "knnag_forward_precomputed": ([_V] * 6 + [_I] * 6 + [_V] * 3 + [_V, _S, _V], _I),
     "knnag_forward_lookup": ([_V] * 6 + [_I] * 7 + [_V] * 4 + [_V, _S, _V], _I),
     "knnag_forward_isotropic": ([_V] * 4 + [_I] * 7 + [_V] * 4 + [_V], _I),
+    "knnag_cloudset_bytes": ([_I, _V], _S),
+    "knnag_cloudset_build_workspace_bytes": ([_I, _V], _S),
+    "knnag_cloudset_init": ([_I, _V, _V, _S, _V], _I),
+    "knnag_cloudset_build": ([_V, _V, _V, _I, _V, _V, _S, _V, _S, _V], _I),
+    "knnag_segments_bytes": ([_I], _S),
+    "knnag_segments_encode": ([_I, _V, _V, _V, _V, _I, _V, _I, _V, _S], _I),
+    "knnag_ragged_workspace_bytes": ([_I, ctypes.c_longlong], _S),
+    "knnag_ragged_forward": ([_V, _V, _V, _V, _I, _I, ctypes.c_longlong, ctypes.c_longlong, _I, _I, _I]
+                             + [_V] * 4 + [_V, _S, _V], _I),
+    "knnag_ragged_grad_q": ([_V, _V, _V, _V, _I, _V, _V, _I, ctypes.c_longlong, ctypes.c_longlong, _I, _I, _V, _V,
+                             _S, _V], _I),
     "knnag_points_bytes": ([_I, _I, _I], _S),
     "knnag_pack_points": ([_V, _V, _V, _I, _I, _I, _V, _V], _I),
     "knnag_adjacency_bytes": ([_I, _I, _I, _I], _S),

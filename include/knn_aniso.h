@@ -45,7 +45,8 @@ typedef enum {
   KNNAG_ERR_WORKSPACE = 4,  /* workspace smaller than the *_bytes() query */
   KNNAG_ERR_TOO_LARGE = 5,  /* B*Q*K or B*P exceeds the 32-bit index range */
   KNNAG_ERR_CUDA = 6,       /* a launch failed (cudaGetLastError) */
-  KNNAG_ERR_DEVICE = 7,     /* latched on the device: a bounded wait gave up */
+  KNNAG_ERR_DEVICE = 7,     /* latched on the device: a bounded wait gave up, or a
+                               segment table failed validation (ragged calls) */
   KNNAG_ERR_SCRATCH_LIMIT = 8 /* needs more than knnag_forward_noalloc's fixed scratch */
 } knnag_status;
 
@@ -213,6 +214,79 @@ int knnag_backward_2nd(const void* grad_grad_q, const void* grad_f_out, const vo
 /* Copy the device status word latched in a forward/backward workspace to the
  * host (synchronises `stream`) and clear it; returns KNNAG_OK or KNNAG_ERR_DEVICE. */
 int knnag_read_device_status(void* workspace, void* stream);
+
+/* ------------------------------------------- ragged batches (FP32 only)
+ *
+ * No single reference entry point: the reference takes one uniform batch per
+ * call, so a batch of clouds with different P, Q and K is a host loop over
+ * knn_aggregate_aniso_forward (csrc/knn_aggregate.cpp:26-47), one call per
+ * cloud.  These entry points serve such a batch -- or a stream of requests
+ * against resident clouds -- in one launch sequence.
+ *
+ * Cloud set: C clouds with P[c] points, their p [sum P, 3], sigma
+ * [sum P, 3], R [sum P, 3, 3] and features f [sum P, F] concatenated in
+ * cloud order.  The cloud-set buffer (device, 256-byte aligned,
+ * knnag_cloudset_bytes) holds the packed records and the search index of
+ * every cloud and describes itself; kernels need only its address. */
+
+/* Bytes of a cloud set of C clouds with P[c] >= 1 points (host array); 0 if invalid. */
+size_t knnag_cloudset_bytes(int C, const int* P);
+
+/* Scratch bytes of knnag_cloudset_build. */
+size_t knnag_cloudset_build_workspace_bytes(int C, const int* P);
+
+/* Write the cloud set's header and cloud table (host -> device copy; the
+ * call synchronises `stream`, so it cannot be captured).  Needed once per
+ * buffer and size list. */
+int knnag_cloudset_init(int C, const int* P, void* cloudset, size_t cloudset_bytes, void* stream);
+
+/* Pack the clouds' records and build their search index (Morton order, sorted
+ * tiles, tile key bounds) from p, sigma, R.  Kernels only (capturable); call
+ * again whenever the geometry changes.  The buffer must have been set up by
+ * knnag_cloudset_init with the same C and P. */
+int knnag_cloudset_build(const float* p, const float* sigma, const float* R, int C, const int* P, void* cloudset,
+                         size_t cloudset_bytes, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Segment table: nseg query sets; segment s has Q[s] queries against cloud
+ * cloud[s] with K[s] neighbours (1 <= K[s] <= P of that cloud).  Its queries
+ * are rows [q_off, q_off + Q[s]) of q [sum Q, 3] and f_out [sum Q, F] (q_off
+ * = sum of the Q before it), its neighbours entries [e_off, e_off + Q[s] K[s])
+ * of w_out, dists, idxs (e_off = sum of Q K before it), idxs being point
+ * indices within the cloud.  knnag_segments_encode writes the table into a
+ * HOST buffer of knnag_segments_bytes(nseg); the caller copies it to a
+ * device buffer (256-byte aligned) before the call that uses it.  `splits`
+ * (1, 2 or 4 warps per 32 queries) must match the forward's.  want_grad
+ * (NULL: every segment) marks the segments knnag_ragged_grad_q serves; they
+ * must come first. */
+size_t knnag_segments_bytes(int nseg);
+int knnag_segments_encode(int nseg, const int* cloud, const int* Q, const int* K, const int* want_grad, int C,
+                          const int* cloud_P, int splits, void* table, size_t table_bytes);
+
+/* Scratch bytes of knnag_ragged_forward for tables of at most cap_segments
+ * segments and cap_queries queries. */
+size_t knnag_ragged_workspace_bytes(int cap_segments, long long cap_queries);
+
+/* Forward of every segment: kNN under the segment's cloud's anisotropic
+ * keys, MinK order and tie rules, w_out = exp(-dists), f_out = sum_k w_k
+ * f[idx_k] -- per segment bit-identical to knnag_forward on that cloud and
+ * query set.  Sizes are read from the device table, so a captured graph of
+ * this call replays on any table within the capacities (cap_segments,
+ * cap_queries, cap_entries = sum Q K, max_k >= every K, max_cloud_points >=
+ * every cloud's P).  A table outside them latches KNNAG_ERR_DEVICE in the
+ * workspace status word (knnag_read_device_status) and writes nothing. */
+int knnag_ragged_forward(const void* cloudset, const void* segments, const float* q, const float* f, int F,
+                         int cap_segments, long long cap_queries, long long cap_entries, int max_k,
+                         int max_cloud_points, int splits, float* f_out, float* w_out, float* dists, int64_t* idxs,
+                         void* workspace, size_t workspace_bytes, void* stream);
+
+/* dq = d<grad_f_out, f_out>/dq of the segments marked want_grad (rows
+ * [0, their total Q)) at the forward's idxs (weights recomputed; grad_f_out
+ * NULL means all ones, i.e. d(sum f_out)/dq) -- the first-order query
+ * gradient of knnag_backward.  workspace: 256 bytes (status word). */
+int knnag_ragged_grad_q(const void* cloudset, const void* segments, const float* q, const float* f, int F,
+                        const float* grad_f_out, const int64_t* idxs, int cap_segments, long long cap_queries,
+                        long long cap_entries, int max_k, int max_cloud_points, float* dq, void* workspace,
+                        size_t workspace_bytes, void* stream);
 
 /* ---------------------------------------------------------- instrumentation
  * No reference counterpart (the reference has no timing hooks). */
