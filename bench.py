@@ -262,6 +262,202 @@ def time_reference_ext(device, steps, warmup):
             "how": "reference extension compiled from its own sources (sm_100), reference autograd wiring, eager"}
 
 
+# ------------------------------------------------------------ ragged / served
+
+def _events():
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def ragged_block(device, steps=10, ref_steps=2):
+    """Ragged batch of 64 clouds (P ~ logU[1024, 32768], Q ~ logU[2048,
+    65536], K in {8, 16, 32}, F=64, Gaussian-mixture clouds): one captured
+    graph of cloud-set build + ragged forward, against a per-cloud loop of
+    the uniform op (one eager call per cloud) and a per-cloud loop of the
+    reference extension.  Forward only; L2 flushed between steps."""
+    from cuda_knn_aggregate import capi, knn_aggregate_aniso
+    from cuda_knn_aggregate import workloads as W
+    from cuda_knn_aggregate.ragged import CloudSet, RaggedExecutor, autotune_splits
+
+    rb = W.ragged_batch()
+    C = len(rb.sizes)
+    p, sigma, R, f, q = [t.to(device) for t in (rb.p, rb.sigma, rb.R, rb.f, rb.q)]
+    cs = CloudSet(p, sigma, R, f, rb.sizes)
+    total_q = sum(rb.Qs)
+    qsegs = [q[a:a + n] for a, n in zip(_prefix(rb.Qs), rb.Qs)]
+    splits = autotune_splits(cs, list(range(C)), qsegs, rb.Ks)
+    ex = RaggedExecutor(cs, cap_segments=C, cap_queries=total_q, max_k=max(rb.Ks), splits=splits, graph=False,
+                        copy_out=False)
+    ex.submit(list(range(C)), qsegs, rb.Ks)
+    ex.result()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
+
+    def ragged_step():
+        cs.build()
+        ex._kernels()
+
+    side = torch.cuda.Stream(device)
+    side.wait_stream(torch.cuda.current_stream(device))
+    with torch.cuda.stream(side):
+        ragged_step()
+    torch.cuda.current_stream(device).wait_stream(side)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        c0 = capi.launch_count()
+        ragged_step()
+        launches = capi.launch_count() - c0
+    for _ in range(3):
+        g.replay()
+    torch.cuda.synchronize()
+    t_graph = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = _events()
+        e0.record()
+        g.replay()
+        e1.record()
+        e1.synchronize()
+        t_graph.append(e0.elapsed_time(e1))
+    ex.check_status()
+    res_f = ex.f_out[:total_q].clone()
+
+    clouds = [[t.contiguous() for t in cs.cloud(c)] for c in range(C)]
+    qs = [q[a:a + n].contiguous() for a, n in zip(_prefix(rb.Qs), rb.Qs)]
+
+    def loop(op):
+        outs = []
+        with torch.no_grad():
+            for c in range(C):
+                pc, sc, Rc, fc = clouds[c]
+                outs.append(op(qs[c][None], pc[None], fc[None], sc[None], Rc[None], rb.Ks[c])[0])
+        return outs
+
+    for _ in range(2):
+        loop(knn_aggregate_aniso)
+    torch.cuda.synchronize()
+    t_loop = []
+    for _ in range(max(3, steps // 2)):
+        flush.zero_()
+        e0, e1 = _events()
+        e0.record()
+        outs = loop(knn_aggregate_aniso)
+        e1.record()
+        e1.synchronize()
+        t_loop.append(e0.elapsed_time(e1))
+    same = all(torch.equal(o[0], res_f[a:a + n]) for o, a, n in zip(outs, _prefix(rb.Qs), rb.Qs))
+    ms, ms_loop = statistics.median(t_graph), statistics.median(t_loop)
+    pairs = sum(a * b for a, b in zip(rb.Qs, rb.sizes))
+    out = {"workload": "ragged: 64 clouds, P~logU[1024,32768], Q~logU[2048,65536], K in {8,16,32}, F=64, "
+                       "8-Gaussian mixtures; forward (cloud-set build + ragged search/aggregation)",
+           "clouds": C, "queries": total_q, "points": sum(rb.sizes), "pairs": pairs,
+           "ms_per_step": ms, "value": total_q / (ms / 1e3), "unit": UNIT, "execution": "one CUDA graph",
+           "gpu_launches_per_step": launches, "splits": splits,
+           "per_cloud_loop": {"ms_per_step": ms_loop, "value": total_q / (ms_loop / 1e3),
+                              "how": "eager loop of knn_aggregate_aniso, one call per cloud"},
+           "speedup_vs_loop": ms_loop / ms, "f_out_identical_to_loop": bool(same)}
+    ref, why = load_reference_ext()
+    if ref is None:
+        out["reference_ext_loop"] = {"unavailable": why}
+    else:
+        rop = lambda *a: ref.knn_aggregate_aniso_forward(*a)
+        loop(rop)
+        torch.cuda.synchronize()
+        t_ref = []
+        for _ in range(ref_steps):
+            flush.zero_()
+            e0, e1 = _events()
+            e0.record()
+            loop(rop)
+            e1.record()
+            e1.synchronize()
+            t_ref.append(e0.elapsed_time(e1))
+        mr = statistics.median(t_ref)
+        out["reference_ext_loop"] = {"ms_per_step": mr, "value": total_q / (mr / 1e3),
+                                     "how": "reference extension forward, one call per cloud"}
+        out["speedup_vs_reference_loop"] = mr / ms
+    return out
+
+
+def _prefix(xs):
+    a, o = 0, []
+    for x in xs:
+        o.append(a)
+        a += x
+    return o
+
+
+def served_block(device, seconds_per_rate=2.0, loads=(0.5, 0.8, 0.95)):
+    """Serving over 16 resident sphere-layout clouds (P cycling 16384 /
+    65536 / 131072, F=64): requests with Q ~ logU[256, 65536] against a random
+    cloud, K=16, 30% also asking d(sum f_out)/dq, host query buffers in and
+    host outputs out.  Saturated throughput (every request queued at t=0),
+    then Poisson arrivals at fractions of it with p50/p99 latency; beside it
+    the same requests served by a per-request loop of the uniform op."""
+    from cuda_knn_aggregate import knn_aggregate_aniso
+    from cuda_knn_aggregate import workloads as W
+    from cuda_knn_aggregate.ragged import CloudSet
+    from cuda_knn_aggregate.serving import Request, Server
+
+    p, sigma, R, f, sizes = W.serving_clouds()
+    cs = CloudSet(p.to(device), sigma.to(device), R.to(device), f.to(device), sizes)
+
+    def requests(n, rate, seed):
+        raw = W.serving_requests(n, rate, seed=seed)
+        return [Request(cloud=r["cloud"], q=r["q"].pin_memory(), K=r["K"], want_grad=r["want_grad"],
+                        arrival=r["arrival"]) for r in raw]
+
+    warm = requests(40, None, 7)
+    srv = Server(cs, hbm_budget_bytes=40e9, max_k=16, step_queries=1 << 18, inflight=3, cap_segments=256,
+                 splits="auto", tune_requests=warm, host_budget_bytes=2e9)
+    srv.run(warm, keep_outputs=False)  # warm-up
+    sat = srv.run(requests(300, None, 8), keep_outputs=False)
+    mean_q = sat.queries / max(1, sat.n_requests)
+    sat_rps = sat.throughput / mean_q
+    out = {"workload": "served: 16 resident sphere clouds (P 16384/65536/131072, F=64), Q~logU[256,65536], K=16, "
+                       "30% fwd + d(sum f_out)/dq, pinned host queries in, host f_out/dq out",
+           "hbm_budget_gb": 40, "device_bytes": srv.device_bytes, "step_queries": srv.step_queries,
+           "inflight_steps": len(srv.execs), "splits": srv.splits, "host_ring_gb": srv.ring.cap / 1e9,
+           "saturated": {**sat.summary(), "requests_per_s": sat_rps}, "rates": []}
+    for i, frac in enumerate(loads):
+        rate = frac * sat_rps
+        n = max(20, int(rate * seconds_per_rate))
+        st = srv.run(requests(n, rate, 100 + i), keep_outputs=False)
+        out["rates"].append({"load": frac, "rate_rps": rate, **st.summary()})
+    mid = out["rates"][len(out["rates"]) // 2] if out["rates"] else None
+    if mid:
+        out["p50_ms"], out["p99_ms"], out["at_load"] = mid["p50_ms"], mid["p99_ms"], mid["load"]
+
+    # per-request plain loop of the uniform op (same requests, saturated)
+    reqs = requests(60, None, 9)
+    clouds = [[t.contiguous() for t in cs.cloud(c)] for c in range(cs.C)]
+
+    def plain(r):
+        pc, sc, Rc, fc = clouds[r.cloud]
+        qd = r.q.to(device, non_blocking=True)[None]
+        if r.want_grad:
+            qd.requires_grad_(True)
+            fo = knn_aggregate_aniso(qd, pc[None], fc[None], sc[None], Rc[None], r.K)[0]
+            dq = torch.autograd.grad(fo.sum(), qd)[0]
+            dq.to("cpu", non_blocking=True)
+        else:
+            with torch.no_grad():
+                fo = knn_aggregate_aniso(qd, pc[None], fc[None], sc[None], Rc[None], r.K)[0]
+        fo.detach().to("cpu", non_blocking=True)
+
+    for r in reqs[:5]:
+        plain(r)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for r in reqs:
+        plain(r)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    qn = sum(int(r.q.shape[0]) for r in reqs)
+    out["per_request_loop"] = {"throughput_qps": qn / el, "requests": len(reqs),
+                               "how": "eager loop of knn_aggregate_aniso (+autograd dq), one call per request"}
+    out["speedup_vs_loop"] = out["saturated"]["throughput_qps"] / (qn / el)
+    return out
+
+
 # ------------------------------------------------------------------- arms
 
 def fp32_peak_tflops(device):
@@ -423,6 +619,12 @@ def run_ours(args):
         if "ms_per_step" in out["reference_ext"]:
             out["reference_ext"]["speedup_value"] = out["reference_ext"]["ms_per_step"] / ms
             out["reference_ext"]["speedup_e2e"] = out["reference_ext"]["ms_per_step"] / e2e_ms
+    if ws == 1 and not args.no_ragged:
+        out["ragged"] = ragged_block(device)
+    if ws == 1 and not args.no_served:
+        out["served"] = served_block(device)
+        out["served_p50_ms"] = out["served"].get("p50_ms")
+        out["served_p99_ms"] = out["served"].get("p99_ms")
     if ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_block()
     print(json.dumps(out), flush=True)
@@ -474,6 +676,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-ext"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-ext", action="store_true")
+    ap.add_argument("--no-ragged", action="store_true", help="skip the ragged-batch block")
+    ap.add_argument("--no-served", action="store_true", help="skip the serving block")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":

@@ -2,7 +2,7 @@
 //
 // A cloud set holds C point clouds of different sizes in one device buffer
 // that describes itself: a header, one CloudDesc per cloud, then the packed
-// point records, the Morton-sorted search tiles, the tile boxes and the
+// point records, the Hilbert-sorted search tiles, the tile boxes and the
 // per-cloud bounds of all clouds back to back.  Kernels find every region
 // from the header, so the host needs only the buffer's address.
 //

@@ -399,6 +399,23 @@ struct SearchItem {
   int Q, P, K, ntile, qblock;
 };
 
+// Lower bound on the key of any query in box [bmin, bmax] against any point
+// of a tile (its box ti[0..5], bound factor mu = ti[6]): mu * dist(box,
+// tile box)^2, shrunk by 1e-5 for the rounding of this product; -inf when
+// the tile has no bound (mu < 0).
+__device__ __forceinline__ float tile_lower_bound(const float* ti, const float* bmin, const float* bmax) {
+  const float mu = ti[6];
+  if (!(mu >= 0.f)) return -INFINITY;
+  float d2 = 0.f;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float g = fmaxf(fmaxf(ti[c] - bmax[c], bmin[c] - ti[3 + c]), 0.f);
+    d2 = __fmaf_rn(g, g, d2);
+  }
+  const float lb = mu * d2 * 0.99999f;
+  return lb >= 0.f ? lb : 0.f;  // NaN: 0 (keys are >= 0 when mu >= 0)
+}
+
 // The two tile-buffer mbarriers of a search CTA.
 __device__ __forceinline__ uint64_t* search_barriers(unsigned char* smem, size_t region_a) {
   return reinterpret_cast<uint64_t*>(smem + region_a + (size_t)kQueueCap * kSearchThreads * 8 +
@@ -490,15 +507,8 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     float lb = INFINITY;
     if (t < it.ntile) {
       const float* ti = tinfo_b + t * 8;
-      float d2 = 0.f;
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float g = fmaxf(fmaxf(ti[c] - bmax[c], bmin[c] - ti[3 + c]), 0.f);
-        d2 = __fmaf_rn(g, g, d2);
-      }
-      lb = ti[6] * d2 * 0.99999f;
-      if (!(lb >= 0.f)) lb = 0.f;  // NaN or negative: no bound
-      lb = fminf(lb, 3.4e38f);     // real tiles sort before the +inf padding entries
+      lb = tile_lower_bound(ti, bmin, bmax);
+      lb = fminf(lb, 3.4e38f);  // real tiles sort before the +inf padding entries
     }
     lbk[t] = lb;
     lbt[t] = t;
@@ -565,8 +575,20 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     const int buf = t & 1;
     const bool ok = mbar_wait_bounded(&full[buf], (uses[buf] + (t >> 1)) & 1);
     const float4* tp = reinterpret_cast<const float4*>(regA + buf * kTileBytes) + split * PPS * 8;
+    // Per-warp culling: the CTA visits a tile when it may matter to any of
+    // its query groups; a warp whose own query box bounds every key of the
+    // tile above all of its lanes' thresholds skips it (it could add no
+    // candidate: keys above a lane's threshold are dropped anyway).
+    bool run = true;
+    if (G < 4) {
+      const float lbw = tile_lower_bound(tinfo_b + (int64_t)lbt[t] * 8, qbox + warp * 6, qbox + warp * 6 + 3);
+      float tw = valid ? tau : -INFINITY;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) tw = fmaxf(tw, __shfl_xor_sync(0xffffffffu, tw, o));
+      run = !(lbw > tw);
+    }
 #pragma unroll 2
-    for (int m = 0; m < PPS; ++m) {
+    for (int m = 0; run && m < PPS; ++m) {
       float2 pr[16];
 #pragma unroll
       for (int u = 0; u < 8; ++u) {

@@ -1,5 +1,5 @@
 // Spatial ordering for the search: points and queries of every batch element
-// are counting-sorted by the Morton code of a uniform grid cell, the search
+// are counting-sorted by the Hilbert-curve index of a uniform grid cell, the search
 // tiles are packed in that order (each record keeps its original point
 // index), and every 128-point tile gets an axis-aligned box and a lower bound
 // on the key of any query against any of its points:
@@ -8,7 +8,9 @@
 //               - 1e-5 * sum_a |sigma_a| |R_a|^2,
 // where lambda_min is computed in double and the second term covers the
 // rounding of the FP32 key (|key_fp32 - key_exact| <= ~12 * 2^-24 *
-// |q - p|^2 * sum_a |sigma_a| |R_a|^2).  Non-finite data give mu = 0 (no bound).
+// |q - p|^2 * sum_a |sigma_a| |R_a|^2).  With every sigma >= 0 every key is
+// >= 0, so mu = 0 still bounds; a tile holding a negative or non-finite
+// value gets mu = -1: no bound at all (its keys may be negative).
 // The search visits tiles nearest-first by this bound and stops when the
 // bound exceeds every query's threshold; the order of points inside a cell
 // (atomic scatter) never changes a result, only the work done.
@@ -30,6 +32,40 @@ __device__ __forceinline__ uint32_t spread3(uint32_t v) {
   return v;
 }
 
+// Position of grid cell (x, y, z) (bits bits per axis) along the 3-D Hilbert
+// curve, by J. Skilling's transpose algorithm ("Programming the Hilbert
+// curve", AIP Conf. Proc. 707, 2004): undo the excess work, Gray-encode,
+// then interleave the transposed coordinates (X[0] most significant).
+// Consecutive cells along the curve are always face neighbours, so a run of
+// sorted points (a search tile) or queries (a CTA) stays compact; the
+// Z-order curve jumps across the box at every level.
+__device__ __forceinline__ uint32_t hilbert3(uint32_t x, uint32_t y, uint32_t z, int bits) {
+  uint32_t X[3] = {x, y, z};
+  const uint32_t M = 1u << (bits - 1);
+  for (uint32_t Q = M; Q > 1; Q >>= 1) {
+    const uint32_t P = Q - 1;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      if (X[i] & Q) {
+        X[0] ^= P;
+      } else {
+        const uint32_t t = (X[0] ^ X[i]) & P;
+        X[0] ^= t;
+        X[i] ^= t;
+      }
+    }
+  }
+  X[1] ^= X[0];
+  X[2] ^= X[1];
+  uint32_t t = 0;
+  for (uint32_t Q = M; Q > 1; Q >>= 1)
+    if (X[2] & Q) t ^= Q - 1;
+  X[0] ^= t;
+  X[1] ^= t;
+  X[2] ^= t;
+  return (spread3(X[0]) << 2) | (spread3(X[1]) << 1) | spread3(X[2]);
+}
+
 __device__ __forceinline__ uint32_t cell_of(float x, float y, float z, const float* bnd, int bits) {
   const float res = (float)(1 << bits);
   uint32_t c[3];
@@ -41,7 +77,7 @@ __device__ __forceinline__ uint32_t cell_of(float x, float y, float z, const flo
     t = fminf(fmaxf(t, 0.f), res - 1.f);  // NaN -> 0
     c[a] = (uint32_t)t;
   }
-  return spread3(c[0]) | (spread3(c[1]) << 1) | (spread3(c[2]) << 2);
+  return hilbert3(c[0], c[1], c[2], bits);
 }
 
 // Element groups of a counting sort: the batch elements of a uniform batch
@@ -230,6 +266,7 @@ __global__ void tile_info_kernel(const float* __restrict__ rec, const int* __res
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         const double s = v[kS0 + a];
+        if (!(s >= 0.0)) bad = true;  // a negative (or NaN) precision: keys may be negative
         double rn = 0.0;
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
@@ -262,7 +299,7 @@ __global__ void tile_info_kernel(const float* __restrict__ rec, const int* __res
         o[a] = mn[a];
         o[3 + a] = mx[a];
       }
-      o[6] = (bad || !(mu < INFINITY)) ? 0.0f : mu;
+      o[6] = bad ? -1.0f : (mu < INFINITY ? mu : 0.0f);  // -1: the tile has no key bound
       o[7] = 0.0f;
     }
   }
@@ -317,7 +354,7 @@ int launch_spatial_index(const float* q, const float* rec, int B, int Q, int P, 
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 
-// Cloud-set index: bounds, Morton order, sorted tiles and tile boxes of
+// Cloud-set index: bounds, Hilbert order, sorted tiles and tile boxes of
 // every cloud (records already packed).  Scratch: cell counts and offsets
 // [total_cells (+1)], point permutation [total_p].
 int launch_cloudset_index(char* cs, const CloudSetHeader& h, const CloudDesc* cd_dev, int max_p, int max_ntile,
@@ -346,7 +383,7 @@ int launch_cloudset_index(char* cs, const CloudSetHeader& h, const CloudDesc* cd
 }
 
 // Query order of a segment table: every segment's queries counting-sorted by
-// the Morton code of a grid over its cloud's box.  cnt/off hold cap_cells
+// the Hilbert index of a grid cell over its cloud's box.  cnt/off hold cap_cells
 // (+1) cells (the encoded total is at most that); perm_q gets, at each
 // segment's rows, the segment-local query indices in sorted order.  Sizes
 // come from the device copy of the table, so the launches replay on new

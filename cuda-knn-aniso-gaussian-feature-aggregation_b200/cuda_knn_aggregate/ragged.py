@@ -19,7 +19,6 @@ host loop of calls.  Here:
 from __future__ import annotations
 
 import ctypes
-import math
 from dataclasses import dataclass
 
 import torch
@@ -241,6 +240,54 @@ def ragged_forward(cloudset: CloudSet, q, clouds, Qs, Ks, splits=None, grad_q=No
     return res
 
 
+# ---------------------------------------------------------------- autotuner
+
+_TUNE_CACHE: dict = {}
+
+
+def shape_bucket(cloudset: CloudSet, Qs, Ks):
+    """Shape bucket of a ragged step: log2 of the largest cloud, of the step's
+    total queries and of its mean segment size, and the K register bucket."""
+    total = max(1, sum(int(q) for q in Qs))
+    kmax = max(int(k) for k in Ks)
+    kb = 8 if kmax <= 8 else 16 if kmax <= 16 else 32 if kmax <= 32 else 64
+    return (int(cloudset.max_points).bit_length(), total.bit_length(), max(1, total // len(Qs)).bit_length(), kb)
+
+
+def autotune_splits(cloudset: CloudSet, clouds, qs, Ks, reps=3, cache=True):
+    """Warps per 32-query group (1, 2 or 4) for steps shaped like this one:
+    each candidate runs the step as a captured graph ``reps`` times (after a
+    warm-up) and the fastest median wins.  Cached per ``shape_bucket``."""
+    Qs = [int(x.shape[0]) for x in qs]
+    key = shape_bucket(cloudset, Qs, Ks)
+    if cache and key in _TUNE_CACHE:
+        return _TUNE_CACHE[key]
+    times = {}
+    for g in _SPLITS:
+        ex = RaggedExecutor(cloudset, len(clouds), sum(Qs), max(Ks), splits=g, copy_out=False)
+        ex.submit(clouds, qs, Ks)
+        ex.result()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(ex.stream):
+                e0.record()
+                ex.graph.replay()
+                e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        times[g] = sorted(ts)[len(ts) // 2]
+        del ex
+    best = min(times, key=times.get)
+    _TUNE_CACHE[key] = best
+    return best
+
+
+def tune_cache():
+    """The autotuner's choices so far: {shape bucket: splits}."""
+    return dict(_TUNE_CACHE)
+
+
 class RaggedExecutor:
     """Fixed-capacity ragged step (forward, and dq for the segments that ask)
     captured in a CUDA graph on its own stream.
@@ -314,9 +361,13 @@ class RaggedExecutor:
                                      self.max_k, self.cs.max_points, _ptr(self.dq), _ptr(self.gws), self.gws.numel(),
                                      st))
 
-    def submit(self, clouds, qs, Ks, want_grad=None):
-        """Start one step.  Segments wanting dq are reordered first; the
-        result keeps the caller's order (``order``)."""
+    def submit(self, clouds, qs, Ks, want_grad=None, outs=None):
+        """Start one step.  Segments wanting dq are moved first; ``order``
+        (returned by result) maps table position -> caller's index.  ``outs``
+        (optional, caller's order): per segment a pair of host tensors
+        (f_dst [Q, F], dq_dst [Q, 3] or None) that receive the segment's
+        f_out / dq by device-to-host copies inside the step; without it the
+        whole f_out (and dq) range is copied to f_host / dq_host."""
         if self.pending is not None:
             raise RuntimeError("previous step not collected")
         n = len(clouds)
@@ -326,6 +377,7 @@ class RaggedExecutor:
         qs = [qs[i] for i in order]
         Ks = [int(Ks[i]) for i in order]
         wg = [wg[i] for i in order]
+        outs = None if outs is None else [outs[i] for i in order]
         Qs = [int(x.shape[0]) for x in qs]
         total = sum(Qs)
         if total > self.cap_q or n > self.cap_segments or max(Ks) > self.max_k:
@@ -333,7 +385,9 @@ class RaggedExecutor:
         self._encode(clouds, Qs, Ks, wg)
         q_off = self.meta[2]
         with torch.cuda.stream(self.stream):
-            on_host = [not x.is_cuda for x in qs]
+            # device or pinned sources go straight to the device; pageable
+            # ones through the pinned staging buffer
+            on_host = [not x.is_cuda and not x.is_pinned() for x in qs]
             for i, x in enumerate(qs):
                 rows = slice(q_off[i], q_off[i] + Qs[i])
                 if on_host[i]:
@@ -342,7 +396,7 @@ class RaggedExecutor:
                     self.q_dev[rows].copy_(x, non_blocking=True)
             if all(on_host):
                 self.q_dev[:total].copy_(self.q_host[:total], non_blocking=True)
-            else:
+            elif any(on_host):
                 for i in (i for i in range(n) if on_host[i]):
                     rows = slice(q_off[i], q_off[i] + Qs[i])
                     self.q_dev[rows].copy_(self.q_host[rows], non_blocking=True)
@@ -351,7 +405,14 @@ class RaggedExecutor:
                 self.graph.replay()
             else:
                 self._kernels()
-            if self.copy_out:
+            if outs is not None:
+                for i, (fd, dd) in enumerate(outs):
+                    rows = slice(q_off[i], q_off[i] + Qs[i])
+                    if fd is not None:
+                        fd.copy_(self.f_out[rows], non_blocking=True)
+                    if dd is not None and wg[i]:
+                        dd.copy_(self.dq[rows], non_blocking=True)
+            elif self.copy_out:
                 self.f_host[:total].copy_(self.f_out[:total], non_blocking=True)
                 g = sum(Q for Q, w in zip(Qs, wg) if w)
                 if g:

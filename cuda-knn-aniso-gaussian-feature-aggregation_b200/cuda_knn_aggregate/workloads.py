@@ -148,3 +148,104 @@ def pairs_count(shape: Shape) -> int:
 def log_uniform_int(g: torch.Generator, lo: int, hi: int, n: int) -> torch.Tensor:
     u = torch.rand(n, generator=g, dtype=torch.float64)
     return torch.exp(math.log(lo) + u * (math.log(hi) - math.log(lo))).floor().long().clamp(lo, hi)
+
+
+# ---------------------------------------------------------------- ragged
+
+
+@dataclass
+class RaggedBatch:
+    """Clouds of different sizes, concatenated in cloud order (p, sigma, R,
+    f [sum P, ...]); one query set per cloud (q [sum Q, 3], cloud c at rows
+    q_off[c]:q_off[c]+Qs[c]) with its own K."""
+    p: torch.Tensor
+    sigma: torch.Tensor
+    R: torch.Tensor
+    f: torch.Tensor
+    sizes: list
+    q: torch.Tensor
+    Qs: list
+    Ks: list
+
+    def cloud(self, c):
+        a = sum(self.sizes[:c])
+        b = a + self.sizes[c]
+        return self.p[a:b], self.sigma[a:b], self.R[a:b], self.f[a:b]
+
+    def queries(self, c):
+        a = sum(self.Qs[:c])
+        return self.q[a: a + self.Qs[c]]
+
+
+def _mixture(g, centres, n, std, dtype):
+    comp = torch.randint(0, centres.shape[0], (n,), generator=g)
+    return (centres[comp] + std * torch.randn(n, 3, generator=g, dtype=torch.float64)).to(dtype)
+
+
+def ragged_batch(n_clouds=64, seed=1003, F=64, p_range=(1024, 32768), q_range=(2048, 65536), ks=(8, 16, 32),
+                 dtype=torch.float32):
+    """Ragged-batch workload: P ~ logU[p_range], Q ~ logU[q_range], K drawn
+    from ``ks`` per cloud; points and queries from a mixture of 8 isotropic
+    Gaussians (centres U[0,1)^3, std 0.05) per cloud, R random orthonormal,
+    sigma ~ U[0.01, 0.1]^3, f ~ U[0,1)."""
+    g = torch.Generator().manual_seed(seed)
+    sizes = log_uniform_int(g, *p_range, n_clouds).tolist()
+    Qs = log_uniform_int(g, *q_range, n_clouds).tolist()
+    Ks = [int(ks[i]) for i in torch.randint(0, len(ks), (n_clouds,), generator=g).tolist()]
+    ps, qs = [], []
+    for P, Q in zip(sizes, Qs):
+        centres = torch.rand(8, 3, generator=g, dtype=torch.float64)
+        ps.append(_mixture(g, centres, P, 0.05, dtype))
+        qs.append(_mixture(g, centres, Q, 0.05, dtype))
+    n = sum(sizes)
+    p = torch.cat(ps).contiguous()
+    R = random_rotations(n, g, dtype)
+    sigma = (0.01 + 0.09 * torch.rand(n, 3, generator=g, dtype=torch.float64)).to(dtype)
+    f = torch.rand(n, F, generator=g, dtype=torch.float64).to(dtype)
+    return RaggedBatch(p, sigma.contiguous(), R, f.contiguous(), sizes, torch.cat(qs).contiguous(), Qs, Ks)
+
+
+def serving_clouds(n_clouds=16, seed=1004, F=64, sizes=(16384, 65536, 131072), dtype=torch.float32):
+    """Resident clouds of the serving workload: sizes cycle through ``sizes``;
+    sphere-surface layout of the large single-cloud workload (unit sphere
+    with N(0, 0.01) radial noise, R's third column the normal, sigma = (0.02,
+    0.02, 0.005)), f ~ U[0,1)."""
+    g = torch.Generator().manual_seed(seed)
+    P = [int(sizes[i % len(sizes)]) for i in range(n_clouds)]
+    ps, Rs, fs = [], [], []
+    for n_pts in P:
+        n = torch.randn(n_pts, 3, generator=g, dtype=torch.float64)
+        n = n / n.norm(dim=-1, keepdim=True)
+        eps = 0.01 * torch.randn(n_pts, 1, generator=g, dtype=torch.float64)
+        ps.append(n * (1.0 + eps))
+        Rs.append(_tangent_frames(n))
+        fs.append(torch.rand(n_pts, F, generator=g, dtype=torch.float64))
+    n = sum(P)
+    sigma = torch.tensor([0.02, 0.02, 0.005], dtype=torch.float64).expand(n, 3)
+    cat = lambda xs: torch.cat(xs).to(dtype).contiguous()
+    return cat(ps), sigma.to(dtype).contiguous(), cat(Rs), cat(fs), P
+
+
+def serving_requests(n_requests, rate_hz, n_clouds=16, seed=1005, q_range=(256, 65536), K=16, grad_fraction=0.3,
+                     dtype=torch.float32):
+    """Requests of the serving workload: Poisson arrivals at ``rate_hz``
+    (exponential gaps; every arrival 0 when rate_hz is None), a uniformly
+    random cloud, Q ~ logU[q_range] queries = unit-sphere samples + N(0,
+    0.05)^3 offsets, K neighbours, and a ``grad_fraction`` chance of also
+    asking for d(sum f_out)/dq.  Returns a list of dicts."""
+    g = torch.Generator().manual_seed(seed)
+    Qs = log_uniform_int(g, *q_range, n_requests).tolist()
+    clouds = torch.randint(0, n_clouds, (n_requests,), generator=g).tolist()
+    grads = (torch.rand(n_requests, generator=g) < grad_fraction).tolist()
+    if rate_hz:
+        gaps = -torch.log(1.0 - torch.rand(n_requests, generator=g, dtype=torch.float64)) / rate_hz
+        t = torch.cumsum(gaps, 0).tolist()
+    else:
+        t = [0.0] * n_requests
+    out = []
+    for i in range(n_requests):
+        s = torch.randn(Qs[i], 3, generator=g, dtype=torch.float64)
+        s = s / s.norm(dim=-1, keepdim=True)
+        q = (s + 0.05 * torch.randn(Qs[i], 3, generator=g, dtype=torch.float64)).to(dtype).contiguous()
+        out.append(dict(cloud=clouds[i], q=q, K=K, want_grad=bool(grads[i]), arrival=t[i]))
+    return out

@@ -279,3 +279,32 @@ def test_cloudset_rebuild_after_geometry_change():
     uf, uw, ud, ui, _ = _uniform(moved, q, 16, False)
     f_out, w, d, idx = res.segment(0)
     assert torch.equal(idx, ui) and torch.equal(d, ud) and torch.equal(f_out, uf)
+
+
+@pytest.mark.gpu
+def test_server_results_match_uniform_op():
+    """Requests served under continuous batching (Poisson arrivals, several
+    steps in flight, large requests split into chunks) get exactly the
+    uniform op's f_out and d(sum f_out)/dq."""
+    from cuda_knn_aggregate import workloads as W
+    from cuda_knn_aggregate.ragged import CloudSet
+    from cuda_knn_aggregate.serving import Request, Server
+
+    p, sigma, R, f, sizes = W.serving_clouds(n_clouds=4, F=16, sizes=(3000, 9000))
+    cs = CloudSet(p.cuda(), sigma.cuda(), R.cuda(), f.cuda(), sizes)
+    srv = Server(cs, hbm_budget_bytes=4e9, max_k=16, step_queries=6000, inflight=3, cap_segments=16)
+    raw = W.serving_requests(40, rate_hz=400.0, n_clouds=4, q_range=(64, 9000), seed=11)
+    reqs = [Request(cloud=r["cloud"], q=r["q"], K=r["K"], want_grad=r["want_grad"], arrival=r["arrival"]) for r in raw]
+    stats = srv.run(reqs)
+    assert stats.n_requests == 40 and len(stats.latencies_ms) == 40
+    assert stats.steps >= 2 and stats.pct(99) >= stats.pct(50) > 0
+    assert any(r.q.shape[0] > 6000 for r in reqs)  # some requests were chunked
+    for r in reqs:
+        uf, _, _, _, udq = _uniform(cs_cloud(cs, r.cloud), r.q, r.K, r.want_grad)
+        assert torch.equal(r.f_out, uf.cpu())
+        if r.want_grad:
+            assert torch.equal(r.dq, udq.cpu())
+
+
+def cs_cloud(cs, c):
+    return [t.cpu() for t in cs.cloud(c)]
