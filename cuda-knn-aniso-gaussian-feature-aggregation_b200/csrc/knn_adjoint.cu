@@ -107,6 +107,97 @@ __global__ void __launch_bounds__(1024) adj_scan_kernel(int* __restrict__ count,
   if (tid == 0) rowptr[n] = carry_s;
 }
 
+// Multi-CTA exclusive scan for long arrays, in three passes over chunks of
+// kScanChunk elements (1024 threads x 8): (1) each CTA writes its chunk's
+// sum to out[chunk start]; (2) one CTA replaces those sums by their
+// exclusive prefix and writes the total to out[n]; (3) each CTA scans its
+// chunk from that prefix into out and zeroes count.  The chunk sums live in
+// out itself, so no scratch is needed.
+constexpr int kScanChunk = 8192;
+
+__device__ __forceinline__ int block_exclusive_scan_1024(int local, int* warp_sums, int& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) warp_sums[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const int ws = warp_sums[lane];
+    int wi = ws;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += t;
+    }
+    warp_sums[lane] = wi - ws;
+    if (lane == 31) warp_sums[32] = wi;
+  }
+  __syncthreads();
+  total = warp_sums[32];
+  return warp_sums[warp] + incl - local;
+}
+
+__global__ void __launch_bounds__(1024) scan_chunk_sums_kernel(const int* __restrict__ count, int64_t n,
+                                                               int* __restrict__ out) {
+  __shared__ int warp_sums[33];
+  const int64_t base = (int64_t)blockIdx.x * kScanChunk + (int64_t)threadIdx.x * 8;
+  int local = 0;
+#pragma unroll
+  for (int u = 0; u < 8; ++u)
+    if (base + u < n) local += count[base + u];
+  int total;
+  block_exclusive_scan_1024(local, warp_sums, total);
+  if (threadIdx.x == 0) out[(int64_t)blockIdx.x * kScanChunk] = total;
+}
+
+__global__ void __launch_bounds__(1024) scan_chunk_prefix_kernel(int* __restrict__ out, int64_t n, int chunks) {
+  __shared__ int warp_sums[33];
+  __shared__ int carry_s;
+  if (threadIdx.x == 0) carry_s = 0;
+  __syncthreads();
+  for (int c0 = 0; c0 < chunks; c0 += 1024) {
+    const int c = c0 + threadIdx.x;
+    const int v = c < chunks ? out[(int64_t)c * kScanChunk] : 0;
+    int total;
+    const int ex = block_exclusive_scan_1024(v, warp_sums, total);
+    if (c < chunks) out[(int64_t)c * kScanChunk] = carry_s + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) carry_s += total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[n] = carry_s;
+}
+
+__global__ void __launch_bounds__(1024) scan_chunk_apply_kernel(int* __restrict__ count, int64_t n,
+                                                                int* __restrict__ out) {
+  __shared__ int warp_sums[33];
+  __shared__ int prefix_s;
+  const int64_t chunk0 = (int64_t)blockIdx.x * kScanChunk;
+  if (threadIdx.x == 0) prefix_s = out[chunk0];
+  const int64_t base = chunk0 + (int64_t)threadIdx.x * 8;
+  int v[8];
+  int local = 0;
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    v[u] = base + u < n ? count[base + u] : 0;
+    local += v[u];
+  }
+  int total;
+  int run = block_exclusive_scan_1024(local, warp_sums, total) + prefix_s;  // barriers order the prefix read
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    if (base + u < n) {
+      out[base + u] = run;
+      count[base + u] = 0;
+    }
+    run += v[u];
+  }
+}
+
 __global__ void adj_fill_kernel(const int64_t* __restrict__ idxs, int n, int qk, int P, const int* __restrict__ rowptr,
                                 int* __restrict__ cursor, int* __restrict__ unsorted) {
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
@@ -188,9 +279,20 @@ inline unsigned blocks_for(int64_t n, int threads) {
 }
 }  // namespace
 
+// Exclusive scan of count[0..n) into out[0..n] (out[n] = total); count is
+// zeroed so it can serve as a fill cursor.  One CTA for short arrays, the
+// three-pass multi-CTA scan for long ones.
 int launch_exclusive_scan(int* count, int n, int* out, cudaStream_t st) {
-  adj_scan_kernel<<<1, 1024, 0, st>>>(count, n, out);
-  note_launches(1);
+  if (n <= 4 * kScanChunk) {
+    adj_scan_kernel<<<1, 1024, 0, st>>>(count, n, out);
+    note_launches(1);
+  } else {
+    const int chunks = (int)(((int64_t)n + kScanChunk - 1) / kScanChunk);
+    scan_chunk_sums_kernel<<<chunks, 1024, 0, st>>>(count, n, out);
+    scan_chunk_prefix_kernel<<<1, 1024, 0, st>>>(out, n, chunks);
+    scan_chunk_apply_kernel<<<chunks, 1024, 0, st>>>(count, n, out);
+    note_launches(3);
+  }
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 
@@ -204,10 +306,11 @@ int launch_build_adjacency(const int64_t* idxs, int B, int Q, int P, int K, void
   const int n = B * Q * K, rows = B * P, qk = Q * K;  // sizes checked < 2^31 by the caller
   if (cudaMemsetAsync(cursor, 0, (size_t)rows * 4, st) != cudaSuccess) return KNNAG_ERR_CUDA;
   adj_count_kernel<<<blocks_for(n, 256), 256, 0, st>>>(idxs, n, qk, P, cursor);
-  adj_scan_kernel<<<1, 1024, 0, st>>>(cursor, rows, rowptr);
+  const int rc = launch_exclusive_scan(cursor, rows, rowptr, st);
+  if (rc) return rc;
   adj_fill_kernel<<<blocks_for(n, 256), 256, 0, st>>>(idxs, n, qk, P, rowptr, cursor, unsorted);
   adj_sort_kernel<<<blocks_for((int64_t)rows * 32, 256), 256, 0, st>>>(rowptr, unsorted, rows, entries);
-  note_launches(4);
+  note_launches(3);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 

@@ -372,7 +372,11 @@ class RaggedExecutor:
             raise RuntimeError("previous step not collected")
         n = len(clouds)
         wg = [bool(w) for w in (want_grad or [False] * n)]
-        order = sorted(range(n), key=lambda i: not wg[i])
+        # segments wanting dq first (the table's dq prefix); within each
+        # group the heaviest (cloud size x K) first, so the persistent search
+        # starts the long work items early and the tail is short
+        sizes = self.cs.sizes
+        order = sorted(range(n), key=lambda i: (not wg[i], -sizes[int(clouds[i])] * int(Ks[i])))
         clouds = [int(clouds[i]) for i in order]
         qs = [qs[i] for i in order]
         Ks = [int(Ks[i]) for i in order]

@@ -308,3 +308,41 @@ def test_server_results_match_uniform_op():
 
 def cs_cloud(cs, c):
     return [t.cpu() for t in cs.cloud(c)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rows", [32768, 32769, 100003, 1 << 20])
+def test_adjacency_long_scan(rows):
+    """Point->entry adjacency over more rows than one scan CTA covers (the
+    three-pass scan): row pointers equal the exclusive prefix of a numpy
+    histogram, every row holds exactly its entries in ascending order."""
+    from cuda_knn_aggregate import capi
+
+    g = torch.Generator().manual_seed(rows)
+    Q, K = 20000, 8
+    idxs = torch.randint(0, rows, (1, Q, K), generator=g)
+    adj = capi.build_adjacency(idxs.cuda(), rows)
+    rowptr, entries = capi.adjacency_arrays(adj, 1, Q, rows, K)
+    torch.cuda.synchronize()
+    counts = np.bincount(idxs.numpy().ravel(), minlength=rows)
+    ref = np.concatenate([[0], np.cumsum(counts)])
+    assert np.array_equal(rowptr.cpu().numpy(), ref)
+    e = entries.cpu().numpy()
+    flat = idxs.numpy().ravel()
+    order = np.argsort(flat, kind="stable")
+    assert np.array_equal(e, order)
+
+
+@pytest.mark.gpu
+def test_ragged_long_query_scan():
+    """A ragged call whose query-cell array needs the multi-CTA scan."""
+    from cuda_knn_aggregate.ragged import CloudSet, ragged_forward
+
+    clouds = _clouds([6000, 2500], 8, seed=12)
+    cs = CloudSet.from_clouds([[t.cuda() for t in c] for c in clouds])
+    qs = [_queries(50000, 40), _queries(30000, 41)]
+    res = ragged_forward(cs, torch.cat(qs).cuda(), [0, 1], [50000, 30000], [16, 8])
+    for i, (c, K) in enumerate([(0, 16), (1, 8)]):
+        uf, uw, ud, ui, _ = _uniform(clouds[c], qs[i], K, False)
+        f_out, w, d, idx = res.segment(i)
+        assert torch.equal(idx, ui) and torch.equal(d, ud) and torch.equal(f_out, uf)
