@@ -268,7 +268,7 @@ def _events():
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
 
-def ragged_block(device, steps=10, ref_steps=2):
+def ragged_block(device, steps=10, ref_steps=2, with_reference=True):
     """Ragged batch of 64 clouds (P ~ logU[1024, 32768], Q ~ logU[2048,
     65536], K in {8, 16, 32}, F=64, Gaussian-mixture clouds): one captured
     graph of cloud-set build + ragged forward, against a per-cloud loop of
@@ -356,7 +356,7 @@ def ragged_block(device, steps=10, ref_steps=2):
            "per_cloud_loop": {"ms_per_step": ms_loop, "value": total_q / (ms_loop / 1e3),
                               "how": "eager loop of knn_aggregate_aniso, one call per cloud"},
            "speedup_vs_loop": ms_loop / ms, "f_out_identical_to_loop": bool(same)}
-    ref, why = load_reference_ext()
+    ref, why = load_reference_ext() if with_reference else (None, "skipped (--no-reference-ext)")
     if ref is None:
         out["reference_ext_loop"] = {"unavailable": why}
     else:
@@ -626,7 +626,7 @@ def run_ours(args):
             out["reference_ext"]["speedup_value"] = out["reference_ext"]["ms_per_step"] / ms
             out["reference_ext"]["speedup_e2e"] = out["reference_ext"]["ms_per_step"] / e2e_ms
     if ws == 1 and not args.no_ragged:
-        out["ragged"] = ragged_block(device)
+        out["ragged"] = ragged_block(device, with_reference=not args.no_reference_ext)
     if ws == 1 and not args.no_served:
         out["served"] = served_block(device)
         out["served_p50_ms"] = out["served"].get("p50_ms")
@@ -684,8 +684,18 @@ def main():
     ap.add_argument("--no-reference-ext", action="store_true")
     ap.add_argument("--no-ragged", action="store_true", help="skip the ragged-batch block")
     ap.add_argument("--no-served", action="store_true", help="skip the serving block")
+    ap.add_argument("--workload", default="table", choices=["table", "ragged", "served"],
+                    help="table: the headline line (with the ragged and served blocks attached); ragged / "
+                         "served: only that block, as its own JSON line (for profiling)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.workload != "table" and args.impl == "ours":
+        device = torch.device("cuda", 0)
+        torch.cuda.set_device(device)
+        blk = ragged_block(device, with_reference=not args.no_reference_ext) if args.workload == "ragged" \
+            else served_block(device)
+        print(json.dumps(blk), flush=True)
+        return
     if args.impl == "reference":
         run_reference_cpu(args)
     elif args.impl == "reference-ext":
