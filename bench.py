@@ -379,6 +379,81 @@ def ragged_block(device, steps=10, ref_steps=2, with_reference=True):
     return out
 
 
+def sphere_block(device, steps=5, ref_steps=1, with_reference=True, sample=256):
+    """Large single cloud: B=1, P=131072 sphere-surface points (surface-aligned
+    Gaussians), Q=524288 near-surface queries, F=128, K=16; the Eikonal
+    training step (forward, dq with create_graph, backward), graphed, L2
+    flushed; the reference extension's step beside it; idxs/dists of the
+    first ``sample`` queries checked bit for bit against the CPU oracle."""
+    from cuda_knn_aggregate import knn_aggregate_aniso
+    from cuda_knn_aggregate import workloads as W
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    shape, t = W.make("sphere")
+    ins = [x.to(device).requires_grad_(True) for x in t]
+    step = eikonal_step_fn(knn_aggregate_aniso, ins, shape.K)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
+    side = torch.cuda.Stream(device)
+    side.wait_stream(torch.cuda.current_stream(device))
+    with torch.cuda.stream(side):
+        for _ in range(2):
+            step()
+    torch.cuda.current_stream(device).wait_stream(side)
+    for a in ins:
+        a.grad = None
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        step()
+    g.replay()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = _events()
+        e0.record()
+        g.replay()
+        e1.record()
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    ms = statistics.median(ts)
+    units = shape.B * shape.Q
+    with torch.no_grad():
+        _, _, d, i = knn_aggregate_aniso(*[x.detach() for x in ins], shape.K)
+    q, p, f, sg, R = t
+    _, _, d_or, i_or = O.forward_f32(q[:, :sample], p, f, sg, R, shape.K, with_features=False)
+    match = bool((i[:, :sample].cpu().numpy() == i_or).all() and
+                 (d[:, :sample].cpu().numpy().view("int32") == d_or.view("int32")).all())
+    out = {"workload": "sphere: B=1 P=131072 sphere surface (radial noise 0.01, R third column = normal, "
+                       "sigma (0.02,0.02,0.005)), Q=524288 surface + N(0,0.05) queries, F=128, K=16; "
+                       "fwd + dq(create_graph) + Eikonal backward",
+           "ms_per_step": ms, "value": units / (ms / 1e3), "unit": UNIT, "execution": "CUDA graph replay",
+           "pairs": shape.B * shape.Q * shape.P, "idxs_dists_bit_exact_vs_oracle_sample": match,
+           "oracle_sample_queries": sample}
+    del g
+    ref, why = load_reference_ext() if with_reference else (None, "skipped (--no-reference-ext)")
+    if ref is None:
+        out["reference_ext"] = {"unavailable": why}
+    else:
+        rstep = eikonal_step_fn(reference_ext_op(ref), ins, shape.K)
+        rstep()
+        torch.cuda.synchronize()
+        tr = []
+        for _ in range(ref_steps):
+            flush.zero_()
+            e0, e1 = _events()
+            e0.record()
+            rstep()
+            e1.record()
+            e1.synchronize()
+            tr.append(e0.elapsed_time(e1))
+        mr = statistics.median(tr)
+        out["reference_ext"] = {"ms_per_step": mr, "value": units / (mr / 1e3), "steps": ref_steps}
+        out["speedup_vs_reference"] = mr / ms
+    return out
+
+
 def _prefix(xs):
     a, o = 0, []
     for x in xs:
@@ -627,6 +702,8 @@ def run_ours(args):
             out["reference_ext"]["speedup_e2e"] = out["reference_ext"]["ms_per_step"] / e2e_ms
     if ws == 1 and not args.no_ragged:
         out["ragged"] = ragged_block(device, with_reference=not args.no_reference_ext)
+    if ws == 1 and not args.no_sphere:
+        out["sphere"] = sphere_block(device, with_reference=not args.no_reference_ext)
     if ws == 1 and not args.no_served:
         out["served"] = served_block(device)
         out["served_p50_ms"] = out["served"].get("p50_ms")
@@ -684,7 +761,8 @@ def main():
     ap.add_argument("--no-reference-ext", action="store_true")
     ap.add_argument("--no-ragged", action="store_true", help="skip the ragged-batch block")
     ap.add_argument("--no-served", action="store_true", help="skip the serving block")
-    ap.add_argument("--workload", default="table", choices=["table", "ragged", "served"],
+    ap.add_argument("--no-sphere", action="store_true", help="skip the large single-cloud block")
+    ap.add_argument("--workload", default="table", choices=["table", "ragged", "served", "sphere"],
                     help="table: the headline line (with the ragged and served blocks attached); ragged / "
                          "served: only that block, as its own JSON line (for profiling)")
     args = ap.parse_args()
@@ -692,8 +770,12 @@ def main():
     if args.workload != "table" and args.impl == "ours":
         device = torch.device("cuda", 0)
         torch.cuda.set_device(device)
-        blk = ragged_block(device, with_reference=not args.no_reference_ext) if args.workload == "ragged" \
-            else served_block(device)
+        if args.workload == "ragged":
+            blk = ragged_block(device, with_reference=not args.no_reference_ext)
+        elif args.workload == "sphere":
+            blk = sphere_block(device, with_reference=not args.no_reference_ext)
+        else:
+            blk = served_block(device)
         print(json.dumps(blk), flush=True)
         return
     if args.impl == "reference":

@@ -107,6 +107,7 @@ class KNNAnisotropicAggregate(torch.autograd.Function):
     def forward(ctx, q, p, f, sigma, R, K):
         f_out, w_out, dists, idxs, points = _C.forward_ex(q, p, f, sigma, R, int(K))
         ctx.save_for_backward(q, p, f, sigma, R, idxs)
+        ctx.set_materialize_grads(False)  # unused output grads arrive as None, not zero tensors
         ctx.aux = _Aux(points, p.shape[1], tuple(bool(x) for x in ctx.needs_input_grad[:5]))
         return f_out, w_out, dists, idxs
 
@@ -128,6 +129,7 @@ class KNNLookupAnisotropicAggregate(KNNAnisotropicAggregate):
     def forward(ctx, q, p, f, sigma, R, knn_table, K):
         f_out, w_out, dists, idxs = _C.knn_lookup_aggregate_aniso_forward(q, p, f, sigma, R, knn_table, int(K))
         ctx.save_for_backward(q, p, f, sigma, R, idxs)
+        ctx.set_materialize_grads(False)
         ctx.aux = _Aux(None, p.shape[1], tuple(bool(x) for x in ctx.needs_input_grad[:5]))
         return f_out, w_out, dists, idxs
 
@@ -147,6 +149,7 @@ class KNNPrecomputedAnisotropicAggregate(KNNAnisotropicAggregate):
     def forward(ctx, q, p, f, sigma, R, knn_idxs, K):
         f_out, w_out, dists = _C.knn_precomputed_aggregate_aniso_forward(q, p, f, sigma, R, knn_idxs, int(K))
         ctx.save_for_backward(q, p, f, sigma, R, knn_idxs)
+        ctx.set_materialize_grads(False)
         ctx.aux = _Aux(None, p.shape[1], tuple(bool(x) for x in ctx.needs_input_grad[:5]))
         return f_out, w_out, dists
 
@@ -180,6 +183,7 @@ class KNNAnisotropicAggregateBackward(torch.autograd.Function):
             dq, dp, df, ds, dR, coef = _C.backward_ex(grad_f_out, q, p, f, sigma, R, idxs, aux.points, adj, needs)
             outs = [dq, dp, df, ds, dR]
         ctx.save_for_backward(grad_f_out, q, p, f, sigma, R, idxs, coef)
+        ctx.set_materialize_grads(False)  # only grad of dq is used (Eikonal); the rest stay None
         ctx.aux = aux
         ctx.has_w = w_out is not None
         return tuple(outs)
