@@ -18,6 +18,9 @@ static std::atomic<void*> g_ev_begin{nullptr}, g_ev_end{nullptr};
 
 void note_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+static std::atomic<int> g_search_splits{0};
+int search_splits_setting() { return g_search_splits.load(std::memory_order_relaxed); }
+
 // Record a profiling event on `st`: as an external event node while the
 // stream is being captured into a graph, as a plain record otherwise.  A
 // failed record is cleared so it cannot be mistaken for a launch error.
@@ -323,6 +326,14 @@ void knnag_set_profile_events(void* ev_begin, void* ev_end) {
 }
 
 long long knnag_launch_count(void) { return g_launches.load(); }
+
+int knnag_set_search_splits(int splits) {
+  if (splits != 0 && splits != 1 && splits != 2 && splits != 4) return KNNAG_ERR_ARG;
+  g_search_splits.store(splits, std::memory_order_relaxed);
+  return KNNAG_OK;
+}
+
+int knnag_get_search_splits(void) { return g_search_splits.load(std::memory_order_relaxed); }
 
 int knnag_fp32_peak_probe(float* out, int blocks, int iters, void* stream) {
   if (!out || blocks < 1 || iters < 1) return KNNAG_ERR_ARG;

@@ -150,6 +150,10 @@ struct AdjLayout {
 };
 AdjLayout adj_layout(int B, int Q, int P, int K);
 
+// Process-wide split count of the uniform search (0: automatic), set by
+// knnag_set_search_splits (defined in knn_capi.cu).
+int search_splits_setting();
+
 // Instrumentation shared by the .cu files (defined in knn_capi.cu).
 void note_launches(int n);
 void profile_begin(cudaStream_t st);

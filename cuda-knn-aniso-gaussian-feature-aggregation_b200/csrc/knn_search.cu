@@ -442,6 +442,9 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   int* qv = reinterpret_cast<int*>(qk + kQueueCap * kSearchThreads);
   float* tau_share = reinterpret_cast<float*>(qv + kQueueCap * kSearchThreads);  // [2][128]
   uint64_t* full = reinterpret_cast<uint64_t*>(tau_share + 2 * kSearchThreads);
+  int* cnt = reinterpret_cast<int*>(full + 2);                       // [2] warps done per buffer
+  volatile int* s_final = reinterpret_cast<volatile int*>(cnt + 2);  // visit count once stopped
+  volatile int* s_abort = s_final + 1;                               // a wait gave up
   // region C: per-tile lower bounds (sorted), visit order, query bookkeeping
   const int NTP = search_tiles_pow2(it.ntile);
   float* lbk = reinterpret_cast<float*>(smem + RA + RB);
@@ -470,6 +473,10 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   const float2 qx2 = make_float2(qx, qx), qy2 = make_float2(qy, qy), qz2 = make_float2(qz, qz);
   const float* recb = it.rec;
   if (split == 0) qorig[lq] = valid ? qi : -1;
+  // thresholds published by the warps of this item (read without barriers:
+  // any value written here is a valid bound, so it must not be a stale one
+  // from the previous item)
+  tau_share[split * QPC + lq] = INFINITY;
 
   // MinK's fill phase stores points 0..K-1 whatever their key: a NaN there
   // changes the result in ways only the replay reproduces.
@@ -553,8 +560,9 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     mbar_arrive_expect_tx(&full[buf], kTileBytes);
     bulk_copy_g2s(regA + buf * kTileBytes, pairs_b + (int64_t)lbt[v] * PPT * kPairFloats, kTileBytes, &full[buf]);
   };
-  // thread 0 only: issue position v unless its bound exceeds every threshold
-  // (the order is ascending, so nothing after it is needed either)
+  // Issue position v unless its bound exceeds every threshold (the order is
+  // ascending, so nothing after it is needed either).  Decisions are made
+  // one visit at a time, in order (see below), so *s_nvisit == v here.
   auto decide = [&](int v, float tmax) {
     if (v < ntile && *s_nvisit == v && lbt[v] < ntile && !(lbk[v] > tmax)) {
       *s_nvisit = v + 1;
@@ -562,18 +570,49 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     }
     return false;
   };
+  // No visit v: record the count and complete buffer v&1's next phase with a
+  // plain arrive, so the warps waiting for visit v wake up and stop.
+  auto stop = [&](int v) {
+    *s_final = v;
+    __threadfence_block();
+    mbar_arrive(&full[v & 1]);
+  };
   if (tid == 0) {
     *s_nvisit = 0;
+    *s_final = 0x7fffffff;
+    *s_abort = 0;
+    cnt[0] = cnt[1] = 0;
     fence_proxy_async_smem();  // region A was last written by generic stores
-    for (int v = 0; v < 2; ++v)
-      if (decide(v, INFINITY)) issue(v);
+    for (int v = 0; v < 2; ++v) {
+      if (decide(v, INFINITY)) {
+        issue(v);
+      } else {
+        stop(v);
+        break;
+      }
+    }
   }
   __syncthreads();
 
+  // Tile loop without CTA barriers.  Visit t sits in buffer t & 1; each warp
+  // waits for its copy, reads its split of the pairs, publishes its list top
+  // in tau_share and counts itself out of the tile.  The warp that counts
+  // out last knows every warp is done with the buffer: it re-arms the counter
+  // and decides (and issues) visit t + 2 into the same buffer.  A warp does
+  // that duty before it starts its next tile, so the decision for t + 1 is
+  // complete before any warp can be last for tile t: decisions stay in order.
   int t = 0;
-  for (; t < *s_nvisit; ++t) {
+  for (;; ++t) {
     const int buf = t & 1;
     const bool ok = mbar_wait_bounded(&full[buf], (uses[buf] + (t >> 1)) & 1);
+    if (!ok) {
+      if (lane == 0) {
+        atomicOr(a.status, kStatusWaitTimeout);
+        *s_abort = 1;
+      }
+      break;
+    }
+    if (*s_abort || t >= *s_final) break;
     const float4* tp = reinterpret_cast<const float4*>(regA + buf * kTileBytes) + split * PPS * 8;
     // Per-warp culling: the CTA visits a tile when it may matter to any of
     // its query groups; a warp whose own query box bounds every key of the
@@ -610,19 +649,22 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
       if (__any_sync(0xffffffffu, qn > kQueueCap - 2)) flush_queue<L>(keys, vals, qn, tie_key, tau, qk, qv, tid);
     }
     flush_queue<L>(keys, vals, qn, tie_key, tau, qk, qv, tid);
-    tau_share[buf * kSearchThreads + split * QPC + lq] = keys[L - 1];
-    const int abort = __syncthreads_or(!ok);
-    if (abort) {
-      if (tid == 0) {
-        atomicOr(a.status, kStatusWaitTimeout);
-        mbar_wait_bounded(&full[buf], (uses[buf] + (t >> 1)) & 1);
-        if (*s_nvisit > t + 1) mbar_wait_bounded(&full[buf ^ 1], (uses[buf ^ 1] + ((t + 1) >> 1)) & 1);
-      }
-      return false;
+    tau_share[split * QPC + lq] = keys[L - 1];
+    // count this warp out of the tile (release: its reads of the buffer and
+    // its tau_share write come first)
+    __syncwarp();
+    int last = 0;
+    if (lane == 0) {
+      __threadfence_block();
+      last = atomicAdd(&cnt[buf], 1) == kSearchThreads / 32 - 1;
+      if (last) __threadfence_block();
     }
+    last = __shfl_sync(0xffffffffu, last, 0);
     if (seed && t == kSeedTiles - 1) {
-      // Both tile buffers are free (the next copies are deferred until now):
-      // merge the G lists of every query into split 0, restart the others.
+      // All warps are done with both tile buffers once they meet here (the
+      // next copies are deferred until now): merge the G lists of every
+      // query into split 0, restart the others.
+      __syncthreads();
       const int slot = split * QPC + lq;
 #pragma unroll
       for (int s = 0; s < L; ++s) {
@@ -647,43 +689,73 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
         }
       }
       tau = fminf(tau, tau0);
+      tau_share[split * QPC + lq] = keys[L - 1];
       float tmax = -INFINITY;
       if (warp == 0) {
         for (int i = lane; i < QPC; i += 32) tmax = fmaxf(tmax, mf[i]);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
       }
-      bool go[2] = {false, false};
-      if (tid == 0)
-        for (int v = kSeedTiles; v < kSeedTiles + 2; ++v) go[v - kSeedTiles] = decide(v, tmax);
-      __syncthreads();
+      __syncthreads();  // everyone has read the merge data in region A before new copies land
       if (tid == 0) {
+        cnt[buf] = 0;
         fence_proxy_async_smem();
-        for (int v = kSeedTiles; v < kSeedTiles + 2; ++v)
-          if (go[v - kSeedTiles]) issue(v);
+        for (int v = kSeedTiles; v < kSeedTiles + 2; ++v) {
+          if (decide(v, tmax)) {
+            issue(v);
+          } else {
+            stop(v);
+            break;
+          }
+        }
       }
       continue;
     }
     float tm = keys[L - 1];
 #pragma unroll
-    for (int g = 0; g < G; ++g) tm = fminf(tm, tau_share[buf * kSearchThreads + g * QPC + lq]);
+    for (int g = 0; g < G; ++g) tm = fminf(tm, tau_share[g * QPC + lq]);
     tau = fminf(tau, tm);
-    const bool deferred = seed && t < kSeedTiles - 1;
-    if (warp == 0 && !deferred) {
+    if (last) {
+      // every warp is done with this buffer: re-arm its counter, then decide
+      // visit t + 2 (deferred during the seed tiles) unless a stop was made
+      const bool deferred = seed && t < kSeedTiles - 1;
       float tmax = -INFINITY;
+      if (!deferred) {
 #pragma unroll
-      for (int i = 0; i < kSearchThreads / 32; ++i) tmax = fmaxf(tmax, tau_share[buf * kSearchThreads + i * 32 + lane]);
+        for (int i = 0; i < kSearchThreads / 32; ++i) tmax = fmaxf(tmax, tau_share[i * 32 + lane]);
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
-      if (lane == 0 && decide(t + 2, tmax)) {
-        fence_proxy_async_smem();
-        issue(t + 2);
+        for (int o = 16; o > 0; o >>= 1) tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
+      }
+      if (lane == 0) {
+        cnt[buf] = 0;
+        if (!deferred && *s_final == 0x7fffffff && !*s_abort) {
+          if (decide(t + 2, tmax)) {
+            fence_proxy_async_smem();
+            issue(t + 2);
+          } else {
+            stop(t + 2);
+          }
+        }
       }
     }
   }
-
-  uses[0] += (t + 1) >> 1;
-  uses[1] += t >> 1;
+  // Every warp has left the loop once all meet here; no copy is in flight
+  // then (each issued visit was waited for by every warp), unless a wait
+  // gave up.
+  __syncthreads();
+  if (*s_abort) {
+    if (tid == 0) {
+      // best effort: let the copies of the last two issued visits land
+      for (int v = *s_nvisit - 2; v < *s_nvisit; ++v)
+        if (v >= 0) mbar_wait_bounded(&full[v & 1], (uses[v & 1] + (v >> 1)) & 1);
+    }
+    return false;
+  }
+  {
+    const int n = t + 1;  // phases waited on: visits 0..t (t = the stop visit)
+    uses[0] += (n + 1) >> 1;
+    uses[1] += n >> 1;
+  }
 
   // ---- merge the G split lists; region A is free (no copy in flight, all
   // tile reads ended before the last barrier).
@@ -944,8 +1016,11 @@ int launch_search_k(const SearchParams& a, int G, cudaStream_t st) {
   return launch_search_t<KMAX, 4>(a, st);
 }
 
-// Splits per query group: the fewest that still give ~4 CTAs per SM.
+// Splits per query group: the process-wide setting when one is made
+// (knnag_set_search_splits), else the fewest that still give ~4 CTAs per SM.
 int choose_splits(int B, int Q, int dev) {
+  const int forced = search_splits_setting();
+  if (forced == 1 || forced == 2 || forced == 4) return forced;
   const int64_t target = (int64_t)num_sms(dev) * 4;
   for (int g = 1; g <= 4; g *= 2) {
     const int qpc = 32 * (4 / g);

@@ -57,6 +57,8 @@ _SIGS = {
     "knnag_set_profile_events": ([_V, _V], None),
     "knnag_launch_count": ([], ctypes.c_longlong),
     "knnag_fp32_peak_probe": ([_V, _I, _I, _V], _I),
+    "knnag_set_search_splits": ([_I], _I),
+    "knnag_get_search_splits": ([], _I),
 }
 
 _lib = None
@@ -236,3 +238,12 @@ def launch_count():
 
 def fp32_peak_probe(out, blocks, iters):
     _check(lib().knnag_fp32_peak_probe(_p(out), blocks, iters, _stream(out.device)))
+
+
+def set_search_splits(splits):
+    """Process-wide split count of the uniform search (0: automatic)."""
+    _check(lib().knnag_set_search_splits(int(splits)))
+
+
+def search_splits():
+    return int(lib().knnag_get_search_splits())

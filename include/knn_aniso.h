@@ -301,6 +301,15 @@ void knnag_set_profile_events(void* ev_begin, void* ev_end);
 /* Process-wide count of kernels this library has launched so far. */
 long long knnag_launch_count(void);
 
+/* Tuning: warps per 32-query group (1, 2 or 4) of the FP32 search of every
+ * later knnag_forward / knnag_forward_noalloc in the process (the autotuner
+ * sets it from timings cached per shape bucket); 0 restores the automatic
+ * choice (the fewest splits that still give about 4 CTAs per SM).  Results
+ * do not depend on it.  Returns KNNAG_ERR_ARG for other values.  No
+ * reference counterpart. */
+int knnag_set_search_splits(int splits);
+int knnag_get_search_splits(void);
+
 /* Launch an FFMA-bound kernel (blocks x 256 threads, `iters` iterations of 16
  * independent FMA chains per thread, 32*iters FLOP per thread) writing one
  * float per thread to `out`; used to measure the FP32 peak the search kernel

@@ -173,3 +173,32 @@ def test_capi_rejects_bad_arguments():
     with pytest.raises(RuntimeError, match="K must satisfy"):
         C.forward(q, p, torch.rand(1, 5, 2, device=dev), torch.rand(1, 5, 3, device=dev),
                   torch.rand(1, 5, 3, 3, device=dev), 6)
+
+
+@pytest.mark.gpu
+def test_search_splits_setting_does_not_change_results():
+    """The process-wide split setting (and the autotuner that picks it)
+    changes only the time: every split gives identical outputs."""
+    import cuda_knn_aggregate as C
+    from cuda_knn_aggregate import capi, tuning
+    from cuda_knn_aggregate import workloads as W
+
+    _, t = W.make("table", Q=3000, P=2000, seed=77)
+    ins = [x.cuda() for x in t]
+    outs = []
+    try:
+        for g in (1, 2, 4, 0):
+            capi.set_search_splits(g)
+            outs.append(C._C.knn_aggregate_aniso_forward(*ins, 16))
+        best = tuning.autotune_search_splits(*ins, 16)
+        assert best in (1, 2, 4)
+        tuning.use_tuned(ins[0], ins[1], 16)
+        assert capi.search_splits() == best
+        outs.append(C._C.knn_aggregate_aniso_forward(*ins, 16))
+    finally:
+        capi.set_search_splits(0)
+    for o in outs[1:]:
+        for a, b in zip(o, outs[0]):
+            assert torch.equal(a, b)
+    with pytest.raises(RuntimeError):
+        capi.set_search_splits(3)
