@@ -510,34 +510,64 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     bmax[c] = fmaxf(fmaxf(qbox[3 + c], qbox[9 + c]), fmaxf(qbox[15 + c], qbox[21 + c]));
   }
   const float* tinfo_b = it.tinfo;
-  for (int t = tid; t < NTP; t += kSearchThreads) {
-    float lb = INFINITY;
-    if (t < it.ntile) {
-      const float* ti = tinfo_b + t * 8;
-      lb = tile_lower_bound(ti, bmin, bmax);
-      lb = fminf(lb, 3.4e38f);  // real tiles sort before the +inf padding entries
-    }
-    lbk[t] = lb;
-    lbt[t] = t;
-  }
-  __syncthreads();
-  for (int kk = 2; kk <= NTP; kk <<= 1) {  // bitonic sort of (bound, tile) ascending
-    for (int j = kk >> 1; j > 0; j >>= 1) {
-      for (int i = tid; i < NTP; i += kSearchThreads) {
-        const int ixj = i ^ j;
-        if (ixj > i) {
-          const bool up = (i & kk) == 0;
-          const float ki = lbk[i], kj = lbk[ixj];
-          if ((ki > kj) == up) {
-            lbk[i] = kj;
-            lbk[ixj] = ki;
-            const int ti = lbt[i];
-            lbt[i] = lbt[ixj];
-            lbt[ixj] = ti;
+  if (NTP <= 32) {
+    // Up to 32 tiles: warp 0 computes the bounds and sorts (bound, tile)
+    // ascending in registers with a shuffle bitonic network (ties by tile).
+    if (warp == 0) {
+      float lb = INFINITY;
+      int ti = lane;
+      if (lane < it.ntile) lb = fminf(tile_lower_bound(tinfo_b + lane * 8, bmin, bmax), 3.4e38f);
+#pragma unroll
+      for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+        for (int j = kk >> 1; j > 0; j >>= 1) {
+          const float ok = __shfl_xor_sync(0xffffffffu, lb, j);
+          const int oi = __shfl_xor_sync(0xffffffffu, ti, j);
+          const bool up = (lane & kk) == 0;
+          const bool lower = (lane & j) == 0;
+          const bool other_less = ok < lb || (ok == lb && oi < ti);
+          if (lower == up ? other_less : !other_less) {
+            lb = ok;
+            ti = oi;
           }
         }
       }
-      __syncthreads();
+      if (lane < NTP) {
+        lbk[lane] = lb;
+        lbt[lane] = ti;
+      }
+    }
+    __syncthreads();
+  } else {
+    for (int t = tid; t < NTP; t += kSearchThreads) {
+      float lb = INFINITY;
+      if (t < it.ntile) {
+        const float* ti = tinfo_b + t * 8;
+        lb = tile_lower_bound(ti, bmin, bmax);
+        lb = fminf(lb, 3.4e38f);  // real tiles sort before the +inf padding entries
+      }
+      lbk[t] = lb;
+      lbt[t] = t;
+    }
+    __syncthreads();
+    for (int kk = 2; kk <= NTP; kk <<= 1) {  // bitonic sort of (bound, tile) ascending
+      for (int j = kk >> 1; j > 0; j >>= 1) {
+        for (int i = tid; i < NTP; i += kSearchThreads) {
+          const int ixj = i ^ j;
+          if (ixj > i) {
+            const bool up = (i & kk) == 0;
+            const float ki = lbk[i], kj = lbk[ixj];
+            if ((ki > kj) == up) {
+              lbk[i] = kj;
+              lbk[ixj] = ki;
+              const int ti = lbt[i];
+              lbt[i] = lbt[ixj];
+              lbt[ixj] = ti;
+            }
+          }
+        }
+        __syncthreads();
+      }
     }
   }
 
