@@ -323,6 +323,96 @@ std::vector<torch::Tensor> backward2_ex(torch::Tensor ggq, torch::Tensor gfo, to
   return backward_impl(2, ggq, gfo, q, p, f, sigma, R, c10::nullopt, idxs, points, adjacency, coef, needs, false);
 }
 
+// ------------------------------------------------------------- autograd
+//
+// The autograd pair of knn_aggregate_aniso (reference
+// cuda_knn_aggregate/__init__.py:64-117, 216-289) as C++ Functions.  Inside
+// a C++ backward, ctx->needs_input_grad(i) asks the running graph task
+// whether input i's gradient is used -- autograd.grad(f_out.sum(), q), the
+// first step of an Eikonal loss, uses only dq -- so each order computes only
+// the gradients that are used (the point-side kernels and the adjacency are
+// skipped when no point gradient is wanted).  Only f_out is differentiable;
+// the second order flows only through dq.  Outputs that are not computed are
+// zero-size placeholders that are never returned as gradients.
+
+using torch::autograd::AutogradContext;
+using torch::autograd::variable_list;
+
+constexpr int64_t kNeedBits[5] = {KNNAG_NEED_DQ, KNNAG_NEED_DP, KNNAG_NEED_DF, KNNAG_NEED_DSIGMA, KNNAG_NEED_DR};
+constexpr int64_t kPointBits = KNNAG_NEED_DP | KNNAG_NEED_DF | KNNAG_NEED_DSIGMA | KNNAG_NEED_DR;
+
+torch::Tensor or_placeholder(const torch::Tensor& t, const torch::Tensor& like) {
+  return t.defined() ? t : torch::empty({0}, like.options());
+}
+
+struct AggBackwardFn : public torch::autograd::Function<AggBackwardFn> {
+  // differentiable inputs: gfo, q, p, f, sigma, R; then idxs, points (no grad)
+  static variable_list forward(AutogradContext* ctx, torch::Tensor gfo, torch::Tensor q, torch::Tensor p,
+                               torch::Tensor f, torch::Tensor sigma, torch::Tensor R, torch::Tensor idxs,
+                               torch::Tensor points, int64_t needs) {
+    torch::Tensor adj;
+    if (needs & kPointBits) adj = build_adjacency(idxs, p.size(1));
+    auto o = backward_impl(1, c10::nullopt, gfo, q, p, f, sigma, R, c10::nullopt, idxs, points,
+                           adj.defined() ? c10::optional<torch::Tensor>(adj) : c10::nullopt, c10::nullopt, needs,
+                           true);
+    ctx->save_for_backward({gfo, q, p, f, sigma, R, idxs, points});
+    ctx->saved_data["coef"] = o[5];
+    if (adj.defined()) ctx->saved_data["adj"] = adj;
+    ctx->set_materialize_grads(false);
+    return {or_placeholder(o[0], q), or_placeholder(o[1], q), or_placeholder(o[2], q), or_placeholder(o[3], q),
+            or_placeholder(o[4], q)};
+  }
+
+  static variable_list backward(AutogradContext* ctx, variable_list gg) {
+    variable_list out(9);
+    if (gg.empty() || !gg[0].defined()) return out;  // only dq is differentiated
+    int64_t needs = 0;
+    if (ctx->needs_input_grad(0)) needs |= KNNAG_NEED_DGFO;
+    for (int i = 0; i < 5; ++i)
+      if (ctx->needs_input_grad(1 + i)) needs |= kNeedBits[i];
+    if (!needs) return out;
+    auto s = ctx->get_saved_variables();
+    torch::Tensor adj;
+    if (ctx->saved_data.count("adj")) adj = ctx->saved_data["adj"].toTensor();
+    if ((needs & kPointBits) && !adj.defined()) adj = build_adjacency(s[6], s[2].size(1));
+    auto o = backward_impl(2, gg[0].contiguous(), s[0], s[1], s[2], s[3], s[4], s[5], c10::nullopt, s[6], s[7],
+                           adj.defined() ? c10::optional<torch::Tensor>(adj) : c10::nullopt,
+                           ctx->saved_data["coef"].toTensor(), needs, false);
+    for (int i = 0; i < 6; ++i) out[i] = o[i];
+    return out;
+  }
+};
+
+struct AggFn : public torch::autograd::Function<AggFn> {
+  static variable_list forward(AutogradContext* ctx, torch::Tensor q, torch::Tensor p, torch::Tensor f,
+                               torch::Tensor sigma, torch::Tensor R, int64_t K) {
+    auto o = forward_impl(q, p, f, sigma, R, K, true);
+    ctx->save_for_backward({q, p, f, sigma, R, o[3]});
+    ctx->saved_data["points"] = o[4];
+    ctx->set_materialize_grads(false);
+    return {o[0], o[1], o[2], o[3]};
+  }
+
+  static variable_list backward(AutogradContext* ctx, variable_list g) {
+    variable_list out(6);
+    if (g.empty() || !g[0].defined()) return out;  // grad_w_out / grad_dists are not propagated
+    int64_t needs = 0;
+    for (int i = 0; i < 5; ++i)
+      if (ctx->needs_input_grad(i)) needs |= kNeedBits[i];
+    if (!needs) return out;
+    auto s = ctx->get_saved_variables();
+    auto r = AggBackwardFn::apply(g[0].contiguous(), s[0], s[1], s[2], s[3], s[4], s[5],
+                                  ctx->saved_data["points"].toTensor(), needs);
+    for (int i = 0; i < 5; ++i) out[i] = (needs & kNeedBits[i]) ? r[i] : torch::Tensor();
+    return out;
+  }
+};
+
+std::vector<torch::Tensor> knn_aggregate_aniso_autograd(torch::Tensor q, torch::Tensor p, torch::Tensor f,
+                                                        torch::Tensor sigma, torch::Tensor R, int64_t K) {
+  return AggFn::apply(q, p, f, sigma, R, K);
+}
+
 }  // namespace
 
 PYBIND11_MODULE(_C, m) {
@@ -335,6 +425,8 @@ PYBIND11_MODULE(_C, m) {
   m.def("knn_precomputed_aggregate_aniso_forward", &knn_precomputed_aggregate_aniso_forward,
         "KNN precomputed aggregate aniso forward");
   m.def("forward_ex", &forward_ex, "forward that also returns the packed point records");
+  m.def("knn_aggregate_aniso_autograd", &knn_aggregate_aniso_autograd,
+        "differentiable forward (C++ autograd Functions; gradients computed only where the graph task uses them)");
   m.def("build_adjacency", &build_adjacency, "point -> entry adjacency (CSR) of idxs");
   m.def("adjacency_views", &adjacency_views, "rowptr / entry views of an adjacency buffer");
   m.def("backward_ex", &backward_ex, "first-order adjoint with selectable outputs; also returns coef");

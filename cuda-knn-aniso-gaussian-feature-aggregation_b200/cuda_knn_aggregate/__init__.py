@@ -99,9 +99,28 @@ def _mask(flags):
     return m
 
 
-class KNNAnisotropicAggregate(torch.autograd.Function):
+class KNNAnisotropicAggregate:
     """Fused kNN search and aggregation (reference
-    ``cuda_knn_aggregate/__init__.py:64-117``)."""
+    ``cuda_knn_aggregate/__init__.py:64-117``):
+    ``KNNAnisotropicAggregate.apply(q, p, f, sigma, R, K)`` returns
+    ``(f_out, w_out, dists, idxs)``.
+
+    The autograd nodes are C++ Functions of the extension: their backward
+    asks the running graph task which input gradients are used, so e.g.
+    ``autograd.grad(f_out.sum(), q, create_graph=True)`` (the first step of
+    an Eikonal loss) computes dq only, and the following ``backward()``
+    computes the second-order gradients only for inputs that need them.
+    """
+
+    @staticmethod
+    def apply(q, p, f, sigma, R, K):
+        return tuple(_C.knn_aggregate_aniso_autograd(q, p, f, sigma, R, int(K)))
+
+
+class _AggregatePy(torch.autograd.Function):
+    """Python autograd Function of the fused op; base of the lookup and
+    precomputed variants (whose backward is the same adjoint at their
+    indices)."""
 
     @staticmethod
     def forward(ctx, q, p, f, sigma, R, K):
@@ -121,9 +140,9 @@ class KNNAnisotropicAggregate(torch.autograd.Function):
         return (*grads, None)
 
 
-class KNNLookupAnisotropicAggregate(KNNAnisotropicAggregate):
-    """Lookup variant (reference ``__init__.py:120-165``); gradients as
-    KNNAnisotropicAggregate at the looked-up indices, none for the table."""
+class KNNLookupAnisotropicAggregate(_AggregatePy):
+    """Lookup variant (reference ``__init__.py:120-165``); gradients as the
+    fused op's at the looked-up indices, none for the table."""
 
     @staticmethod
     def forward(ctx, q, p, f, sigma, R, knn_table, K):
@@ -135,10 +154,10 @@ class KNNLookupAnisotropicAggregate(KNNAnisotropicAggregate):
 
     @staticmethod
     def backward(ctx, grad_f_out, grad_w_out, grad_dists, grad_idxs):
-        return KNNAnisotropicAggregate.backward(ctx, grad_f_out, grad_w_out, grad_dists, grad_idxs) + (None,)
+        return _AggregatePy.backward(ctx, grad_f_out, grad_w_out, grad_dists, grad_idxs) + (None,)
 
 
-class KNNPrecomputedAnisotropicAggregate(KNNAnisotropicAggregate):
+class KNNPrecomputedAnisotropicAggregate(_AggregatePy):
     """Aggregation at caller-given neighbour indices (reference
     ``__init__.py:167-213``): returns f_out, w_out, dists; gradients as
     KNNAnisotropicAggregate, none for the indices.  (The reference's backward
@@ -155,7 +174,7 @@ class KNNPrecomputedAnisotropicAggregate(KNNAnisotropicAggregate):
 
     @staticmethod
     def backward(ctx, grad_f_out, grad_w_out, grad_dists):
-        return KNNAnisotropicAggregate.backward(ctx, grad_f_out, grad_w_out, grad_dists, None) + (None,)
+        return _AggregatePy.backward(ctx, grad_f_out, grad_w_out, grad_dists, None) + (None,)
 
 
 class KNNAnisotropicAggregateBackward(torch.autograd.Function):

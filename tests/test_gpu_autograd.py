@@ -165,3 +165,33 @@ def test_step_is_capturable_in_a_cuda_graph():
     assert torch.equal(out, eager)
     for a, e in zip(ins, eager_grads):
         assert torch.equal(a.grad, e)
+
+
+@pytest.mark.gpu
+def test_backward_computes_only_requested_gradients():
+    """The autograd nodes ask the running graph task which gradients are
+    used: autograd.grad(f_out.sum(), q) launches fewer kernels than a request
+    for every input (no point-side kernels, no adjacency), with identical dq;
+    the Eikonal second order then still gives every input's gradient."""
+    import cuda_knn_aggregate as C
+    from cuda_knn_aggregate import capi
+    from cuda_knn_aggregate import workloads as W
+
+    _, t = W.make("small", seed=5)
+    ins = [x.cuda().requires_grad_(True) for x in t]
+    f_out = C.knn_aggregate_aniso(*ins, 12)[0]
+    c0 = capi.launch_count()
+    (dq_only,) = torch.autograd.grad(f_out.sum(), ins[0], retain_graph=True)
+    torch.cuda.synchronize()
+    n_q = capi.launch_count() - c0
+    c0 = capi.launch_count()
+    grads_all = torch.autograd.grad(f_out.sum(), ins, retain_graph=True)
+    torch.cuda.synchronize()
+    n_all = capi.launch_count() - c0
+    assert n_q < n_all
+    assert torch.equal(dq_only, grads_all[0])
+    # Eikonal step: every input gets a second-order gradient
+    (gq,) = torch.autograd.grad(f_out.sum(), ins[0], create_graph=True)
+    ((gq.norm(dim=-1) - 1.0) ** 2).mean().backward()
+    for x in ins:
+        assert x.grad is not None and torch.isfinite(x.grad).all()
