@@ -524,7 +524,7 @@ def served_block(device, seconds_per_rate=2.0, loads=(0.5, 0.8, 0.95)):
                 fo = knn_aggregate_aniso(qd, pc[None], fc[None], sc[None], Rc[None], r.K)[0]
         fo_host[:Q].copy_(fo[0].detach(), non_blocking=True)
 
-    for r in reqs[:5]:
+    for r in reqs:  # warm-up pass over every request shape
         plain(r)
     torch.cuda.synchronize()
     t0 = time.perf_counter()

@@ -179,8 +179,10 @@ struct BwdArgs {
 };
 int backward_impl(const BwdArgs& x, cudaStream_t st);
 
+// Packs the point records; block 0 also zeroes zero_words[0..n_zero) (a
+// call's status words) so no separate memset is needed.
 int launch_pack_points(const void* p, const void* sigma, const void* R, int B, int P, int dtype, void* rec,
-                       cudaStream_t st);
+                       cudaStream_t st, int* zero_words = nullptr, int n_zero = 0);
 int forward_impl(const void* q, const void* p, const void* f, const void* sigma, const void* R, int B, int Q,
                  int P, int F, int K, int dtype, void* f_out, void* w_out, void* dists, int64_t* idxs,
                  void* points, void* workspace, cudaStream_t st);

@@ -16,7 +16,9 @@ namespace knnag {
 // rec[(b*P+i)*16 + field]: -p, R (row-major), sigma, pad.
 template <typename T>
 __global__ void pack_points_kernel(const T* __restrict__ p, const T* __restrict__ sigma,
-                                   const T* __restrict__ R, int64_t n_points, T* __restrict__ rec) {
+                                   const T* __restrict__ R, int64_t n_points, T* __restrict__ rec,
+                                   int* __restrict__ zero_words, int n_zero) {
+  if (blockIdx.x == 0 && (int)threadIdx.x < n_zero) zero_words[threadIdx.x] = 0;  // the call's status words
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_points;
        i += (int64_t)gridDim.x * blockDim.x) {
     T v[kRecLen];
@@ -1118,14 +1120,14 @@ FwdLayout fwd_layout(int B, int Q, int P, int K, int dtype, bool own_rec) {
     off += align256((size_t)B * L.P_pad * kRecLen * 4);
     L.bounds = off;
     off += align256((size_t)B * 8 * 4);
+    // point and query cells of each batch element, sorted together
     L.cell_count = off;
-    off += align256((size_t)B * cells * 4);
+    off += align256(2 * (size_t)B * cells * 4);
     L.cell_offset = off;
-    off += align256(((size_t)B * cells + 1) * 4);
-    L.perm_p = off;
-    off += align256((size_t)B * P * 4);
-    L.perm_q = off;
-    off += align256((size_t)B * Q * 4);
+    off += align256((2 * (size_t)B * cells + 1) * 4);
+    L.perm_p = off;  // perm_q follows perm_p without a gap (one scatter fills both)
+    L.perm_q = off + (size_t)B * P * 4;
+    off += align256((size_t)B * P * 4 + (size_t)B * Q * 4);
     L.tinfo = off;
     off += align256((size_t)B * (L.P_pad / kTilePoints) * 8 * 4);
   }
@@ -1134,16 +1136,17 @@ FwdLayout fwd_layout(int B, int Q, int P, int K, int dtype, bool own_rec) {
 }
 
 int launch_pack_points(const void* p, const void* sigma, const void* R, int B, int P, int dtype, void* rec,
-                       cudaStream_t st) {
+                       cudaStream_t st, int* zero_words, int n_zero) {
   int dev = 0;
   cudaGetDevice(&dev);
   const int64_t n = (int64_t)B * P;
   if (dtype == KNNAG_F64)
     pack_points_kernel<double><<<grid_for(n, 256, dev), 256, 0, st>>>(
-        (const double*)p, (const double*)sigma, (const double*)R, n, (double*)rec);
+        (const double*)p, (const double*)sigma, (const double*)R, n, (double*)rec, zero_words, n_zero);
   else
     pack_points_kernel<float><<<grid_for(n, 256, dev), 256, 0, st>>>((const float*)p, (const float*)sigma,
-                                                                     (const float*)R, n, (float*)rec);
+                                                                     (const float*)R, n, (float*)rec, zero_words,
+                                                                     n_zero);
   note_launches(1);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
@@ -1165,8 +1168,7 @@ int forward_impl(const void* q, const void* p, const void* f, const void* sigma,
   int* flag_count = status + 1;
   int* flag_list = reinterpret_cast<int*>(ws + L.flag_list);
   void* rec = own_rec ? (void*)(ws + L.rec) : points;
-  if (cudaMemsetAsync(status, 0, 2 * sizeof(int), st) != cudaSuccess) return KNNAG_ERR_CUDA;
-  int rc = launch_pack_points(p, sigma, R, B, P, dtype, rec, st);
+  int rc = launch_pack_points(p, sigma, R, B, P, dtype, rec, st, status, 2);  // also zeroes status, flag_count
   if (rc) return rc;
   if (dtype == KNNAG_F64)
     return forward_exact_all<double>((const double*)q, (const double*)rec, (const double*)f, B, Q, P, F, K,

@@ -152,32 +152,43 @@ __global__ void __launch_bounds__(512) point_bounds_kernel(const float* __restri
   }
 }
 
-// Cell histogram of the elements of group blockIdx.y (points from records,
-// queries from q).
-__global__ void cell_count_kernel(const float* __restrict__ xyz, int stride, int negate, GroupMap m,
-                                  const float* __restrict__ bnd, int* __restrict__ count) {
+// A counting-sort job: the elements of the groups of `m` (points from
+// records, or queries from q) and where their cells start in the shared
+// count / offset arrays.  One launch can run two jobs (blockIdx.z), e.g. the
+// points and the queries of a batch, whose cells are then scanned together.
+struct CellJob {
+  const float* xyz;
+  int stride, negate;
+  GroupMap m;
+  int cell_base;
+};
+
+// Cell histogram of the elements of group blockIdx.y of job blockIdx.z.
+__global__ void cell_count_kernel(CellJob j0, CellJob j1, const float* __restrict__ bnd, int* __restrict__ count) {
+  const CellJob& j = blockIdx.z ? j1 : j0;
   GroupRange r;
-  if (!group_range(m, blockIdx.y, r)) return;
-  const float s = negate ? -1.f : 1.f;
-  const float* gb = group_bounds(m, bnd) + r.bnd * 8;
+  if (!group_range(j.m, blockIdx.y, r)) return;
+  const float s = j.negate ? -1.f : 1.f;
+  const float* gb = group_bounds(j.m, bnd) + r.bnd * 8;
+  int* cnt = count + j.cell_base + r.cell_off;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n; i += gridDim.x * blockDim.x) {
-    const float* v = xyz + (r.start + i) * stride;
-    const uint32_t c = cell_of(s * v[0], s * v[1], s * v[2], gb, r.bits);
-    atomicAdd(&count[r.cell_off + (int)c], 1);
+    const float* v = j.xyz + (r.start + i) * j.stride;
+    atomicAdd(&cnt[cell_of(s * v[0], s * v[1], s * v[2], gb, r.bits)], 1);
   }
 }
 
 // perm[offset[cell] + rank] = index within the group.
-__global__ void cell_scatter_kernel(const float* __restrict__ xyz, int stride, int negate, GroupMap m,
-                                    const float* __restrict__ bnd, const int* __restrict__ offset,
-                                    int* __restrict__ cursor, int* __restrict__ perm) {
+__global__ void cell_scatter_kernel(CellJob j0, CellJob j1, const float* __restrict__ bnd,
+                                    const int* __restrict__ offset, int* __restrict__ cursor, int* __restrict__ perm) {
+  const CellJob& j = blockIdx.z ? j1 : j0;
   GroupRange r;
-  if (!group_range(m, blockIdx.y, r)) return;
-  const float s = negate ? -1.f : 1.f;
-  const float* gb = group_bounds(m, bnd) + r.bnd * 8;
+  if (!group_range(j.m, blockIdx.y, r)) return;
+  const float s = j.negate ? -1.f : 1.f;
+  const float* gb = group_bounds(j.m, bnd) + r.bnd * 8;
+  const int base = j.cell_base + r.cell_off;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n; i += gridDim.x * blockDim.x) {
-    const float* v = xyz + (r.start + i) * stride;
-    const int c = r.cell_off + (int)cell_of(s * v[0], s * v[1], s * v[2], gb, r.bits);
+    const float* v = j.xyz + (r.start + i) * j.stride;
+    const int c = base + (int)cell_of(s * v[0], s * v[1], s * v[2], gb, r.bits);
     perm[offset[c] + atomicAdd(&cursor[c], 1)] = i;
   }
 }
@@ -191,32 +202,6 @@ struct TileGroup {
 __device__ __forceinline__ TileGroup tile_group(const CloudDesc* cd, int b, int P, int ntile) {
   if (cd) return TileGroup{cd[b].p_off, cd[b].tile_off, cd[b].P, cd[b].ntile};
   return TileGroup{(int64_t)b * P, (int64_t)b * ntile, P, ntile};
-}
-
-// Pair-interleaved tiles of group blockIdx.y in sorted order; field kRecPad
-// carries the original point index (int bits), -1 for padding (whose sigma
-// is NaN).
-__global__ void pack_pairs_sorted_kernel(const float* __restrict__ rec, const int* __restrict__ perm,
-                                         const CloudDesc* __restrict__ cd, int P, int ntile,
-                                         float* __restrict__ pairs) {
-  const TileGroup g = tile_group(cd, blockIdx.y, P, ntile);
-  const int64_t total = (int64_t)g.ntile * kTilePoints * kRecLen;
-  float* out = pairs + g.t0 * kTilePoints * kRecLen;
-  for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < total; o += (int64_t)gridDim.x * blockDim.x) {
-    const int half = (int)(o & 1);
-    const int field = (int)((o >> 1) & (kRecLen - 1));
-    const int64_t pos = 2 * (o >> 5) + half;
-    float v;
-    if (pos < g.P) {
-      const int i = perm[g.p0 + pos];
-      v = field == kRecPad ? __int_as_float(i) : rec[(g.p0 + i) * kRecLen + field];
-    } else if (field == kRecPad) {
-      v = __int_as_float(-1);
-    } else {
-      v = (field == kS0 || field == kS1 || field == kS2) ? __int_as_float(0x7fc00000) : 0.0f;
-    }
-    out[o] = v;
-  }
 }
 
 // Smallest eigenvalue of a symmetric 3x3 matrix (closed form), double.
@@ -235,73 +220,109 @@ __device__ double sym3_min_eig(double a00, double a11, double a22, double a01, d
   return qm + 2.0 * p * cos(phi + 2.0943951023931957);  // + 2 pi / 3
 }
 
-// tinfo[(tile of group blockIdx.y)*8] = {min xyz, max xyz, mu, 0}; one warp
-// per tile.
-__global__ void tile_info_kernel(const float* __restrict__ rec, const int* __restrict__ perm,
-                                 const CloudDesc* __restrict__ cd, int P, int ntile, float* __restrict__ tinfo) {
+// One CTA of 128 threads per search tile (tile blockIdx.x of group
+// blockIdx.y), one sorted point per thread: packs the tile in the
+// pair-interleaved layout (field kRecPad carries the original point index,
+// -1 for padding, whose sigma is NaN so its key is never a candidate) and
+// writes tinfo[tile*8] = {min xyz, max xyz, mu, 0}.
+__global__ void __launch_bounds__(kTilePoints) tile_info_kernel(const float* __restrict__ rec,
+                                                                const int* __restrict__ perm,
+                                                                const CloudDesc* __restrict__ cd, int P, int ntile,
+                                                                float* __restrict__ pairs,
+                                                                float* __restrict__ tinfo) {
   const TileGroup g = tile_group(cd, blockIdx.y, P, ntile);
-  const int lane = threadIdx.x & 31;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
-  for (int t = gw; t < g.ntile; t += nw) {
-    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-    float mu = INFINITY;
-    bool bad = false;
-    for (int k = lane; k < kTilePoints; k += 32) {
-      const int pos = t * kTilePoints + k;
-      if (pos >= g.P) continue;
-      const float* r = rec + (g.p0 + perm[g.p0 + pos]) * kRecLen;
-      float v[kRecLen];
+  const int t = blockIdx.x;
+  if (t >= g.ntile) return;
+  __shared__ float red[kTilePoints / 32][8];
+  __shared__ __align__(16) float tile[kTilePoints * kRecLen];
+  const int k = threadIdx.x, lane = k & 31, warp = k >> 5;
+  float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  float mu = INFINITY;
+  bool bad = false;
+  const int pos = t * kTilePoints + k;
+  float* slot = tile + (k >> 1) * kPairFloats + (k & 1);  // field f at slot[2 f]
+  if (pos >= g.P) {
 #pragma unroll
-      for (int m = 0; m < kRecLen; ++m) v[m] = r[m];
+    for (int m = 0; m < kRecLen; ++m)
+      slot[2 * m] = m == kRecPad ? __int_as_float(-1)
+                                 : ((m == kS0 || m == kS1 || m == kS2) ? __int_as_float(0x7fc00000) : 0.0f);
+  } else {
+    const int idx = perm[g.p0 + pos];
+    const float* r = rec + (g.p0 + idx) * kRecLen;
+    float v[kRecLen];
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const float c = -v[kNPX + a];
-        mn[a] = fminf(mn[a], c);
-        mx[a] = fmaxf(mx[a], c);
-        if (!isfinite(c)) bad = true;
-      }
-      double M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-      double err = 0.0;
+    for (int m = 0; m < kRecLen; ++m) v[m] = r[m];
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const double s = v[kS0 + a];
-        if (!(s >= 0.0)) bad = true;  // a negative (or NaN) precision: keys may be negative
-        double rn = 0.0;
+    for (int m = 0; m < kRecLen; ++m) slot[2 * m] = m == kRecPad ? __int_as_float(idx) : v[m];
 #pragma unroll
-        for (int m = 0; m < 3; ++m) {
-          const double ra = v[kR00 + 3 * a + m];
-          rn += ra * ra;
-#pragma unroll
-          for (int n2 = 0; n2 < 3; ++n2) M[m][n2] += s * ra * (double)v[kR00 + 3 * a + n2];
-        }
-        err += fabs(s) * rn;
-      }
-      const double lam = sym3_min_eig(M[0][0], M[1][1], M[2][2], M[0][1], M[0][2], M[1][2]);
-      const double scale = fabs(M[0][0]) + fabs(M[1][1]) + fabs(M[2][2]) + fabs(M[0][1]) + fabs(M[0][2]) + fabs(M[1][2]);
-      const double m = lam - 1e-9 * scale - 1e-5 * err;
-      if (!isfinite(m)) bad = true;
-      mu = fminf(mu, (m > 0.0 && isfinite(m)) ? (float)(m * (1.0 - 1e-6)) : 0.0f);
+    for (int a = 0; a < 3; ++a) {
+      const float c = -v[kNPX + a];
+      mn[a] = fminf(mn[a], c);
+      mx[a] = fmaxf(mx[a], c);
+      if (!isfinite(c)) bad = true;
     }
+    double M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    double err = 0.0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
+    for (int a = 0; a < 3; ++a) {
+      const double s = v[kS0 + a];
+      if (!(s >= 0.0)) bad = true;  // a negative (or NaN) precision: keys may be negative
+      double rn = 0.0;
 #pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        mn[a] = fminf(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], o));
-        mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
+      for (int m = 0; m < 3; ++m) {
+        const double ra = v[kR00 + 3 * a + m];
+        rn += ra * ra;
+#pragma unroll
+        for (int n2 = 0; n2 < 3; ++n2) M[m][n2] += s * ra * (double)v[kR00 + 3 * a + n2];
       }
-      mu = fminf(mu, __shfl_xor_sync(0xffffffffu, mu, o));
+      err += fabs(s) * rn;
     }
-    bad = __any_sync(0xffffffffu, bad);
-    if (lane == 0) {
-      float* o = tinfo + (g.t0 + t) * 8;
+    const double lam = sym3_min_eig(M[0][0], M[1][1], M[2][2], M[0][1], M[0][2], M[1][2]);
+    const double scale = fabs(M[0][0]) + fabs(M[1][1]) + fabs(M[2][2]) + fabs(M[0][1]) + fabs(M[0][2]) + fabs(M[1][2]);
+    const double m = lam - 1e-9 * scale - 1e-5 * err;
+    if (!isfinite(m)) bad = true;
+    mu = fminf(mu, (m > 0.0 && isfinite(m)) ? (float)(m * (1.0 - 1e-6)) : 0.0f);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      mn[a] = fminf(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], o));
+      mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
+    }
+    mu = fminf(mu, __shfl_xor_sync(0xffffffffu, mu, o));
+  }
+  bad = __any_sync(0xffffffffu, bad);
+  if (lane == 0) {
+    for (int a = 0; a < 3; ++a) {
+      red[warp][a] = mn[a];
+      red[warp][3 + a] = mx[a];
+    }
+    red[warp][6] = mu;
+    red[warp][7] = bad ? 1.0f : 0.0f;
+  }
+  __syncthreads();
+  {
+    const float4* src = reinterpret_cast<const float4*>(tile);
+    float4* dst = reinterpret_cast<float4*>(pairs + (g.t0 + t) * kTilePoints * kRecLen);
+    for (int i = k; i < kTilePoints * kRecLen / 4; i += kTilePoints) dst[i] = src[i];
+  }
+  if (k == 0) {
+    for (int w = 1; w < kTilePoints / 32; ++w) {
       for (int a = 0; a < 3; ++a) {
-        o[a] = mn[a];
-        o[3 + a] = mx[a];
+        mn[a] = fminf(mn[a], red[w][a]);
+        mx[a] = fmaxf(mx[a], red[w][3 + a]);
       }
-      o[6] = bad ? -1.0f : (mu < INFINITY ? mu : 0.0f);  // -1: the tile has no key bound
-      o[7] = 0.0f;
+      mu = fminf(mu, red[w][6]);
+      bad = bad || red[w][7] != 0.0f;
     }
+    float* o = tinfo + (g.t0 + t) * 8;
+    for (int a = 0; a < 3; ++a) {
+      o[a] = mn[a];
+      o[3 + a] = mx[a];
+    }
+    o[6] = bad ? -1.0f : (mu < INFINITY ? mu : 0.0f);  // -1: the tile has no key bound
+    o[7] = 0.0f;
   }
 }
 
@@ -327,30 +348,27 @@ int launch_spatial_index(const float* q, const float* rec, int B, int Q, int P, 
   float* bnd = reinterpret_cast<float*>(ws + L.bounds);
   int* cnt = reinterpret_cast<int*>(ws + L.cell_count);
   int* off = reinterpret_cast<int*>(ws + L.cell_offset);
-  int* perm_p = reinterpret_cast<int*>(ws + L.perm_p);
-  int* perm_q = reinterpret_cast<int*>(ws + L.perm_q);
+  int* perm = reinterpret_cast<int*>(ws + L.perm_p);  // perm_q follows perm_p directly
   float* pairs = reinterpret_cast<float*>(ws + L.pairs);
   float* tinfo = reinterpret_cast<float*>(ws + L.tinfo);
   const int ntile = P_pad / kTilePoints;
   GroupMap pm{P, bits, nullptr, nullptr, nullptr, nullptr, nullptr};
   GroupMap qm{Q, bits, nullptr, nullptr, nullptr, nullptr, nullptr};
   point_bounds_kernel<<<B, 512, 0, st>>>(rec, pm, bnd);
-  // points
-  if (cudaMemsetAsync(cnt, 0, (size_t)B * cells * 4, st) != cudaSuccess) return KNNAG_ERR_CUDA;
-  cell_count_kernel<<<dim3(grid_x(P, sms, B), B), 256, 0, st>>>(rec + kNPX, kRecLen, 1, pm, bnd, cnt);
-  int rc = launch_exclusive_scan(cnt, B * cells, off, st);
+  // points and queries in one counting sort: their cells are scanned
+  // together, so the queries' positions start after all points' and land in
+  // perm_q, which follows perm_p
+  const int64_t nc = 2 * (int64_t)B * cells;
+  if (cudaMemsetAsync(cnt, 0, (size_t)nc * 4, st) != cudaSuccess) return KNNAG_ERR_CUDA;
+  const CellJob jp{rec + kNPX, kRecLen, 1, pm, 0};
+  const CellJob jq{q, 3, 0, qm, B * cells};
+  const dim3 grid(grid_x(P > Q ? P : Q, sms, B), B, 2);
+  cell_count_kernel<<<grid, 256, 0, st>>>(jp, jq, bnd, cnt);
+  int rc = launch_exclusive_scan(cnt, (int)nc, off, st);
   if (rc) return rc;
-  cell_scatter_kernel<<<dim3(grid_x(P, sms, B), B), 256, 0, st>>>(rec + kNPX, kRecLen, 1, pm, bnd, off, cnt, perm_p);
-  // queries (the scatter left the point counts in cnt)
-  if (cudaMemsetAsync(cnt, 0, (size_t)B * cells * 4, st) != cudaSuccess) return KNNAG_ERR_CUDA;
-  cell_count_kernel<<<dim3(grid_x(Q, sms, B), B), 256, 0, st>>>(q, 3, 0, qm, bnd, cnt);
-  rc = launch_exclusive_scan(cnt, B * cells, off, st);
-  if (rc) return rc;
-  cell_scatter_kernel<<<dim3(grid_x(Q, sms, B), B), 256, 0, st>>>(q, 3, 0, qm, bnd, off, cnt, perm_q);
-  pack_pairs_sorted_kernel<<<dim3(grid_x((int64_t)P_pad * kRecLen, sms, B), B), 256, 0, st>>>(rec, perm_p, nullptr, P,
-                                                                                               ntile, pairs);
-  tile_info_kernel<<<dim3(grid_x((int64_t)ntile * 32, sms, B), B), 256, 0, st>>>(rec, perm_p, nullptr, P, ntile, tinfo);
-  note_launches(7);  // + 2 scans, counted by launch_exclusive_scan
+  cell_scatter_kernel<<<grid, 256, 0, st>>>(jp, jq, bnd, off, cnt, perm);
+  tile_info_kernel<<<dim3(ntile, B), kTilePoints, 0, st>>>(rec, perm, nullptr, P, ntile, pairs, tinfo);
+  note_launches(4);  // + 1 scan, counted by launch_exclusive_scan
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 
@@ -370,15 +388,14 @@ int launch_cloudset_index(char* cs, const CloudSetHeader& h, const CloudDesc* cd
   GroupMap pm{0, 0, cd_dev, nullptr, nullptr, nullptr, nullptr};
   point_bounds_kernel<<<C, 512, 0, st>>>(rec, pm, bnd);
   if (cudaMemsetAsync(cnt, 0, (size_t)h.total_cells * 4, st) != cudaSuccess) return KNNAG_ERR_CUDA;
-  cell_count_kernel<<<dim3(grid_x(max_p, sms, C), C), 256, 0, st>>>(rec + kNPX, kRecLen, 1, pm, bnd, cnt);
+  const CellJob jp{rec + kNPX, kRecLen, 1, pm, 0};
+  const dim3 grid(grid_x(max_p, sms, C), C, 1);
+  cell_count_kernel<<<grid, 256, 0, st>>>(jp, jp, bnd, cnt);
   int rc = launch_exclusive_scan(cnt, h.total_cells, off, st);
   if (rc) return rc;
-  cell_scatter_kernel<<<dim3(grid_x(max_p, sms, C), C), 256, 0, st>>>(rec + kNPX, kRecLen, 1, pm, bnd, off, cnt,
-                                                                       perm_p);
-  pack_pairs_sorted_kernel<<<dim3(grid_x((int64_t)max_ntile * kTilePoints * kRecLen, sms, C), C), 256, 0, st>>>(
-      rec, perm_p, cd_dev, 0, 0, pairs);
-  tile_info_kernel<<<dim3(grid_x((int64_t)max_ntile * 32, sms, C), C), 256, 0, st>>>(rec, perm_p, cd_dev, 0, 0, tinfo);
-  note_launches(5);  // + 1 scan
+  cell_scatter_kernel<<<grid, 256, 0, st>>>(jp, jp, bnd, off, cnt, perm_p);
+  tile_info_kernel<<<dim3(max_ntile, C), kTilePoints, 0, st>>>(rec, perm_p, cd_dev, 0, 0, pairs, tinfo);
+  note_launches(4);  // + 1 scan
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 
@@ -395,11 +412,12 @@ int launch_query_order(const float* q, const char* cs, const void* segs_dev, int
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   GroupMap qm{0, 0, nullptr, seg_descs(segs_dev), static_cast<const SegHeader*>(segs_dev), cs, status};
   if (cudaMemsetAsync(cnt, 0, (size_t)cap_cells * 4, st) != cudaSuccess) return KNNAG_ERR_CUDA;
-  const dim3 grid(grid_x(cap_q, sms, cap_segs), cap_segs);
-  cell_count_kernel<<<grid, 256, 0, st>>>(q, 3, 0, qm, nullptr, cnt);
+  const dim3 grid(grid_x(cap_q, sms, cap_segs), cap_segs, 1);
+  const CellJob jq{q, 3, 0, qm, 0};
+  cell_count_kernel<<<grid, 256, 0, st>>>(jq, jq, nullptr, cnt);
   int rc = launch_exclusive_scan(cnt, cap_cells, off, st);
   if (rc) return rc;
-  cell_scatter_kernel<<<grid, 256, 0, st>>>(q, 3, 0, qm, nullptr, off, cnt, perm_q);
+  cell_scatter_kernel<<<grid, 256, 0, st>>>(jq, jq, nullptr, off, cnt, perm_q);
   note_launches(2);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
