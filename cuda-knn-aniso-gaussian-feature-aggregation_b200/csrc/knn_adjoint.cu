@@ -355,6 +355,9 @@ struct QueryParams {
   const char* cs;
   const void* segs;
   const int* status;
+  // broadcast grad_f_out: gfo points to one value s, and c = s * frowsum[i]
+  // (frowsum = per-point sum over the columns of f)
+  const T* frowsum;
 };
 
 template <typename T>
@@ -373,6 +376,7 @@ struct PointParams {
   T* df;
   T* dsigma;
   T* dR;
+  bool gfo_scalar;  // gfo points to one value broadcast over [B,Q,F]
 };
 
 // v = R^T diag(sigma) u
@@ -387,6 +391,22 @@ __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
+}
+
+// Per-point sum over the columns of f (one warp per row, fixed reduction
+// order): with a broadcast grad_f_out s, c = gfo[q] . f[i] = s * rowsum[i].
+template <typename T>
+__global__ void __launch_bounds__(256) row_sum_kernel(const T* __restrict__ f, int64_t rows, int F,
+                                                      T* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (gridDim.x * (int64_t)blockDim.x) >> 5;
+  for (int64_t r = gw; r < rows; r += nw) {
+    T acc = T(0);
+    for (int c = lane; c < F; c += 32) acc += f[r * F + c];
+    acc = warp_sum(acc);
+    if (lane == 0) out[r] = acc;
+  }
 }
 
 // First-order query side: one warp per query.  For each group of 8
@@ -407,7 +427,7 @@ __global__ void __launch_bounds__(256, 3) query_order1_kernel(QueryParams<T> a) 
   for (int64_t bq = gw; bq < BQ; bq += nw) {
     // the query's cloud: records, features, sizes and first entry
     int K, P;
-    int64_t e0;
+    int64_t e0, pbase;
     const T* recb;
     const T* fb;
     if (sh) {
@@ -417,6 +437,7 @@ __global__ void __launch_bounds__(256, 3) query_order1_kernel(QueryParams<T> a) 
       K = g.K;
       P = c.P;
       e0 = g.e_off + (bq - g.q_off) * K;
+      pbase = c.p_off;
       recb = reinterpret_cast<const T*>(a.cs + reinterpret_cast<const CloudSetHeader*>(a.cs)->rec_off) +
              c.p_off * kRecLen;
       fb = a.f + c.p_off * F;
@@ -425,6 +446,7 @@ __global__ void __launch_bounds__(256, 3) query_order1_kernel(QueryParams<T> a) 
       K = a.K;
       P = a.P;
       e0 = bq * K;
+      pbase = b * a.P;
       recb = a.rec + b * a.P * kRecLen;
       fb = a.f + b * a.P * F;
     }
@@ -433,6 +455,13 @@ __global__ void __launch_bounds__(256, 3) query_order1_kernel(QueryParams<T> a) 
     T acc[3] = {T(0), T(0), T(0)};
     for (int k0 = 0; k0 < K; k0 += NG) {
       const int nk = min(NG, K - k0);
+      const int m_own = lane >> 2;
+      T c_own;
+      if (a.frowsum) {
+        // broadcast grad_f_out s: c_k = s * rowsum(f)[idx_k], no F-wide dot product
+        const int64_t idx = m_own < nk ? a.idxs[e0 + k0 + m_own] : -1;
+        c_own = (idx >= 0 && idx < P) ? a.gfo[0] * a.frowsum[pbase + idx] : T(0);
+      } else {
       int ik[NG];  // neighbour point index within the batch, -1 if none
 #pragma unroll
       for (int kk = 0; kk < NG; ++kk) {
@@ -459,9 +488,9 @@ __global__ void __launch_bounds__(256, 3) query_order1_kernel(QueryParams<T> a) 
           part[i] = keep + __shfl_xor_sync(0xffffffffu, send, m);
         }
       }
-      T c_own = part[0] + __shfl_xor_sync(0xffffffffu, part[0], 2);
+      c_own = part[0] + __shfl_xor_sync(0xffffffffu, part[0], 2);
       c_own += __shfl_xor_sync(0xffffffffu, c_own, 1);
-      const int m_own = lane >> 2;
+      }
       const int64_t e = e0 + k0 + m_own;
       if ((lane & 3) == 0 && m_own < nk) {
         if (a.coef_out) a.coef_out[e] = c_own;
@@ -601,7 +630,10 @@ __global__ void __launch_bounds__(256, 4) point_side_kernel(PointParams<T> a) {
     T gp[3] = {T(0), T(0), T(0)}, gs[3] = {T(0), T(0), T(0)}, gR[9];
 #pragma unroll
     for (int m = 0; m < 9; ++m) gR[m] = T(0);
-    for (int c0 = 0; c0 == 0 || (want_df && c0 < F); c0 += 32 * NCOL) {
+    // broadcast grad_f_out s: df[i][c] = s * sum_e wgt_e for every column
+    // (one pass, no gathers of grad_f_out rows); wsum is this lane's share
+    T wsum = T(0);
+    for (int c0 = 0; c0 == 0 || (want_df && !a.gfo_scalar && c0 < F); c0 += 32 * NCOL) {
       T acc[NCOL];
 #pragma unroll
       for (int u = 0; u < NCOL; ++u) acc[u] = T(0);
@@ -659,7 +691,9 @@ __global__ void __launch_bounds__(256, 4) point_side_kernel(PointParams<T> a) {
             }
           }
         }
-        if (want_df) {
+        if (want_df && a.gfo_scalar) {
+          wsum += wgt;  // 0 for lanes without an entry
+        } else if (want_df) {
           const int nvalid = min(32, end - base);
           for (int j0 = 0; j0 < nvalid; j0 += 4) {
             T val[4][NCOL], wj[4];
@@ -683,7 +717,10 @@ __global__ void __launch_bounds__(256, 4) point_side_kernel(PointParams<T> a) {
           }
         }
       }
-      if (want_df) {
+      if (want_df && a.gfo_scalar) {
+        const T val = a.gfo[0] * warp_sum(wsum);
+        for (int cc = lane; cc < F; cc += 32) a.df[(int64_t)row * F + cc] = val;
+      } else if (want_df) {
 #pragma unroll
         for (int u = 0; u < NCOL; ++u) {
           const int cc = c0 + lane + 32 * u;
@@ -728,6 +765,8 @@ BwdLayout bwd_layout(int B, int Q, int P, int F, int K, int dtype) {
   off += adj_layout(B, Q, P, K).total;
   L.coef = off;
   off += align256((size_t)B * Q * K * esz);
+  L.rowsum = off;
+  off += align256((size_t)B * P * esz);
   L.total = off;
   return L;
 }
@@ -806,6 +845,19 @@ int backward_t(const BwdArgs& x, cudaStream_t st) {
   T* coef_ws = reinterpret_cast<T*>(ws + L.coef);
   T* coef_out = static_cast<T*>(x.coef_out);
 
+  const bool gfo_scalar = (x.needs & KNNAG_GFO_SCALAR) != 0;
+  T* rowsum = reinterpret_cast<T*>(ws + L.rowsum);
+  bool rowsum_ready = false;
+  // per-point column sums of f, for the query side with a broadcast grad_f_out
+  auto ensure_rowsum = [&]() -> int {
+    if (rowsum_ready) return KNNAG_OK;
+    row_sum_kernel<T><<<blocks_for((int64_t)x.B * x.P * 32, 256), 256, 0, st>>>((const T*)x.f, (int64_t)x.B * x.P,
+                                                                                  x.F, rowsum);
+    note_launches(1);
+    rowsum_ready = true;
+    return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
+  };
+
   QueryParams<T> qp{};
   qp.gfo = (const T*)x.gfo;
   qp.ggq = (const T*)x.ggq;
@@ -825,6 +877,10 @@ int backward_t(const BwdArgs& x, cudaStream_t st) {
     if ((x.needs & KNNAG_NEED_DQ) || cdst) {
       qp.dq = (x.needs & KNNAG_NEED_DQ) ? (T*)x.dq : nullptr;
       qp.coef_out = cdst;
+      if (gfo_scalar) {
+        if ((rc = ensure_rowsum())) return rc;
+        qp.frowsum = rowsum;
+      }
       rc = launch_query<T>(qp, 1, st);
       if (rc) return rc;
     }
@@ -834,6 +890,10 @@ int backward_t(const BwdArgs& x, cudaStream_t st) {
       QueryParams<T> cp = qp;
       cp.dq = nullptr;
       cp.coef_out = coef_ws;
+      if (gfo_scalar) {
+        if ((rc = ensure_rowsum())) return rc;
+        cp.frowsum = rowsum;
+      }
       rc = launch_query<T>(cp, 1, st);
       if (rc) return rc;
       coef = coef_ws;
@@ -874,6 +934,7 @@ int backward_t(const BwdArgs& x, cudaStream_t st) {
     pp.df = (T*)x.df;
     pp.dsigma = (T*)x.dsigma;
     pp.dR = (T*)x.dR;
+    pp.gfo_scalar = gfo_scalar;
     rc = (x.order == 1) ? launch_point_o<T, 1>(pp, st) : launch_point_o<T, 2>(pp, st);
   }
   return rc;

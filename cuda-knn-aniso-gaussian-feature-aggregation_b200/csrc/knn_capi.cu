@@ -154,7 +154,7 @@ static int backward_common(BwdArgs& x, size_t workspace_bytes, void* stream) {
   if (x.dtype != KNNAG_F32 && x.dtype != KNNAG_F64) return KNNAG_ERR_DTYPE;
   int rc = check_sizes(x.B, x.Q, x.P, x.F, x.K);
   if (rc) return rc;
-  if (x.needs & ~KNNAG_NEED_ALL) return KNNAG_ERR_ARG;
+  if (x.needs & ~(KNNAG_NEED_ALL | KNNAG_GFO_SCALAR)) return KNNAG_ERR_ARG;
   if ((int64_t)x.B * x.Q == 0 && (int64_t)x.B * x.P == 0) return KNNAG_OK;
   if (!x.gfo || !x.q || !x.p || !x.sigma || !x.R || !x.idxs || !x.workspace) return KNNAG_ERR_ARG;
   if (x.F > 0 && !x.f) return KNNAG_ERR_ARG;

@@ -163,7 +163,7 @@ inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 
 // Backward workspace: status | records | adjacency | per-entry coefficients.
 struct BwdLayout {
-  size_t status, rec, adj, coef, total;
+  size_t status, rec, adj, coef, rowsum, total;  // rowsum: sum over columns of f per point (scalar grad_f_out)
 };
 BwdLayout bwd_layout(int B, int Q, int P, int F, int K, int dtype);
 

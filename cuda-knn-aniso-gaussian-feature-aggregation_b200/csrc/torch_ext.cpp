@@ -125,7 +125,13 @@ std::vector<torch::Tensor> backward_impl(int order, const c10::optional<torch::T
   const Dims d = check_inputs(q, p, f, sigma, R);
   check_idxs(idxs, d);
   const int K = (int)idxs.size(2);
-  check_like(gfo, "grad_f_out", {d.B, d.Q, d.F}, q);
+  if (needs & KNNAG_GFO_SCALAR) {
+    // one value broadcast over [B, Q, F]: the kernels read gfo.data_ptr()[0]
+    TORCH_CHECK(gfo.is_cuda() && gfo.numel() > 0 && gfo.scalar_type() == q.scalar_type(),
+                "broadcast grad_f_out must be a CUDA tensor of q's dtype");
+  } else {
+    check_like(gfo, "grad_f_out", {d.B, d.Q, d.F}, q);
+  }
   if (order == 2) check_like(*ggq, "grad_grad_q", {d.B, d.Q, 3}, q);
   if (w_out && w_out->defined()) check_like(*w_out, "w_out", {d.B, d.Q, K}, q);
   if (points && points->defined()) check_like(*points, "points", {d.B, d.P, 16}, q);
@@ -345,6 +351,16 @@ torch::Tensor or_placeholder(const torch::Tensor& t, const torch::Tensor& like) 
   return t.defined() ? t : torch::empty({0}, like.options());
 }
 
+// A gradient that is one value broadcast over its shape (every dimension of
+// size > 1 has stride 0) -- what autograd passes for f_out.sum().  It is
+// handed to the kernels as that one value instead of being materialised.
+bool is_broadcast_scalar(const torch::Tensor& g) {
+  if (!g.defined() || g.numel() == 0) return false;
+  for (int64_t i = 0; i < g.dim(); ++i)
+    if (g.size(i) > 1 && g.stride(i) != 0) return false;
+  return true;
+}
+
 struct AggBackwardFn : public torch::autograd::Function<AggBackwardFn> {
   // differentiable inputs: gfo, q, p, f, sigma, R; then idxs, points (no grad)
   static variable_list forward(AutogradContext* ctx, torch::Tensor gfo, torch::Tensor q, torch::Tensor p,
@@ -357,6 +373,7 @@ struct AggBackwardFn : public torch::autograd::Function<AggBackwardFn> {
                            true);
     ctx->save_for_backward({gfo, q, p, f, sigma, R, idxs, points});
     ctx->saved_data["coef"] = o[5];
+    ctx->saved_data["gfo_scalar"] = (needs & KNNAG_GFO_SCALAR) != 0;
     if (adj.defined()) ctx->saved_data["adj"] = adj;
     ctx->set_materialize_grads(false);
     return {or_placeholder(o[0], q), or_placeholder(o[1], q), or_placeholder(o[2], q), or_placeholder(o[3], q),
@@ -371,6 +388,7 @@ struct AggBackwardFn : public torch::autograd::Function<AggBackwardFn> {
     for (int i = 0; i < 5; ++i)
       if (ctx->needs_input_grad(1 + i)) needs |= kNeedBits[i];
     if (!needs) return out;
+    if (ctx->saved_data["gfo_scalar"].toBool()) needs |= KNNAG_GFO_SCALAR;
     auto s = ctx->get_saved_variables();
     torch::Tensor adj;
     if (ctx->saved_data.count("adj")) adj = ctx->saved_data["adj"].toTensor();
@@ -401,8 +419,9 @@ struct AggFn : public torch::autograd::Function<AggFn> {
       if (ctx->needs_input_grad(i)) needs |= kNeedBits[i];
     if (!needs) return out;
     auto s = ctx->get_saved_variables();
-    auto r = AggBackwardFn::apply(g[0].contiguous(), s[0], s[1], s[2], s[3], s[4], s[5],
-                                  ctx->saved_data["points"].toTensor(), needs);
+    const bool scalar = is_broadcast_scalar(g[0]);
+    auto r = AggBackwardFn::apply(scalar ? g[0] : g[0].contiguous(), s[0], s[1], s[2], s[3], s[4], s[5],
+                                  ctx->saved_data["points"].toTensor(), needs | (scalar ? KNNAG_GFO_SCALAR : 0));
     for (int i = 0; i < 5; ++i) out[i] = (needs & kNeedBits[i]) ? r[i] : torch::Tensor();
     return out;
   }

@@ -61,7 +61,13 @@ enum {
   KNNAG_NEED_DSIGMA = 8,
   KNNAG_NEED_DR = 16,
   KNNAG_NEED_DGFO = 32,
-  KNNAG_NEED_ALL = 63
+  KNNAG_NEED_ALL = 63,
+  /* Not an output: grad_f_out points to ONE value broadcast over [B,Q,F]
+   * (the gradient of f_out.sum(), whose broadcast autograd does not
+   * materialise).  The kernels then use a row sum of f instead of F-wide
+   * dot products with grad_f_out rows, and write s * sum(w) to every
+   * column of df, instead of gathering grad_f_out rows. */
+  KNNAG_GFO_SCALAR = 64
 };
 
 /* Human-readable text of a status code (static storage). */

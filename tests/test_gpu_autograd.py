@@ -195,3 +195,28 @@ def test_backward_computes_only_requested_gradients():
     ((gq.norm(dim=-1) - 1.0) ** 2).mean().backward()
     for x in ins:
         assert x.grad is not None and torch.isfinite(x.grad).all()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("F", [1, 5, 64])
+def test_broadcast_grad_f_out_matches_dense(F):
+    """f_out.sum() hands the backward one value broadcast over [B,Q,F]; the
+    kernels then use per-point row sums of f instead of grad_f_out rows.
+    First- and second-order (Eikonal) gradients equal the ones computed
+    with the same gradient materialised as a dense tensor."""
+    import cuda_knn_aggregate as C
+    from cuda_knn_aggregate import workloads as W
+
+    _, t = W.make("small", F=F, seed=11)
+    res = []
+    for dense in (False, True):
+        ins = [x.cuda().requires_grad_(True) for x in t]
+        f_out = C.knn_aggregate_aniso(*ins, 12)[0]
+        if dense:
+            first = torch.autograd.grad(f_out, ins, torch.ones_like(f_out).contiguous(), create_graph=True)
+        else:
+            first = torch.autograd.grad(f_out.sum(), ins, create_graph=True)
+        ((first[0].norm(dim=-1) - 1.0) ** 2).mean().backward()
+        res.append([g.detach() for g in first] + [x.grad for x in ins])
+    for a, b in zip(*res):
+        assert rel_err(a.cpu().numpy(), b.cpu().numpy()) < 1e-5
