@@ -395,6 +395,8 @@ __device__ __forceinline__ T warp_sum(T v) {
 
 // Per-point sum over the columns of f (one warp per row, fixed reduction
 // order): with a broadcast grad_f_out s, c = gfo[q] . f[i] = s * rowsum[i].
+// knnag_feature_row_sums exposes the same kernel, so row sums a caller
+// keeps for resident features match the ones a backward call computes.
 template <typename T>
 __global__ void __launch_bounds__(256) row_sum_kernel(const T* __restrict__ f, int64_t rows, int F,
                                                       T* __restrict__ out) {
@@ -406,6 +408,74 @@ __global__ void __launch_bounds__(256) row_sum_kernel(const T* __restrict__ f, i
     for (int c = lane; c < F; c += 32) acc += f[r * F + c];
     acc = warp_sum(acc);
     if (lane == 0) out[r] = acc;
+  }
+}
+
+// First-order query side with a broadcast grad_f_out s: c_k = s *
+// rowsum(f)[idx_k] needs no F-wide dot product, so each lane takes one
+// neighbour, and a warp serves two queries when K <= 16 (uniform calls).
+template <typename T>
+__device__ __forceinline__ void query_order1_scalar(const QueryParams<T>& a, const SegHeader* sh, int64_t BQ) {
+  const int lane = threadIdx.x & 31;
+  const int lpq = (!sh && a.K <= 16) ? 16 : 32;  // lanes per query
+  const int qpw = 32 / lpq, sub = lane / lpq, kl = lane % lpq;
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (gridDim.x * (int64_t)blockDim.x) >> 5;
+  const T sg0 = a.gfo ? a.gfo[0] : T(1);  // ragged calls: no grad_f_out means all ones
+  for (int64_t base = gw * qpw; base < BQ; base += nw * qpw) {
+    const int64_t bq = base + sub;
+    T acc[3] = {T(0), T(0), T(0)};
+    if (bq < BQ) {
+      int K, P;
+      int64_t e0, pbase;
+      const T* recb;
+      if (sh) {
+        const SegDesc* sd = seg_descs(a.segs);
+        const SegDesc g = sd[seg_of_row(sd, sh->nseg, bq)];
+        const CloudDesc c = cloud_descs(a.cs)[g.cloud];
+        K = g.K;
+        P = c.P;
+        e0 = g.e_off + (bq - g.q_off) * K;
+        pbase = c.p_off;
+        recb = reinterpret_cast<const T*>(a.cs + reinterpret_cast<const CloudSetHeader*>(a.cs)->rec_off) +
+               c.p_off * kRecLen;
+      } else {
+        const int64_t b = bq / a.Q;
+        K = a.K;
+        P = a.P;
+        e0 = bq * K;
+        pbase = b * a.P;
+        recb = a.rec + b * a.P * kRecLen;
+      }
+      const T qx = a.q[bq * 3 + 0], qy = a.q[bq * 3 + 1], qz = a.q[bq * 3 + 2];
+      for (int k = kl; k < K; k += lpq) {
+        const int64_t e = e0 + k;
+        const int64_t idx = a.idxs[e];
+        T c = T(0);
+        if (idx >= 0 && idx < P) {
+          c = sg0 * a.frowsum[pbase + idx];
+          const T* rec = recb + idx * kRecLen;
+          Geo<T> geo;
+          geometry(qx, qy, qz, rec, geo);
+          const T w = a.w_in ? a.w_in[e] : geo.w;
+          const T sg[3] = {rec[kS0], rec[kS1], rec[kS2]};
+          T v[3];
+          rot_back(rec + kR00, sg, geo.u, v);
+          const T t = T(-2) * c * w;
+#pragma unroll
+          for (int mm = 0; mm < 3; ++mm) acc[mm] += t * v[mm];
+        }
+        if (a.coef_out) a.coef_out[e] = c;
+      }
+    }
+#pragma unroll
+    for (int mm = 0; mm < 3; ++mm)
+      for (int o = lpq >> 1; o >= 1; o >>= 1) acc[mm] += __shfl_xor_sync(0xffffffffu, acc[mm], o);
+    if (bq < BQ && kl == 0 && a.dq) {
+      a.dq[bq * 3 + 0] = acc[0];
+      a.dq[bq * 3 + 1] = acc[1];
+      a.dq[bq * 3 + 2] = acc[2];
+    }
   }
 }
 
@@ -422,12 +492,16 @@ __global__ void __launch_bounds__(256, 3) query_order1_kernel(QueryParams<T> a) 
   const SegHeader* sh = static_cast<const SegHeader*>(a.segs);
   if (sh && *a.status) return;
   const int64_t BQ = sh ? sh->grad_rows : (int64_t)a.B * a.Q;
+  if (a.frowsum) {
+    query_order1_scalar(a, sh, BQ);
+    return;
+  }
   const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = (gridDim.x * (int64_t)blockDim.x) >> 5;
   for (int64_t bq = gw; bq < BQ; bq += nw) {
     // the query's cloud: records, features, sizes and first entry
     int K, P;
-    int64_t e0, pbase;
+    int64_t e0;
     const T* recb;
     const T* fb;
     if (sh) {
@@ -437,7 +511,6 @@ __global__ void __launch_bounds__(256, 3) query_order1_kernel(QueryParams<T> a) 
       K = g.K;
       P = c.P;
       e0 = g.e_off + (bq - g.q_off) * K;
-      pbase = c.p_off;
       recb = reinterpret_cast<const T*>(a.cs + reinterpret_cast<const CloudSetHeader*>(a.cs)->rec_off) +
              c.p_off * kRecLen;
       fb = a.f + c.p_off * F;
@@ -446,7 +519,6 @@ __global__ void __launch_bounds__(256, 3) query_order1_kernel(QueryParams<T> a) 
       K = a.K;
       P = a.P;
       e0 = bq * K;
-      pbase = b * a.P;
       recb = a.rec + b * a.P * kRecLen;
       fb = a.f + b * a.P * F;
     }
@@ -455,13 +527,6 @@ __global__ void __launch_bounds__(256, 3) query_order1_kernel(QueryParams<T> a) 
     T acc[3] = {T(0), T(0), T(0)};
     for (int k0 = 0; k0 < K; k0 += NG) {
       const int nk = min(NG, K - k0);
-      const int m_own = lane >> 2;
-      T c_own;
-      if (a.frowsum) {
-        // broadcast grad_f_out s: c_k = s * rowsum(f)[idx_k], no F-wide dot product
-        const int64_t idx = m_own < nk ? a.idxs[e0 + k0 + m_own] : -1;
-        c_own = (idx >= 0 && idx < P) ? a.gfo[0] * a.frowsum[pbase + idx] : T(0);
-      } else {
       int ik[NG];  // neighbour point index within the batch, -1 if none
 #pragma unroll
       for (int kk = 0; kk < NG; ++kk) {
@@ -488,9 +553,9 @@ __global__ void __launch_bounds__(256, 3) query_order1_kernel(QueryParams<T> a) 
           part[i] = keep + __shfl_xor_sync(0xffffffffu, send, m);
         }
       }
-      c_own = part[0] + __shfl_xor_sync(0xffffffffu, part[0], 2);
+      T c_own = part[0] + __shfl_xor_sync(0xffffffffu, part[0], 2);
       c_own += __shfl_xor_sync(0xffffffffu, c_own, 1);
-      }
+      const int m_own = lane >> 2;
       const int64_t e = e0 + k0 + m_own;
       if ((lane & 3) == 0 && m_own < nk) {
         if (a.coef_out) a.coef_out[e] = c_own;
@@ -523,8 +588,64 @@ __global__ void __launch_bounds__(256, 3) query_order1_kernel(QueryParams<T> a) 
 // g = grad_grad_q[q], A = g . v, r_a = R_a . g, Mg = sum_a sigma_a r_a R_a:
 // dq += 2 c w (2 A v - Mg); optionally dgfo[q] = sum_k (-2 w_k A_k) f[idx_k]
 // accumulated in k order, lanes spanning columns, 8 rows in flight.
+// Second order without dgfo and with K <= 16 (the Eikonal step): half a
+// warp per query, one neighbour per lane, so a warp serves two queries.
+template <typename T>
+__device__ __forceinline__ void query_order2_half(const QueryParams<T>& a) {
+  const int lane = threadIdx.x & 31;
+  const int sub = lane >> 4, k = lane & 15;
+  const int64_t BQ = (int64_t)a.B * a.Q;
+  const int K = a.K, P = a.P;
+  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (gridDim.x * (int64_t)blockDim.x) >> 5;
+  for (int64_t base = gw * 2; base < BQ; base += nw * 2) {
+    const int64_t bq = base + sub;
+    T acc[3] = {T(0), T(0), T(0)};
+    if (bq < BQ && k < K && a.coef_in) {
+      const int64_t b = bq / a.Q;
+      const int64_t e = bq * K + k;
+      const int64_t idx = a.idxs[e];
+      if (idx >= 0 && idx < P) {
+        const T qx = a.q[bq * 3 + 0], qy = a.q[bq * 3 + 1], qz = a.q[bq * 3 + 2];
+        const T g[3] = {a.ggq[bq * 3 + 0], a.ggq[bq * 3 + 1], a.ggq[bq * 3 + 2]};
+        const T* rec = a.rec + (b * P + idx) * kRecLen;
+        Geo<T> geo;
+        geometry(qx, qy, qz, rec, geo);
+        const T w = a.w_in ? a.w_in[e] : geo.w;
+        const T* r = rec + kR00;
+        const T sg[3] = {rec[kS0], rec[kS1], rec[kS2]};
+        T v[3];
+        rot_back(r, sg, geo.u, v);
+        const T A = g[0] * v[0] + g[1] * v[1] + g[2] * v[2];
+        T rg[3];
+#pragma unroll
+        for (int s2 = 0; s2 < 3; ++s2) rg[s2] = r[3 * s2] * g[0] + r[3 * s2 + 1] * g[1] + r[3 * s2 + 2] * g[2];
+        const T cw2 = T(2) * a.coef_in[e] * w;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          const T mg = sg[0] * rg[0] * r[m] + sg[1] * rg[1] * r[3 + m] + sg[2] * rg[2] * r[6 + m];
+          acc[m] += cw2 * (T(2) * A * v[m] - mg);
+        }
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+      for (int o = 8; o >= 1; o >>= 1) acc[m] += __shfl_xor_sync(0xffffffffu, acc[m], o);
+    if (bq < BQ && k == 0 && a.dq) {
+      a.dq[bq * 3 + 0] = acc[0];
+      a.dq[bq * 3 + 1] = acc[1];
+      a.dq[bq * 3 + 2] = acc[2];
+    }
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) query_order2_kernel(QueryParams<T> a) {
+  if (!a.dgfo && a.K <= 16) {
+    query_order2_half(a);
+    return;
+  }
   const int lane = threadIdx.x & 31;
   const int BQ = a.B * a.Q, K = a.K, F = a.F, P = a.P;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -790,9 +911,11 @@ int launch_query(const QueryParams<T>& p, int order, cudaStream_t st) {
 // d(<gfo, f_out>)/dq of a ragged call (gfo null: all ones), weights
 // recomputed from idxs.  One warp per query row up to the table's total.
 int ragged_grad_q_impl(const char* cs, const void* segs, const float* q, const float* f, int F, const float* gfo,
-                       const int64_t* idxs, int64_t cap_q, float* dq, const int* status, cudaStream_t st) {
+                       const float* f_row_sums, const int64_t* idxs, int64_t cap_q, float* dq, const int* status,
+                       cudaStream_t st) {
   QueryParams<float> p{};
   p.status = status;
+  if (!gfo) p.frowsum = f_row_sums;  // all-ones grad_f_out: c = rowsum(f)[idx]
   p.gfo = gfo;
   p.q = q;
   p.f = f;
@@ -802,6 +925,15 @@ int ragged_grad_q_impl(const char* cs, const void* segs, const float* q, const f
   p.cs = cs;
   p.segs = segs;
   query_order1_kernel<float><<<blocks_for(cap_q * 32, 256), 256, 0, st>>>(p);
+  note_launches(1);
+  return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
+}
+
+int launch_row_sums(const void* f, int64_t rows, int F, int dtype, void* out, cudaStream_t st) {
+  if (dtype == KNNAG_F64)
+    row_sum_kernel<double><<<blocks_for(rows * 32, 256), 256, 0, st>>>((const double*)f, rows, F, (double*)out);
+  else
+    row_sum_kernel<float><<<blocks_for(rows * 32, 256), 256, 0, st>>>((const float*)f, rows, F, (float*)out);
   note_launches(1);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }

@@ -134,7 +134,9 @@ int ragged_forward_impl(const char* cs, const void* segs, const float* q, const 
                         int64_t cap_q, int64_t cap_e, int max_k, int ntile_cap, int splits, float* f_out, float* w_out,
                         float* dists, int64_t* idxs, void* workspace, cudaStream_t st);
 int ragged_grad_q_impl(const char* cs, const void* segs, const float* q, const float* f, int F, const float* gfo,
-                       const int64_t* idxs, int64_t cap_q, float* dq, const int* status, cudaStream_t st);
+                       const float* f_row_sums, const int64_t* idxs, int64_t cap_q, float* dq, const int* status,
+                       cudaStream_t st);
+int launch_row_sums(const void* f, int64_t rows, int F, int dtype, void* out, cudaStream_t st);
 template <typename T>
 int launch_exact(const ExactParams<T>& a, cudaStream_t st);
 int variants_precomputed(const void* q, const void* f, const void* rec, const int64_t* idxs, int B, int Q, int P,

@@ -259,9 +259,9 @@ int knnag_ragged_forward(const void* cloudset, const void* segments, const float
 }
 
 int knnag_ragged_grad_q(const void* cloudset, const void* segments, const float* q, const float* f, int F,
-                        const float* grad_f_out, const int64_t* idxs, int cap_segments, long long cap_queries,
-                        long long cap_entries, int max_k, int max_cloud_points, float* dq, void* workspace,
-                        size_t workspace_bytes, void* stream) {
+                        const float* grad_f_out, const float* f_row_sums, const int64_t* idxs, int cap_segments,
+                        long long cap_queries, long long cap_entries, int max_k, int max_cloud_points, float* dq,
+                        void* workspace, size_t workspace_bytes, void* stream) {
   if (!cloudset || !segments || !q || !f || !idxs || !dq || !workspace) return KNNAG_ERR_ARG;
   if (cap_segments < 1 || cap_queries < 1 || cap_entries < 1 || F < 0 || max_cloud_points < 1) return KNNAG_ERR_ARG;
   if (max_k < 1 || max_k > max_cloud_points) return KNNAG_ERR_K;
@@ -275,8 +275,15 @@ int knnag_ragged_grad_q(const void* cloudset, const void* segments, const float*
   int rc = launch_validate_segments(static_cast<const char*>(cloudset), segments, cap_segments, cap_queries,
                                     cap_entries, max_k, ntile_cap, 0, status, st);
   if (rc) return rc;
-  return ragged_grad_q_impl(static_cast<const char*>(cloudset), segments, q, f, F, grad_f_out, idxs, cap_queries, dq,
-                            status, st);
+  return ragged_grad_q_impl(static_cast<const char*>(cloudset), segments, q, f, F, grad_f_out, f_row_sums, idxs,
+                            cap_queries, dq, status, st);
+}
+
+int knnag_feature_row_sums(const void* f, long long rows, int F, int dtype, void* out, void* stream) {
+  if (!f || !out || rows < 0 || F < 1) return KNNAG_ERR_ARG;
+  if (dtype != KNNAG_F32 && dtype != KNNAG_F64) return KNNAG_ERR_DTYPE;
+  if (rows == 0) return KNNAG_OK;
+  return launch_row_sums(f, rows, F, dtype, out, static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

@@ -44,8 +44,9 @@ _SIGS = {
     "knnag_ragged_workspace_bytes": ([_I, ctypes.c_longlong], _S),
     "knnag_ragged_forward": ([_V, _V, _V, _V, _I, _I, ctypes.c_longlong, ctypes.c_longlong, _I, _I, _I]
                              + [_V] * 4 + [_V, _S, _V], _I),
-    "knnag_ragged_grad_q": ([_V, _V, _V, _V, _I, _V, _V, _I, ctypes.c_longlong, ctypes.c_longlong, _I, _I, _V, _V,
-                             _S, _V], _I),
+    "knnag_ragged_grad_q": ([_V, _V, _V, _V, _I, _V, _V, _V, _I, ctypes.c_longlong, ctypes.c_longlong, _I, _I, _V,
+                             _V, _S, _V], _I),
+    "knnag_feature_row_sums": ([_V, ctypes.c_longlong, _I, _I, _V, _V], _I),
     "knnag_points_bytes": ([_I, _I, _I], _S),
     "knnag_pack_points": ([_V, _V, _V, _I, _I, _I, _V, _V], _I),
     "knnag_adjacency_bytes": ([_I, _I, _I, _I], _S),

@@ -6,8 +6,8 @@ host loop of calls.  Here:
 
 * ``CloudSet`` keeps C clouds (p, sigma, R, f concatenated in cloud order)
   resident on the device together with their search index (packed records,
-  Morton-sorted tiles, tile key bounds), built once and rebuilt in place when
-  the geometry changes.
+  Hilbert-sorted tiles, tile key bounds) and the per-point row sums of f,
+  built once and rebuilt in place when the geometry or the features change.
 * A segment table lists the query sets of one call: segment s has Q_s queries
   against cloud ``cloud_s`` with K_s neighbours.  ``ragged_forward`` runs all
   of them in one launch sequence; per segment the result is bit-identical to
@@ -98,9 +98,11 @@ class CloudSet:
         self.buf = torch.empty(nb, dtype=torch.uint8, device=self.device)
         self._ws = torch.empty(max(1, L.knnag_cloudset_build_workspace_bytes(self.C, self._P)), dtype=torch.uint8,
                                device=self.device)
+        self.f_row_sums = torch.empty(n, device=self.device)
         with torch.cuda.device(self.device):
             _check(L.knnag_cloudset_init(self.C, self._P, _ptr(self.buf), nb, _stream(self.device)))
             self.build()
+            self.features_changed()
 
     @classmethod
     def from_clouds(cls, clouds):
@@ -113,6 +115,12 @@ class CloudSet:
         _check(capi.lib().knnag_cloudset_build(_ptr(self.p), _ptr(self.sigma), _ptr(self.R), self.C, self._P,
                                                _ptr(self.buf), self.buf.numel(), _ptr(self._ws), self._ws.numel(),
                                                _stream(self.device)))
+
+    def features_changed(self):
+        """Recompute the per-point feature row sums d(sum f_out)/dq uses
+        (call after changing f in place; capturable)."""
+        _check(capi.lib().knnag_feature_row_sums(_ptr(self.f), self.f.shape[0], self.F, capi.F32,
+                                                 _ptr(self.f_row_sums), _stream(self.device)))
 
     def cloud(self, c):
         """(p, sigma, R, f) views of cloud c."""
@@ -230,7 +238,8 @@ def ragged_forward(cloudset: CloudSet, q, clouds, Qs, Ks, splits=None, grad_q=No
             dq = torch.zeros(max(total_q, 1), 3, device=dev)[:total_q]
             gws = torch.empty(256, dtype=torch.uint8, device=dev)
             _check(L.knnag_ragged_grad_q(_ptr(cloudset.buf), _ptr(table.dev), _ptr(qp), _ptr(cloudset.f), F,
-                                         _ptr(grad_f_out), _ptr(idxs), len(clouds), cap_q, max(total_e, 1), max_k,
+                                         _ptr(grad_f_out), None if grad_f_out is not None else _ptr(cloudset.f_row_sums),
+                                         _ptr(idxs), len(clouds), cap_q, max(total_e, 1), max_k,
                                          cloudset.max_points, _ptr(dq), _ptr(gws), gws.numel(), st))
             res.dq = dq
         # the pinned table must outlive the asynchronous copy
@@ -357,7 +366,8 @@ class RaggedExecutor:
                                       self.cs.max_points, self.splits, _ptr(self.f_out), _ptr(self.w_out),
                                       _ptr(self.dists), _ptr(self.idxs), _ptr(self.ws), self.ws.numel(), st))
         _check(L.knnag_ragged_grad_q(_ptr(self.cs.buf), _ptr(self.table.dev), _ptr(self.q_dev), _ptr(self.cs.f),
-                                     self.cs.F, None, _ptr(self.idxs), self.cap_segments, self.cap_q, self.cap_e,
+                                     self.cs.F, None, _ptr(self.cs.f_row_sums), _ptr(self.idxs), self.cap_segments,
+                                     self.cap_q, self.cap_e,
                                      self.max_k, self.cs.max_points, _ptr(self.dq), _ptr(self.gws), self.gws.numel(),
                                      st))
 

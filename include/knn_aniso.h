@@ -288,11 +288,19 @@ int knnag_ragged_forward(const void* cloudset, const void* segments, const float
 /* dq = d<grad_f_out, f_out>/dq of the segments marked want_grad (rows
  * [0, their total Q)) at the forward's idxs (weights recomputed; grad_f_out
  * NULL means all ones, i.e. d(sum f_out)/dq) -- the first-order query
- * gradient of knnag_backward.  workspace: 256 bytes (status word). */
+ * gradient of knnag_backward.  With grad_f_out NULL, f_row_sums (optional,
+ * [sum P], from knnag_feature_row_sums of f) replaces the F-wide dot
+ * products by c = rowsum(f)[idx], bit-identical to what the uniform op's
+ * backward of f_out.sum() computes.  workspace: 256 bytes (status word). */
 int knnag_ragged_grad_q(const void* cloudset, const void* segments, const float* q, const float* f, int F,
-                        const float* grad_f_out, const int64_t* idxs, int cap_segments, long long cap_queries,
-                        long long cap_entries, int max_k, int max_cloud_points, float* dq, void* workspace,
-                        size_t workspace_bytes, void* stream);
+                        const float* grad_f_out, const float* f_row_sums, const int64_t* idxs, int cap_segments,
+                        long long cap_queries, long long cap_entries, int max_k, int max_cloud_points, float* dq,
+                        void* workspace, size_t workspace_bytes, void* stream);
+
+/* Per-row sums over the F columns of f [rows, F] (dtype) into out [rows],
+ * in the fixed order the backward entry points use.  No reference
+ * counterpart. */
+int knnag_feature_row_sums(const void* f, long long rows, int F, int dtype, void* out, void* stream);
 
 /* ---------------------------------------------------------- instrumentation
  * No reference counterpart (the reference has no timing hooks). */
