@@ -66,14 +66,20 @@ struct SearchParams {
 // Search CTA: 4 warps; G warps split the points of one 32-query group.
 constexpr int kSearchThreads = 128;
 constexpr int kQueueCap = 8;
+// Tile buffers of the search ring: visit v lands in buffer v % kTileBufs,
+// so kTileBufs - 1 copies are in flight while a tile is being read.
+constexpr int kTileBufs = 2;
+// the tail of region B holds kTileBufs mbarriers (8 B), kTileBufs counters
+// (4 B) and two flags (4 B each)
+static_assert(kTileBufs * 12 + 8 <= 64, "search ring bookkeeping exceeds its 64 bytes");
 
 // Shared-memory bytes of the search kernel for (KMAX, G).
 __host__ __device__ inline constexpr size_t search_merge_bytes(int kmax, int g) {
   return (g > 1) ? (size_t)kSearchThreads * (kmax + 1) * 8 + (size_t)kSearchThreads * 4 : 0;
 }
 __host__ __device__ inline constexpr size_t search_region_a_bytes(int kmax, int g) {
-  // phase 1: two tiles of 64 pairs x 128 B
-  size_t tiles = 2 * 64 * 128;
+  // phase 1: kTileBufs tiles of 64 pairs x 128 B
+  size_t tiles = (size_t)kTileBufs * 64 * 128;
   int qpc = 32 * (4 / g);
   int L = kmax + 1;
   size_t merge = (g > 1) ? (size_t)kSearchThreads * L * 8 + (size_t)kSearchThreads * 4 : 0;
@@ -82,7 +88,8 @@ __host__ __device__ inline constexpr size_t search_region_a_bytes(int kmax, int 
   return tiles > phase2 ? tiles : phase2;
 }
 __host__ __device__ inline constexpr size_t search_region_b_bytes() {
-  // candidate queues (keys + idx), shared thresholds (double-buffered), 2 mbarriers
+  // candidate queues (keys + idx), shared thresholds, then 64 bytes for the
+  // kTileBufs mbarriers, their counters and two flags
   return (size_t)kQueueCap * kSearchThreads * 8 + 2 * (size_t)kSearchThreads * 4 + 64;
 }
 __host__ __device__ inline constexpr size_t search_smem_bytes(int kmax, int g) {

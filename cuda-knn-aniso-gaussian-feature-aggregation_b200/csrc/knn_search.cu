@@ -430,7 +430,7 @@ __device__ __forceinline__ uint64_t* search_barriers(unsigned char* smem, size_t
 // when a tile copy timed out (status flagged; the CTA must stop).
 template <int KMAX, int G>
 __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchItem& it, unsigned char* smem,
-                                            int ntp_cap, uint32_t (&uses)[2]) {
+                                            int ntp_cap, uint32_t (&uses)[kTileBufs]) {
   constexpr int L = KMAX + 1;
   constexpr int QPC = 32 * (4 / G);
   constexpr int PPT = kTilePoints / 2;  // pairs per tile
@@ -444,8 +444,8 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   int* qv = reinterpret_cast<int*>(qk + kQueueCap * kSearchThreads);
   float* tau_share = reinterpret_cast<float*>(qv + kQueueCap * kSearchThreads);  // [2][128]
   uint64_t* full = reinterpret_cast<uint64_t*>(tau_share + 2 * kSearchThreads);
-  int* cnt = reinterpret_cast<int*>(full + 2);                       // [2] warps done per buffer
-  volatile int* s_final = reinterpret_cast<volatile int*>(cnt + 2);  // visit count once stopped
+  int* cnt = reinterpret_cast<int*>(full + kTileBufs);               // warps done per buffer
+  volatile int* s_final = reinterpret_cast<volatile int*>(cnt + kTileBufs);  // visit count once stopped
   volatile int* s_abort = s_final + 1;                               // a wait gave up
   // region C: per-tile lower bounds (sorted), visit order, query bookkeeping
   const int NTP = search_tiles_pow2(it.ntile);
@@ -586,9 +586,9 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   const int ntile = it.ntile;
   const bool seed = G > 1 && ntile > kSeedTiles;
   const float* pairs_b = it.pairs;
-  // visit position v reads tile lbt[v] into buffer v & 1
+  // visit position v reads tile lbt[v] into buffer v % kTileBufs
   auto issue = [&](int v) {
-    const int buf = v & 1;
+    const int buf = v % kTileBufs;
     mbar_arrive_expect_tx(&full[buf], kTileBytes);
     bulk_copy_g2s(regA + buf * kTileBytes, pairs_b + (int64_t)lbt[v] * PPT * kPairFloats, kTileBytes, &full[buf]);
   };
@@ -602,20 +602,21 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     }
     return false;
   };
-  // No visit v: record the count and complete buffer v&1's next phase with a
-  // plain arrive, so the warps waiting for visit v wake up and stop.
+  // No visit v: record the count and complete its buffer's next phase with
+  // a plain arrive, so the warps waiting for visit v wake up and stop.
   auto stop = [&](int v) {
     *s_final = v;
     __threadfence_block();
-    mbar_arrive(&full[v & 1]);
+    mbar_arrive(&full[v % kTileBufs]);
   };
   if (tid == 0) {
     *s_nvisit = 0;
     *s_final = 0x7fffffff;
     *s_abort = 0;
-    cnt[0] = cnt[1] = 0;
+    for (int b = 0; b < kTileBufs; ++b) cnt[b] = 0;
     fence_proxy_async_smem();  // region A was last written by generic stores
-    for (int v = 0; v < 2; ++v) {
+    // the seed merge reuses region A, so only the seed tiles go first then
+    for (int v = 0; v < (seed ? kSeedTiles : kTileBufs); ++v) {
       if (decide(v, INFINITY)) {
         issue(v);
       } else {
@@ -626,17 +627,18 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   }
   __syncthreads();
 
-  // Tile loop without CTA barriers.  Visit t sits in buffer t & 1; each warp
+  // Tile loop without CTA barriers.  Visit t sits in buffer t % kTileBufs; each warp
   // waits for its copy, reads its split of the pairs, publishes its list top
   // in tau_share and counts itself out of the tile.  The warp that counts
   // out last knows every warp is done with the buffer: it re-arms the counter
-  // and decides (and issues) visit t + 2 into the same buffer.  A warp does
-  // that duty before it starts its next tile, so the decision for t + 1 is
-  // complete before any warp can be last for tile t: decisions stay in order.
+  // and decides (and issues) visit t + kTileBufs into the same buffer.  A warp
+  // does that duty before it starts its next tile, so the decision for
+  // t + kTileBufs - 1 is complete before any warp can be last for tile t:
+  // decisions stay in order.
   int t = 0;
   for (;; ++t) {
-    const int buf = t & 1;
-    const bool ok = mbar_wait_bounded(&full[buf], (uses[buf] + (t >> 1)) & 1);
+    const int buf = t % kTileBufs;
+    const bool ok = mbar_wait_bounded(&full[buf], (uses[buf] + t / kTileBufs) & 1);
     if (!ok) {
       if (lane == 0) {
         atomicOr(a.status, kStatusWaitTimeout);
@@ -732,7 +734,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
       if (tid == 0) {
         cnt[buf] = 0;
         fence_proxy_async_smem();
-        for (int v = kSeedTiles; v < kSeedTiles + 2; ++v) {
+        for (int v = kSeedTiles; v < kSeedTiles + kTileBufs; ++v) {
           if (decide(v, tmax)) {
             issue(v);
           } else {
@@ -749,7 +751,8 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     tau = fminf(tau, tm);
     if (last) {
       // every warp is done with this buffer: re-arm its counter, then decide
-      // visit t + 2 (deferred during the seed tiles) unless a stop was made
+      // visit t + kTileBufs (deferred during the seed tiles) unless a stop
+      // was made
       const bool deferred = seed && t < kSeedTiles - 1;
       float tmax = -INFINITY;
       if (!deferred) {
@@ -761,11 +764,11 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
       if (lane == 0) {
         cnt[buf] = 0;
         if (!deferred && *s_final == 0x7fffffff && !*s_abort) {
-          if (decide(t + 2, tmax)) {
+          if (decide(t + kTileBufs, tmax)) {
             fence_proxy_async_smem();
-            issue(t + 2);
+            issue(t + kTileBufs);
           } else {
-            stop(t + 2);
+            stop(t + kTileBufs);
           }
         }
       }
@@ -777,16 +780,16 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   __syncthreads();
   if (*s_abort) {
     if (tid == 0) {
-      // best effort: let the copies of the last two issued visits land
-      for (int v = *s_nvisit - 2; v < *s_nvisit; ++v)
-        if (v >= 0) mbar_wait_bounded(&full[v & 1], (uses[v & 1] + (v >> 1)) & 1);
+      // best effort: let the copies of the last issued visits land
+      for (int v = *s_nvisit - kTileBufs; v < *s_nvisit; ++v)
+        if (v >= 0) mbar_wait_bounded(&full[v % kTileBufs], (uses[v % kTileBufs] + v / kTileBufs) & 1);
     }
     return false;
   }
   {
     const int n = t + 1;  // phases waited on: visits 0..t (t = the stop visit)
-    uses[0] += (n + 1) >> 1;
-    uses[1] += n >> 1;
+#pragma unroll
+    for (int b = 0; b < kTileBufs; ++b) uses[b] += n > b ? (n - b + kTileBufs - 1) / kTileBufs : 0;
   }
 
   // ---- merge the G split lists; region A is free (no copy in flight, all
@@ -882,8 +885,7 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* full = search_barriers(smem, search_region_a_bytes(KMAX, G));
   if (threadIdx.x == 0) {
-    mbar_init(&full[0], 1);
-    mbar_init(&full[1], 1);
+    for (int b = 0; b < kTileBufs; ++b) mbar_init(&full[b], 1);
     fence_mbar_init();
   }
   __syncthreads();
@@ -905,7 +907,7 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
   it.K = a.K;
   it.ntile = a.ntile;
   it.qblock = blockIdx.x;
-  uint32_t uses[2] = {0u, 0u};
+  uint32_t uses[kTileBufs] = {};
   search_item<KMAX, G>(a, it, smem, search_tiles_pow2(a.ntile), uses);
 }
 
@@ -920,8 +922,7 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_r
   if (*a.status) return;  // the table failed validation
   uint64_t* full = search_barriers(smem, search_region_a_bytes(KMAX, G));
   if (threadIdx.x == 0) {
-    mbar_init(&full[0], 1);
-    mbar_init(&full[1], 1);
+    for (int b = 0; b < kTileBufs; ++b) mbar_init(&full[b], 1);
     fence_mbar_init();
   }
   __syncthreads();
@@ -935,7 +936,7 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_r
   const int nseg = sh->nseg, n_items = sh->n_items;
   const int ntp_cap = search_tiles_pow2(a.ntile);
   constexpr int QPC = 32 * (4 / G);
-  uint32_t uses[2] = {0u, 0u};
+  uint32_t uses[kTileBufs] = {};
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(a.item_counter, 1);
     __syncthreads();
