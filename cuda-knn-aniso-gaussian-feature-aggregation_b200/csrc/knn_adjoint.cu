@@ -208,58 +208,115 @@ __global__ void adj_fill_kernel(const int64_t* __restrict__ idxs, int n, int qk,
   }
 }
 
-// Sort every row by entry id, one warp per row.  Rows of up to 64 entries
-// are bitonic-sorted in registers (two per lane); longer rows place each id
-// at the number of smaller ids in the row (ids in a row are distinct because
-// a query selects a point at most once; equal ids keep their order).
-__global__ void adj_sort_kernel(const int* __restrict__ rowptr, const int* __restrict__ unsorted, int n_rows,
-                                int* __restrict__ entries) {
+// Bitonic sort, ascending, of the 32*V ints of a warp: element lane + 32*h
+// sits in x[h].  Stages with a partner distance below 32 exchange through
+// shuffles, the others inside the lane.
+template <int V>
+__device__ __forceinline__ void warp_bitonic_sort(int (&x)[V], int lane) {
+#pragma unroll
+  for (int k = 2; k <= 32 * V; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= 32) {
+#pragma unroll
+        for (int h = 0; h < V; ++h) {
+          const int hp = h ^ (j >> 5);
+          if (hp > h) {
+            const bool up = ((32 * h) & k) == 0;  // lane < 32 <= j < k
+            const int lo = min(x[h], x[hp]), hi = max(x[h], x[hp]);
+            x[h] = up ? lo : hi;
+            x[hp] = up ? hi : lo;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int h = 0; h < V; ++h) {
+          const int e = lane + 32 * h;
+          const int o = __shfl_xor_sync(0xffffffffu, x[h], j);
+          const bool up = (e & k) == 0, lower = (e & j) == 0;
+          x[h] = (lower == up) ? min(x[h], o) : max(x[h], o);
+        }
+      }
+    }
+  }
+}
+
+template <int V>
+__device__ __forceinline__ void sort_row_regs(const int* src, int n, int* dst, int lane) {
+  int x[V];
+#pragma unroll
+  for (int h = 0; h < V; ++h) x[h] = lane + 32 * h < n ? src[lane + 32 * h] : 0x7fffffff;
+  warp_bitonic_sort<V>(x, lane);
+#pragma unroll
+  for (int h = 0; h < V; ++h)
+    if (lane + 32 * h < n) dst[lane + 32 * h] = x[h];
+}
+
+constexpr int kAdjSortWarps = 8;      // warps per CTA of adj_sort_kernel
+constexpr int kAdjSmemSort = 1024;    // longest row sorted in shared memory
+
+// Sort every row by entry id, one warp per row (ids in a row are distinct:
+// a query selects a point at most once).  Rows of up to 256 entries are
+// bitonic-sorted in registers, rows of up to 1024 in the warp's shared
+// memory; longer rows place each id at the number of smaller ids in the row.
+__global__ void __launch_bounds__(kAdjSortWarps * 32) adj_sort_kernel(const int* __restrict__ rowptr,
+                                                                     const int* __restrict__ unsorted, int n_rows,
+                                                                     int* __restrict__ entries) {
+  __shared__ int sbuf[kAdjSortWarps][kAdjSmemSort];
   const int lane = threadIdx.x & 31;
+  int* sb = sbuf[threadIdx.x >> 5];
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int r = gw; r < n_rows; r += nw) {
     const int start = rowptr[r];
     const int n = rowptr[r + 1] - start;
-    if (n <= 64) {
-      int x[2];
-      x[0] = lane < n ? unsorted[start + lane] : 0x7fffffff;
-      x[1] = lane + 32 < n ? unsorted[start + lane + 32] : 0x7fffffff;
-#pragma unroll
-      for (int k = 2; k <= 64; k <<= 1) {
-#pragma unroll
+    const int* src = unsorted + start;
+    int* dst = entries + start;
+    if (n <= 32) {
+      sort_row_regs<1>(src, n, dst, lane);
+    } else if (n <= 64) {
+      sort_row_regs<2>(src, n, dst, lane);
+    } else if (n <= 128) {
+      sort_row_regs<4>(src, n, dst, lane);
+    } else if (n <= 256) {
+      sort_row_regs<8>(src, n, dst, lane);
+    } else if (n <= kAdjSmemSort) {
+      int n2 = 512;
+      while (n2 < n) n2 <<= 1;
+      for (int i = lane; i < n2; i += 32) sb[i] = i < n ? src[i] : 0x7fffffff;
+      __syncwarp();
+      for (int k = 2; k <= n2; k <<= 1) {
         for (int j = k >> 1; j > 0; j >>= 1) {
-          if (j == 32) {
-            const int lo = min(x[0], x[1]), hi = max(x[0], x[1]);
-            x[0] = lo;
-            x[1] = hi;
-          } else {
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              const int e = lane + 32 * h;
-              const int o = __shfl_xor_sync(0xffffffffu, x[h], j);
-              const bool up = (e & k) == 0, lower = (e & j) == 0;
-              x[h] = (lower == up) ? min(x[h], o) : max(x[h], o);
+          for (int i = lane; i < n2; i += 32) {
+            const int ixj = i ^ j;
+            if (ixj > i) {
+              const int a = sb[i], b = sb[ixj];
+              if ((a > b) == ((i & k) == 0)) {
+                sb[i] = b;
+                sb[ixj] = a;
+              }
             }
           }
+          __syncwarp();
         }
       }
-      if (lane < n) entries[start + lane] = x[0];
-      if (lane + 32 < n) entries[start + lane + 32] = x[1];
-      continue;
-    }
-    for (int base = 0; base < n; base += 32) {
-      const int i = base + lane;
-      const int v = (i < n) ? unsorted[start + i] : 0;
-      int rank = 0;
-      for (int jb = 0; jb < n; jb += 32) {
-        const int uj = (jb + lane < n) ? unsorted[start + jb + lane] : 0x7fffffff;
-        const int lim = min(32, n - jb);
-        for (int jj = 0; jj < lim; ++jj) {
-          const int u = __shfl_sync(0xffffffffu, uj, jj);
-          rank += (u < v || (u == v && jb + jj < i)) ? 1 : 0;  // stable even if ids repeat
+      for (int i = lane; i < n; i += 32) dst[i] = sb[i];
+      __syncwarp();
+    } else {
+      for (int base = 0; base < n; base += 32) {
+        const int i = base + lane;
+        const int v = (i < n) ? src[i] : 0;
+        int rank = 0;
+        for (int jb = 0; jb < n; jb += 32) {
+          const int uj = (jb + lane < n) ? src[jb + lane] : 0x7fffffff;
+          const int lim = min(32, n - jb);
+          for (int jj = 0; jj < lim; ++jj) {
+            const int u = __shfl_sync(0xffffffffu, uj, jj);
+            rank += (u < v || (u == v && jb + jj < i)) ? 1 : 0;  // stable even if ids repeat
+          }
         }
+        if (i < n) dst[rank] = v;
       }
-      if (i < n) entries[start + rank] = v;
     }
   }
 }
@@ -309,7 +366,9 @@ int launch_build_adjacency(const int64_t* idxs, int B, int Q, int P, int K, void
   const int rc = launch_exclusive_scan(cursor, rows, rowptr, st);
   if (rc) return rc;
   adj_fill_kernel<<<blocks_for(n, 256), 256, 0, st>>>(idxs, n, qk, P, rowptr, cursor, unsorted);
-  adj_sort_kernel<<<blocks_for((int64_t)rows * 32, 256), 256, 0, st>>>(rowptr, unsorted, rows, entries);
+  const int sort_threads = kAdjSortWarps * 32;
+  adj_sort_kernel<<<blocks_for((int64_t)rows * 32, sort_threads), sort_threads, 0, st>>>(rowptr, unsorted, rows,
+                                                                                       entries);
   note_launches(3);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }

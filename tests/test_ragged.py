@@ -334,6 +334,31 @@ def test_adjacency_long_scan(rows):
 
 
 @pytest.mark.gpu
+def test_adjacency_row_lengths():
+    """Rows of every length class the row sort distinguishes (register
+    networks up to 32/64/128/256 entries, shared memory up to 1024, the
+    ranking loop beyond), each at and one past its limit, in shuffled
+    order: every row holds its entry ids ascending."""
+    from cuda_knn_aggregate import capi
+
+    lengths = [0, 1, 2, 31, 32, 33, 63, 64, 65, 127, 128, 129, 255, 256, 257, 511, 512, 513, 1023, 1024, 1025, 2500]
+    rows = len(lengths) + 5  # a few empty rows at the end
+    K = 4
+    flat = np.concatenate([np.full(n, r, dtype=np.int64) for r, n in enumerate(lengths)])
+    flat = np.concatenate([flat, np.zeros((-len(flat)) % K, dtype=np.int64)])  # pad to whole queries (row 0)
+    rng = np.random.default_rng(7)
+    rng.shuffle(flat)
+    Q = len(flat) // K
+    idxs = torch.from_numpy(flat.reshape(1, Q, K))
+    adj = capi.build_adjacency(idxs.cuda(), rows)
+    rowptr, entries = capi.adjacency_arrays(adj, 1, Q, rows, K)
+    torch.cuda.synchronize()
+    counts = np.bincount(flat, minlength=rows)
+    assert np.array_equal(rowptr.cpu().numpy(), np.concatenate([[0], np.cumsum(counts)]))
+    assert np.array_equal(entries.cpu().numpy(), np.argsort(flat, kind="stable"))
+
+
+@pytest.mark.gpu
 def test_ragged_long_query_scan():
     """A ragged call whose query-cell array needs the multi-CTA scan."""
     from cuda_knn_aggregate.ragged import CloudSet, ragged_forward
