@@ -45,6 +45,7 @@ __host__ __device__ inline int64_t round_up(int64_t x, int64_t m) { return (x + 
 // queries flagged for the exact MinK replay.
 constexpr int kStatusWaitTimeout = 1;
 constexpr int kStatusBadTable = 2;  // a segment table entry the kernel cannot serve
+constexpr int kStatusBadIndex = 4;  // an internal index out of range (self-check; the access was skipped)
 
 // ---------------------------------------------------------------- keys
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }

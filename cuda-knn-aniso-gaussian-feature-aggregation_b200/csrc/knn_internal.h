@@ -32,10 +32,11 @@ struct ExactParams {
   // ragged calls (FP32): per-query sizes and offsets from the segment table,
   // records from the cloud set.  List items are global query rows; without a
   // list the kernel serves the queries of segments with K > 32.  Nothing is
-  // done when *status is nonzero (a table that failed validation).
+  // done when *status is nonzero (a table that failed validation); a list
+  // row out of range latches kStatusBadIndex there.
   const char* cs;
   const void* segs;
-  const int* status;
+  int* status;
 };
 
 struct SearchParams {

@@ -110,6 +110,10 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
       int s;
       if (a.use_list) {
         bq = a.list[item];
+        if (bq < 0 || bq >= sh->total_q) {  // the search lists its own rows: never taken
+          if (tid == 0) atomicOr(a.status, kStatusBadIndex);
+          continue;
+        }
         s = seg_of_row(sd, sh->nseg, bq);
       } else {
         s = seg_of_bigk(sd, sh->nseg, item);
@@ -126,6 +130,7 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
       if (K > a.K || K > P) continue;  // the host checked the table; never reached
     } else {
       bq = a.use_list ? (int64_t)a.list[item] : item;
+      if (bq < 0 || bq >= (int64_t)a.B * a.Q) continue;  // the search lists its own rows: never taken
       b = bq / a.Q;
       K = a.K;
       P = a.P;
@@ -467,8 +472,13 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   const int split = warp % G, grp = warp / G;
   const int lq = grp * 32 + lane;
   const int sp = it.qblock * QPC + lq;  // position in the spatial order
-  const bool valid = sp < it.Q;
-  const int qi = it.perm_q[valid ? sp : it.Q - 1];
+  bool valid = sp < it.Q;
+  int qi = it.perm_q[valid ? sp : it.Q - 1];
+  if ((unsigned)qi >= (unsigned)it.Q) {  // the query order is a permutation: never taken
+    if (valid) atomicOr(a.status, kStatusBadIndex);
+    qi = 0;
+    valid = false;
+  }
   const int K = it.K, P = it.P;
 
   const float qx = it.q[(int64_t)qi * 3 + 0], qy = it.q[(int64_t)qi * 3 + 1], qz = it.q[(int64_t)qi * 3 + 2];
@@ -596,11 +606,14 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   // ascending, so nothing after it is needed either).  Decisions are made
   // one visit at a time, in order (see below), so *s_nvisit == v here.
   auto decide = [&](int v, float tmax) {
-    if (v < ntile && *s_nvisit == v && lbt[v] < ntile && !(lbk[v] > tmax)) {
-      *s_nvisit = v + 1;
-      return true;
+    if (v >= ntile || *s_nvisit != v) return false;
+    if ((unsigned)lbt[v] >= (unsigned)ntile) {  // real tiles sort first: never taken
+      atomicOr(a.status, kStatusBadIndex);
+      return false;
     }
-    return false;
+    if (lbk[v] > tmax) return false;
+    *s_nvisit = v + 1;
+    return true;
   };
   // No visit v: record the count and complete its buffer's next phase with
   // a plain arrive, so the warps waiting for visit v wake up and stop.
@@ -821,16 +834,20 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   }
   if (split == 0) {
     const int nneed = (P > K) ? K + 1 : K;
-    bool fl = nan_fill;
-    for (int j = 0; j < nneed; ++j)
-      if (out_i[lq * L + j] < 0) fl = true;
+    bool fl = nan_fill, bad = false;
+    for (int j = 0; j < nneed; ++j) {
+      const int idx = out_i[lq * L + j];
+      if (idx < 0) fl = true;
+      if (idx >= P) bad = true;  // tiles carry indices of their own cloud: never taken
+    }
+    if (bad && valid) atomicOr(a.status, kStatusBadIndex);
     for (int j = 0; j + 1 < nneed; ++j)
       if (out_k[lq * L + j] == out_k[lq * L + j + 1]) fl = true;
     const float m = (P > K) ? out_k[lq * L + K] : INFINITY;
     if (fl_tie <= m) fl = true;
     for (int j = 0; j < K; ++j) out_w[lq * L + j] = weight_of(out_k[lq * L + j]);
-    out_f[lq] = (fl || !valid) ? 1 : 0;
-    if (valid && fl) {
+    out_f[lq] = (fl || bad || !valid) ? 1 : 0;
+    if (valid && fl && !bad) {
       const int pos = atomicAdd(a.flag_count, 1);
       a.flag_list[pos] = (int)(it.row0 + qi);
     }
@@ -942,6 +959,10 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_r
     __syncthreads();
     const int item = s_item;
     if (item >= n_items) break;
+    if (item < 0) {  // the counter starts at 0 and only grows: never taken
+      if (threadIdx.x == 0) atomicOr(a.status, kStatusBadIndex);
+      break;
+    }
     const SegDesc g = sd[seg_of_item(sd, nseg, item)];
     const CloudDesc c = cd[g.cloud];
     if (g.K < 1 || g.K > KMAX || g.K > c.P || c.ntile > a.ntile || sh->qpc != QPC) {

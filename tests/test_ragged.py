@@ -252,14 +252,17 @@ def test_invalid_table_latches_and_writes_nothing():
     assert rc == 0
     assert L.knnag_read_device_status(_ptr(ws), st) == 7  # KNNAG_ERR_DEVICE
     assert bool((f_out == 7).all()) and bool((w == 7).all()) and bool((i == 7).all())
-    # the same call with room for the table succeeds
+    # the same call with room for the table succeeds (the buffers are held in
+    # names: a temporary passed as _ptr(torch.empty(...)) is freed at once and
+    # its memory handed to the next one)
+    f2, w2, d2 = torch.empty(1200, 4, device="cuda"), torch.empty(9600, device="cuda"), torch.empty(9600, device="cuda")
+    i2 = torch.empty(9600, dtype=torch.int64, device="cuda")
+    ws2 = torch.empty(L.knnag_ragged_workspace_bytes(2, 1200), dtype=torch.uint8, device="cuda")
     rc = L.knnag_ragged_forward(_ptr(cs.buf), _ptr(t.dev), _ptr(q), _ptr(cs.f), 4, 2, 1200, 9600, 8, 1000, 1,
-                                _ptr(torch.empty(1200, 4, device="cuda")), _ptr(torch.empty(9600, device="cuda")),
-                                _ptr(torch.empty(9600, device="cuda")),
-                                _ptr(torch.empty(9600, dtype=torch.int64, device="cuda")),
-                                _ptr(torch.empty(L.knnag_ragged_workspace_bytes(2, 1200), dtype=torch.uint8,
-                                                 device="cuda")), L.knnag_ragged_workspace_bytes(2, 1200), st)
+                                _ptr(f2), _ptr(w2), _ptr(d2), _ptr(i2), _ptr(ws2), ws2.numel(), st)
     assert rc == 0
+    assert L.knnag_read_device_status(_ptr(ws2), st) == 0
+    assert bool((i2 >= 0).all()) and bool((i2 < 1000).all())
 
 
 @pytest.mark.gpu
