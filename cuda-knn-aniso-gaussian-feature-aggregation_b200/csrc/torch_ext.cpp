@@ -8,6 +8,7 @@
 // the reuse of packed points, adjacency and coefficients that the autograd
 // layer uses.
 #include <ATen/cuda/CUDAContext.h>
+#include <ATen/cuda/CUDAEvent.h>
 #include <c10/cuda/CUDAGuard.h>
 #include <torch/extension.h>
 
@@ -301,6 +302,27 @@ torch::Tensor build_adjacency(torch::Tensor idxs, int64_t P) {
   return adj;
 }
 
+// The same on a pool stream forked from the current one, so that it runs
+// beside the next kernels of the current stream.  The buffer is allocated on
+// the current stream; the caller must call join.block(current stream)
+// before the buffer is used or released there.
+torch::Tensor build_adjacency_forked(const torch::Tensor& idxs, int64_t P, at::cuda::CUDAEvent& join) {
+  const int B = (int)idxs.size(0), Q = (int)idxs.size(1), K = (int)idxs.size(2);
+  check_k(K, (int)P);
+  const c10::cuda::CUDAGuard guard(idxs.device());
+  auto adj = scratch(knnag_adjacency_bytes(B, Q, (int)P, K), idxs);
+  const auto dev = idxs.device().index();
+  auto main = at::cuda::getCurrentCUDAStream(dev);
+  auto side = at::cuda::getStreamFromPool(false, dev);
+  at::cuda::CUDAEvent fork;
+  fork.record(main);
+  fork.block(side);
+  check_status(knnag_build_adjacency(idxs.data_ptr<int64_t>(), B, Q, (int)P, K, adj.data_ptr(), side.stream()),
+               "build_adjacency");
+  join.record(side);
+  return adj;
+}
+
 // rowptr [B*P+1] and sorted entry ids [B*Q*K] views of an adjacency buffer.
 std::vector<torch::Tensor> adjacency_views(torch::Tensor adj, int64_t B, int64_t Q, int64_t P, int64_t K) {
   const size_t rows = (size_t)B * P, n = (size_t)B * Q * K;
@@ -346,6 +368,10 @@ using torch::autograd::variable_list;
 
 constexpr int64_t kNeedBits[5] = {KNNAG_NEED_DQ, KNNAG_NEED_DP, KNNAG_NEED_DF, KNNAG_NEED_DSIGMA, KNNAG_NEED_DR};
 constexpr int64_t kPointBits = KNNAG_NEED_DP | KNNAG_NEED_DF | KNNAG_NEED_DSIGMA | KNNAG_NEED_DR;
+// Host-only flag of AggBackwardFn: the graph being built may ask the second
+// order for point gradients, so the adjacency is built now, beside the
+// first-order kernels (never passed to the C ABI).
+constexpr int64_t kPrebuildAdjacency = int64_t(1) << 20;
 
 torch::Tensor or_placeholder(const torch::Tensor& t, const torch::Tensor& like) {
   return t.defined() ? t : torch::empty({0}, like.options());
@@ -367,10 +393,15 @@ struct AggBackwardFn : public torch::autograd::Function<AggBackwardFn> {
                                torch::Tensor f, torch::Tensor sigma, torch::Tensor R, torch::Tensor idxs,
                                torch::Tensor points, int64_t needs) {
     torch::Tensor adj;
+    at::cuda::CUDAEvent join;
+    const bool forked = (needs & kPrebuildAdjacency) && !(needs & kPointBits);
+    needs &= ~kPrebuildAdjacency;
     if (needs & kPointBits) adj = build_adjacency(idxs, p.size(1));
+    if (forked) adj = build_adjacency_forked(idxs, p.size(1), join);
     auto o = backward_impl(1, c10::nullopt, gfo, q, p, f, sigma, R, c10::nullopt, idxs, points,
-                           adj.defined() ? c10::optional<torch::Tensor>(adj) : c10::nullopt, c10::nullopt, needs,
-                           true);
+                           (adj.defined() && !forked) ? c10::optional<torch::Tensor>(adj) : c10::nullopt,
+                           c10::nullopt, needs, true);
+    if (forked) join.block(at::cuda::getCurrentCUDAStream(q.device().index()));
     ctx->save_for_backward({gfo, q, p, f, sigma, R, idxs, points});
     ctx->saved_data["coef"] = o[5];
     ctx->saved_data["gfo_scalar"] = (needs & KNNAG_GFO_SCALAR) != 0;
@@ -420,8 +451,13 @@ struct AggFn : public torch::autograd::Function<AggFn> {
     if (!needs) return out;
     auto s = ctx->get_saved_variables();
     const bool scalar = is_broadcast_scalar(g[0]);
+    // create_graph with point inputs that require grad: the second order of
+    // this graph may want point gradients (the Eikonal step does)
+    const bool prebuild = torch::GradMode::is_enabled() &&
+                          (s[1].requires_grad() || s[2].requires_grad() || s[3].requires_grad() || s[4].requires_grad());
     auto r = AggBackwardFn::apply(scalar ? g[0] : g[0].contiguous(), s[0], s[1], s[2], s[3], s[4], s[5],
-                                  ctx->saved_data["points"].toTensor(), needs | (scalar ? KNNAG_GFO_SCALAR : 0));
+                                  ctx->saved_data["points"].toTensor(),
+                                  needs | (scalar ? KNNAG_GFO_SCALAR : 0) | (prebuild ? kPrebuildAdjacency : 0));
     for (int i = 0; i < 5; ++i) out[i] = (needs & kNeedBits[i]) ? r[i] : torch::Tensor();
     return out;
   }
