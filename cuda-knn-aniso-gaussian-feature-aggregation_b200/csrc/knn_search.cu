@@ -298,11 +298,13 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
 // key is a candidate when key <= tau (the tightest list top known to the
 // group); candidates are appended to a per-thread queue in shared memory and
 // folded into the list when any lane's queue is nearly full and at every
-// tile end, when the G splits also exchange their list tops.  After the
-// first kSeedTiles tiles the G lists of a query are merged once: split 0
-// keeps the exact top-(K+1) of those points and the other splits restart
-// from placeholder entries (index -2) at its (K+1)-th key, so they only
-// accept keys below it and no split refills a list from scratch.
+// tile end.  At every tile end each split also publishes two bounds on the
+// (K+1)-th smallest key of the union of the G lists of its query: its own
+// list top (the union holds K+1 keys at or below it) and its c-th smallest
+// key, c = ceil((K+1)/G) (the G splits together hold G*c >= K+1 keys at or
+// below the largest of those).  tau is the smallest of these bounds; any
+// published value, however stale, is a valid bound because a list only ever
+// gets smaller keys.  The G lists are merged once, after the last tile.
 //
 // Exactness.  The result equals the reference's MinK selection whenever the
 // K+1 smallest keys are pairwise distinct (then the top-K set and its order
@@ -314,7 +316,6 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
 // keys or an empty slot, when tie_key <= its merged (K+1)-th key, or when a
 // fill-phase key is NaN.
 
-constexpr int kSeedTiles = 2;
 constexpr unsigned kTileBytes = (kTilePoints / 2) * kPairFloats * 4;
 
 template <int L>
@@ -423,6 +424,20 @@ __device__ __forceinline__ float tile_lower_bound(const float* ti, const float* 
   return lb >= 0.f ? lb : 0.f;  // NaN: 0 (keys are >= 0 when mu >= 0)
 }
 
+// Bound on the (K+1)-th smallest key of query lq's G split lists, from the
+// published list tops (any one split's top) and c-th keys (the largest of
+// the G).
+template <int G, int QPC>
+__device__ __forceinline__ float query_bound(const float* tops, const float* cths, int lq) {
+  float tm = tops[lq], tc = cths[lq];
+#pragma unroll
+  for (int g = 1; g < G; ++g) {
+    tm = fminf(tm, tops[g * QPC + lq]);
+    tc = fmaxf(tc, cths[g * QPC + lq]);
+  }
+  return G > 1 ? fminf(tm, tc) : tm;
+}
+
 // The two tile-buffer mbarriers of a search CTA.
 __device__ __forceinline__ uint64_t* search_barriers(unsigned char* smem, size_t region_a) {
   return reinterpret_cast<uint64_t*>(smem + region_a + (size_t)kQueueCap * kSearchThreads * 8 +
@@ -447,7 +462,9 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   unsigned char* regA = smem;
   float* qk = reinterpret_cast<float*>(smem + RA);
   int* qv = reinterpret_cast<int*>(qk + kQueueCap * kSearchThreads);
-  float* tau_share = reinterpret_cast<float*>(qv + kQueueCap * kSearchThreads);  // [2][128]
+  // per split and query: list top, and c-th smallest key (G > 1)
+  float* tau_share = reinterpret_cast<float*>(qv + kQueueCap * kSearchThreads);  // [128]
+  float* cth_share = tau_share + kSearchThreads;                                 // [128]
   uint64_t* full = reinterpret_cast<uint64_t*>(tau_share + 2 * kSearchThreads);
   int* cnt = reinterpret_cast<int*>(full + kTileBufs);               // warps done per buffer
   volatile int* s_final = reinterpret_cast<volatile int*>(cnt + kTileBufs);  // visit count once stopped
@@ -489,6 +506,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   // any value written here is a valid bound, so it must not be a stale one
   // from the previous item)
   tau_share[split * QPC + lq] = INFINITY;
+  cth_share[split * QPC + lq] = INFINITY;
 
   // MinK's fill phase stores points 0..K-1 whatever their key: a NaN there
   // changes the result in ways only the replay reproduces.
@@ -594,7 +612,8 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   int qn = 0;
 
   const int ntile = it.ntile;
-  const bool seed = G > 1 && ntile > kSeedTiles;
+  // slot of this list's c-th smallest real key, c = ceil((K+1)/G)
+  const int cslot = (KMAX - K) + (K + G) / G - 1;
   const float* pairs_b = it.pairs;
   // visit position v reads tile lbt[v] into buffer v % kTileBufs
   auto issue = [&](int v) {
@@ -628,8 +647,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     *s_abort = 0;
     for (int b = 0; b < kTileBufs; ++b) cnt[b] = 0;
     fence_proxy_async_smem();  // region A was last written by generic stores
-    // the seed merge reuses region A, so only the seed tiles go first then
-    for (int v = 0; v < (seed ? kSeedTiles : kTileBufs); ++v) {
+    for (int v = 0; v < kTileBufs; ++v) {
       if (decide(v, INFINITY)) {
         issue(v);
       } else {
@@ -697,8 +715,14 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     }
     flush_queue<L>(keys, vals, qn, tie_key, tau, qk, qv, tid);
     tau_share[split * QPC + lq] = keys[L - 1];
+    if (G > 1) {
+      float cth = keys[0];  // keys[cslot] without a dynamic register index
+#pragma unroll
+      for (int s = 1; s < L; ++s) cth = (s == cslot) ? keys[s] : cth;
+      cth_share[split * QPC + lq] = cth;
+    }
     // count this warp out of the tile (release: its reads of the buffer and
-    // its tau_share write come first)
+    // its bound writes come first)
     __syncwarp();
     int last = 0;
     if (lane == 0) {
@@ -707,76 +731,19 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
       if (last) __threadfence_block();
     }
     last = __shfl_sync(0xffffffffu, last, 0);
-    if (seed && t == kSeedTiles - 1) {
-      // All warps are done with both tile buffers once they meet here (the
-      // next copies are deferred until now): merge the G lists of every
-      // query into split 0, restart the others.
-      __syncthreads();
-      const int slot = split * QPC + lq;
-#pragma unroll
-      for (int s = 0; s < L; ++s) {
-        mk[slot * L + s] = keys[s];
-        mv[slot * L + s] = vals[s];
-      }
-      __syncthreads();
-      if (split == 0) {
-        const float next = merge_splits<G, L>(mk, mv, QPC, lq, KMAX - K, K + 1, out_k + lq * L, out_i + lq * L);
-        const float tau0 = out_k[lq * L + K];
-        if (next == tau0) tie_key = fminf(tie_key, next);
-        mf[lq] = tau0;
-      }
-      __syncthreads();
-      const float tau0 = mf[lq];
-#pragma unroll
-      for (int s = 0; s < L; ++s) {
-        const int j = s - (KMAX - K);
-        if (j >= 0) {
-          keys[s] = split == 0 ? out_k[lq * L + j] : tau0;
-          vals[s] = split == 0 ? out_i[lq * L + j] : -2;
-        }
-      }
-      tau = fminf(tau, tau0);
-      tau_share[split * QPC + lq] = keys[L - 1];
-      float tmax = -INFINITY;
-      if (warp == 0) {
-        for (int i = lane; i < QPC; i += 32) tmax = fmaxf(tmax, mf[i]);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
-      }
-      __syncthreads();  // everyone has read the merge data in region A before new copies land
-      if (tid == 0) {
-        cnt[buf] = 0;
-        fence_proxy_async_smem();
-        for (int v = kSeedTiles; v < kSeedTiles + kTileBufs; ++v) {
-          if (decide(v, tmax)) {
-            issue(v);
-          } else {
-            stop(v);
-            break;
-          }
-        }
-      }
-      continue;
-    }
-    float tm = keys[L - 1];
-#pragma unroll
-    for (int g = 0; g < G; ++g) tm = fminf(tm, tau_share[g * QPC + lq]);
-    tau = fminf(tau, tm);
+    tau = fminf(tau, query_bound<G, QPC>(tau_share, cth_share, lq));
     if (last) {
       // every warp is done with this buffer: re-arm its counter, then decide
-      // visit t + kTileBufs (deferred during the seed tiles) unless a stop
-      // was made
-      const bool deferred = seed && t < kSeedTiles - 1;
+      // visit t + kTileBufs unless a stop was made; a tile is needed while
+      // its bound is below some query's bound
       float tmax = -INFINITY;
-      if (!deferred) {
 #pragma unroll
-        for (int i = 0; i < kSearchThreads / 32; ++i) tmax = fmaxf(tmax, tau_share[i * 32 + lane]);
+      for (int i = lane; i < QPC; i += 32) tmax = fmaxf(tmax, query_bound<G, QPC>(tau_share, cth_share, i));
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
-      }
+      for (int o = 16; o > 0; o >>= 1) tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
       if (lane == 0) {
         cnt[buf] = 0;
-        if (!deferred && *s_final == 0x7fffffff && !*s_abort) {
+        if (*s_final == 0x7fffffff && !*s_abort) {
           if (decide(t + kTileBufs, tmax)) {
             fence_proxy_async_smem();
             issue(t + kTileBufs);
