@@ -394,6 +394,30 @@ __device__ __forceinline__ void geometry(T qx, T qy, T qz, const T* rec, Geo<T>&
   g.w = weight_of(g.s);
 }
 
+// A point record (16 values, 64 B in FP32 / 128 B in FP64, 16-byte
+// aligned) into registers with 128-bit loads: four (eight) load
+// instructions per entry instead of fifteen scalar ones.
+__device__ __forceinline__ void load_rec(const float* p, float (&r)[kRecLen]) {
+  const float4* v = reinterpret_cast<const float4*>(p);
+#pragma unroll
+  for (int i = 0; i < kRecLen / 4; ++i) {
+    const float4 x = __ldg(v + i);
+    r[4 * i + 0] = x.x;
+    r[4 * i + 1] = x.y;
+    r[4 * i + 2] = x.z;
+    r[4 * i + 3] = x.w;
+  }
+}
+__device__ __forceinline__ void load_rec(const double* p, double (&r)[kRecLen]) {
+  const double2* v = reinterpret_cast<const double2*>(p);
+#pragma unroll
+  for (int i = 0; i < kRecLen / 2; ++i) {
+    const double2 x = __ldg(v + i);
+    r[2 * i + 0] = x.x;
+    r[2 * i + 1] = x.y;
+  }
+}
+
 template <typename T>
 struct QueryParams {
   const T* gfo;
@@ -513,7 +537,9 @@ __device__ __forceinline__ void query_order1_scalar(const QueryParams<T>& a, con
         T c = T(0);
         if (idx >= 0 && idx < P) {
           c = sg0 * a.frowsum[pbase + idx];
-          const T* rec = recb + idx * kRecLen;
+          T rr[kRecLen];
+          load_rec(recb + idx * kRecLen, rr);
+          const T* rec = rr;
           Geo<T> geo;
           geometry(qx, qy, qz, rec, geo);
           const T w = a.w_in ? a.w_in[e] : geo.w;
@@ -620,7 +646,9 @@ __global__ void __launch_bounds__(256, 3) query_order1_kernel(QueryParams<T> a) 
         if (a.coef_out) a.coef_out[e] = c_own;
         const int64_t idx = a.idxs[e];
         if (idx >= 0 && idx < P) {
-          const T* rec = recb + idx * kRecLen;
+          T rr[kRecLen];
+          load_rec(recb + idx * kRecLen, rr);
+          const T* rec = rr;
           Geo<T> geo;
           geometry(qx, qy, qz, rec, geo);
           const T w = a.w_in ? a.w_in[e] : geo.w;
@@ -667,7 +695,9 @@ __device__ __forceinline__ void query_order2_half(const QueryParams<T>& a) {
       if (idx >= 0 && idx < P) {
         const T qx = a.q[bq * 3 + 0], qy = a.q[bq * 3 + 1], qz = a.q[bq * 3 + 2];
         const T g[3] = {a.ggq[bq * 3 + 0], a.ggq[bq * 3 + 1], a.ggq[bq * 3 + 2]};
-        const T* rec = a.rec + (b * P + idx) * kRecLen;
+        T rr[kRecLen];
+        load_rec(a.rec + (b * P + idx) * kRecLen, rr);
+        const T* rec = rr;
         Geo<T> geo;
         geometry(qx, qy, qz, rec, geo);
         const T w = a.w_in ? a.w_in[e] : geo.w;
@@ -724,7 +754,9 @@ __global__ void __launch_bounds__(256) query_order2_kernel(QueryParams<T> a) {
         const int64_t idx = a.idxs[e];
         if (idx >= 0 && idx < P) {
           row = idx * F;
-          const T* rec = a.rec + ((int64_t)b * P + idx) * kRecLen;
+          T rr[kRecLen];
+          load_rec(a.rec + ((int64_t)b * P + idx) * kRecLen, rr);
+          const T* rec = rr;
           Geo<T> geo;
           geometry(qx, qy, qz, rec, geo);
           const T w = a.w_in ? a.w_in[e] : geo.w;

@@ -138,7 +138,7 @@ int knnag_pack_points(const void* p, const void* sigma, const void* R, int B, in
   if (dtype != KNNAG_F32 && dtype != KNNAG_F64) return KNNAG_ERR_DTYPE;
   if (B < 0 || P < 0) return KNNAG_ERR_ARG;
   if ((int64_t)B * P == 0) return KNNAG_OK;
-  if (!p || !sigma || !R || !points) return KNNAG_ERR_ARG;
+  if (!p || !sigma || !R || !points || !aligned16(points)) return KNNAG_ERR_ARG;
   return launch_pack_points(p, sigma, R, B, P, dtype, points, static_cast<cudaStream_t>(stream));
 }
 
@@ -159,6 +159,7 @@ static int backward_common(BwdArgs& x, size_t workspace_bytes, void* stream) {
   if (!x.gfo || !x.q || !x.p || !x.sigma || !x.R || !x.idxs || !x.workspace) return KNNAG_ERR_ARG;
   if (x.F > 0 && !x.f) return KNNAG_ERR_ARG;
   if (x.order == 2 && !x.ggq) return KNNAG_ERR_ARG;
+  if (x.points && !aligned16(x.points)) return KNNAG_ERR_ARG;  // records are read with 16-byte loads
   if (((x.needs & KNNAG_NEED_DQ) && !x.dq) || ((x.needs & KNNAG_NEED_DP) && !x.dp) ||
       ((x.needs & KNNAG_NEED_DF) && !x.df && x.F > 0) || ((x.needs & KNNAG_NEED_DSIGMA) && !x.dsigma) ||
       ((x.needs & KNNAG_NEED_DR) && !x.dR) || ((x.needs & KNNAG_NEED_DGFO) && !x.dgfo && x.F > 0))

@@ -148,6 +148,7 @@ size_t knnag_cloudset_build_workspace_bytes(int C, const int* P) {
 
 int knnag_cloudset_init(int C, const int* P, void* cloudset, size_t cloudset_bytes, void* stream) {
   if (!cloudset || !P || C < 1) return KNNAG_ERR_ARG;
+  if ((uintptr_t)cloudset & 15u) return KNNAG_ERR_ARG;  // records and tiles are read with 16-byte loads
   CloudSetHeader h{};
   std::vector<CloudDesc> d((size_t)C);
   const size_t need = cloudset_layout(C, P, &h, d.data());
@@ -165,6 +166,7 @@ int knnag_cloudset_init(int C, const int* P, void* cloudset, size_t cloudset_byt
 int knnag_cloudset_build(const float* p, const float* sigma, const float* R, int C, const int* P, void* cloudset,
                          size_t cloudset_bytes, void* workspace, size_t workspace_bytes, void* stream) {
   if (!p || !sigma || !R || !cloudset || !workspace || !P || C < 1) return KNNAG_ERR_ARG;
+  if ((uintptr_t)cloudset & 15u) return KNNAG_ERR_ARG;  // records and tiles are read with 16-byte loads
   CloudSetHeader h{};
   const size_t need = cloudset_layout(C, P, &h, nullptr);
   if (!need) return KNNAG_ERR_TOO_LARGE;
@@ -246,6 +248,7 @@ int knnag_ragged_forward(const void* cloudset, const void* segments, const float
                          int max_cloud_points, int splits, float* f_out, float* w_out, float* dists, int64_t* idxs,
                          void* workspace, size_t workspace_bytes, void* stream) {
   if (!cloudset || !segments || !f || !f_out || !w_out || !dists || !idxs || !workspace) return KNNAG_ERR_ARG;
+  if ((uintptr_t)cloudset & 15u) return KNNAG_ERR_ARG;  // records and tiles are read with 16-byte loads
   if (cap_segments < 1 || cap_queries < 1 || cap_entries < 1 || F < 0 || max_cloud_points < 1) return KNNAG_ERR_ARG;
   if ((!q && cap_queries > 0) || !qpc_of(splits)) return KNNAG_ERR_ARG;
   if (max_k < 1 || max_k > max_cloud_points) return KNNAG_ERR_K;
@@ -263,6 +266,7 @@ int knnag_ragged_grad_q(const void* cloudset, const void* segments, const float*
                         long long cap_queries, long long cap_entries, int max_k, int max_cloud_points, float* dq,
                         void* workspace, size_t workspace_bytes, void* stream) {
   if (!cloudset || !segments || !q || !f || !idxs || !dq || !workspace) return KNNAG_ERR_ARG;
+  if ((uintptr_t)cloudset & 15u) return KNNAG_ERR_ARG;  // records and tiles are read with 16-byte loads
   if (cap_segments < 1 || cap_queries < 1 || cap_entries < 1 || F < 0 || max_cloud_points < 1) return KNNAG_ERR_ARG;
   if (max_k < 1 || max_k > max_cloud_points) return KNNAG_ERR_K;
   if (cap_queries > kI32Max / 2 || cap_segments > (1 << 24)) return KNNAG_ERR_TOO_LARGE;

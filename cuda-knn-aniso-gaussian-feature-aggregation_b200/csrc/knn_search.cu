@@ -13,6 +13,17 @@ namespace knnag {
 
 // ------------------------------------------------------------------ packing
 
+// A record row (64 B / 128 B, 16-byte aligned) with 128-bit stores.
+__device__ __forceinline__ void store_rec(float* dst, const float (&v)[kRecLen]) {
+#pragma unroll
+  for (int m = 0; m < kRecLen; m += 4)
+    *reinterpret_cast<float4*>(dst + m) = make_float4(v[m], v[m + 1], v[m + 2], v[m + 3]);
+}
+__device__ __forceinline__ void store_rec(double* dst, const double (&v)[kRecLen]) {
+#pragma unroll
+  for (int m = 0; m < kRecLen; m += 2) *reinterpret_cast<double2*>(dst + m) = make_double2(v[m], v[m + 1]);
+}
+
 // rec[(b*P+i)*16 + field]: -p, R (row-major), sigma, pad.
 template <typename T>
 __global__ void pack_points_kernel(const T* __restrict__ p, const T* __restrict__ sigma,
@@ -31,8 +42,7 @@ __global__ void pack_points_kernel(const T* __restrict__ p, const T* __restrict_
     v[kS1] = sigma[i * 3 + 1];
     v[kS2] = sigma[i * 3 + 2];
     v[kRecPad] = T(0);
-#pragma unroll
-    for (int m = 0; m < kRecLen; ++m) rec[i * kRecLen + m] = v[m];
+    store_rec(rec + i * kRecLen, v);
   }
 }
 

@@ -123,6 +123,7 @@ __global__ void __launch_bounds__(512) point_bounds_kernel(const float* __restri
   GroupRange r;
   group_range(m, b, r);
   float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+#pragma unroll 4
   for (int i = tid; i < r.n; i += blockDim.x) {
     const float* rr = rec + (r.start + i) * kRecLen;
 #pragma unroll

@@ -156,7 +156,8 @@ int knnag_forward_isotropic(const void* q, const void* p, const void* f, const v
 
 /* ---------------------------------------------------------- adjoint index */
 
-/* Bytes of the packed per-point records (16 values of dtype per point). */
+/* Bytes of the packed per-point records (16 values of dtype per point).  A
+ * points buffer must be 16-byte aligned (KNNAG_ERR_ARG otherwise). */
 size_t knnag_points_bytes(int B, int P, int dtype);
 
 /* Pack p, sigma and R into per-point records (what knnag_forward also writes). */
@@ -231,7 +232,8 @@ int knnag_read_device_status(void* workspace, void* stream);
  *
  * Cloud set: C clouds with P[c] points, their p [sum P, 3], sigma
  * [sum P, 3], R [sum P, 3, 3] and features f [sum P, F] concatenated in
- * cloud order.  The cloud-set buffer (device, 256-byte aligned,
+ * cloud order.  The cloud-set buffer (device, 256-byte aligned -- calls
+ * reject one that is not 16-byte aligned with KNNAG_ERR_ARG --
  * knnag_cloudset_bytes) holds the packed records and the search index of
  * every cloud and describes itself; kernels need only its address. */
 
@@ -246,7 +248,7 @@ size_t knnag_cloudset_build_workspace_bytes(int C, const int* P);
  * buffer and size list. */
 int knnag_cloudset_init(int C, const int* P, void* cloudset, size_t cloudset_bytes, void* stream);
 
-/* Pack the clouds' records and build their search index (Morton order, sorted
+/* Pack the clouds' records and build their search index (Hilbert order, sorted
  * tiles, tile key bounds) from p, sigma, R.  Kernels only (capturable); call
  * again whenever the geometry changes.  The buffer must have been set up by
  * knnag_cloudset_init with the same C and P. */

@@ -62,6 +62,22 @@ def test_validation_before_device_work():
     assert lib.knnag_forward(*args) == 0  # B = 0: nothing to do
 
 
+def test_misaligned_record_buffers_rejected():
+    """Packed records and cloud sets are read with 16-byte loads and bulk
+    copies: a buffer that is not 16-byte aligned is refused before any
+    device work."""
+    from cuda_knn_aggregate import capi
+
+    lib = capi.lib()
+    V = ctypes.c_void_p
+    one, odd = V(16), V(24)  # never dereferenced
+    assert lib.knnag_pack_points(one, one, one, 1, 4, capi.F32, odd, None) == 1
+    P = (ctypes.c_int * 1)(100)
+    nb = lib.knnag_cloudset_bytes(1, P)
+    assert lib.knnag_cloudset_init(1, P, odd, nb, None) == 1
+    assert lib.knnag_cloudset_init(1, P, None, nb, None) == 1
+
+
 def test_python_api_rejects_cpu_tensors():
     from cuda_knn_aggregate import knn_aggregate_aniso
 
