@@ -76,9 +76,35 @@ __device__ __forceinline__ T key_from_offset(T x, T y, T z, const T* r, T s0, T 
   return quad_form(j, k, l, s0, s1, s2);
 }
 
-// Key of query (qx,qy,qz) against a per-point record.
+// A point record (16 values, 64 B in FP32 / 128 B in FP64, 16-byte
+// aligned) into registers with 128-bit loads: four (eight) load
+// instructions per record instead of fifteen scalar ones.
+__device__ __forceinline__ void load_rec(const float* p, float (&r)[kRecLen]) {
+  const float4* v = reinterpret_cast<const float4*>(p);
+#pragma unroll
+  for (int i = 0; i < kRecLen / 4; ++i) {
+    const float4 x = __ldg(v + i);
+    r[4 * i + 0] = x.x;
+    r[4 * i + 1] = x.y;
+    r[4 * i + 2] = x.z;
+    r[4 * i + 3] = x.w;
+  }
+}
+__device__ __forceinline__ void load_rec(const double* p, double (&r)[kRecLen]) {
+  const double2* v = reinterpret_cast<const double2*>(p);
+#pragma unroll
+  for (int i = 0; i < kRecLen / 2; ++i) {
+    const double2 x = __ldg(v + i);
+    r[2 * i + 0] = x.x;
+    r[2 * i + 1] = x.y;
+  }
+}
+
+// Key of query (qx,qy,qz) against a per-point record in global memory.
 template <typename T>
-__device__ __forceinline__ T key_rec(T qx, T qy, T qz, const T* rec) {
+__device__ __forceinline__ T key_rec(T qx, T qy, T qz, const T* rec_g) {
+  T rec[kRecLen];
+  load_rec(rec_g, rec);
   T x = add_rn(qx, rec[kNPX]);
   T y = add_rn(qy, rec[kNPY]);
   T z = add_rn(qz, rec[kNPZ]);

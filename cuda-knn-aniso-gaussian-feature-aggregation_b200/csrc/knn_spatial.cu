@@ -251,8 +251,7 @@ __global__ void __launch_bounds__(kTilePoints) tile_info_kernel(const float* __r
     const int idx = perm[g.p0 + pos];
     const float* r = rec + (g.p0 + idx) * kRecLen;
     float v[kRecLen];
-#pragma unroll
-    for (int m = 0; m < kRecLen; ++m) v[m] = r[m];
+    load_rec(r, v);
 #pragma unroll
     for (int m = 0; m < kRecLen; ++m) slot[2 * m] = m == kRecPad ? __int_as_float(idx) : v[m];
 #pragma unroll
