@@ -850,14 +850,28 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
       const int l = x / C4, c = x - l * C4;
       if (out_f[l]) continue;
       float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-      for (int k = 0; k < K; ++k) {
-        const int idx = out_i[l * L + k];
-        const float w = out_w[l * L + k];
-        const float4 v = __ldg(reinterpret_cast<const float4*>(fb + (int64_t)idx * F) + c);
-        acc.x = __fmaf_rn(v.x, w, acc.x);
-        acc.y = __fmaf_rn(v.y, w, acc.y);
-        acc.z = __fmaf_rn(v.z, w, acc.z);
-        acc.w = __fmaf_rn(v.w, w, acc.w);
+      // KMAX <= 16: eight rows in flight, summed in k order (the KMAX = 32
+      // kernels, at 128 registers, run the plain loop: measured faster there)
+      constexpr int RB = KMAX <= 16 ? 8 : 1;
+      for (int k0 = 0; k0 < K; k0 += RB) {
+        float4 v[RB];
+        float w[RB];
+#pragma unroll
+        for (int j = 0; j < RB; ++j) {
+          const bool in = k0 + j < K;
+          const int idx = in ? out_i[l * L + k0 + j] : 0;
+          w[j] = in ? out_w[l * L + k0 + j] : 0.f;
+          v[j] = in ? __ldg(reinterpret_cast<const float4*>(fb + (int64_t)idx * F) + c) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int j = 0; j < RB; ++j) {
+          if (k0 + j < K) {
+            acc.x = __fmaf_rn(v[j].x, w[j], acc.x);
+            acc.y = __fmaf_rn(v[j].y, w[j], acc.y);
+            acc.z = __fmaf_rn(v[j].z, w[j], acc.z);
+            acc.w = __fmaf_rn(v[j].w, w[j], acc.w);
+          }
+        }
       }
       reinterpret_cast<float4*>(it.f_out + (int64_t)qorig[l] * F)[c] = acc;
     }
