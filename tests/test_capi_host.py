@@ -100,3 +100,48 @@ def test_workload_generators():
     n = R[..., :, 2]
     assert torch.allclose((p / p.norm(dim=-1, keepdim=True) * n).sum(-1), torch.ones(1, 2000), atol=1e-5)
     assert torch.allclose(sigma[0, 0], torch.tensor([0.02, 0.02, 0.005]))
+
+
+def _header_prototypes():
+    """{name: (return class, [parameter classes])} parsed from the header,
+    classes being 'ptr', 'int', 'size', 'i64' or 'void'."""
+    import re
+    from cuda_knn_aggregate import capi
+
+    text = re.sub(r"/\*.*?\*/", " ", open(capi.HEADER).read(), flags=re.S)
+    protos = {}
+    for m in re.finditer(r"(const\s+char\s*\*|int|size_t|void|long\s+long)\s+(knnag_\w+)\s*\(([^)]*)\)\s*;", text):
+        ret, name, params = m.group(1), m.group(2), m.group(3)
+
+        def cls(decl):
+            decl = decl.strip()
+            if "*" in decl:
+                return "ptr"
+            if decl.startswith("size_t"):
+                return "size"
+            if decl.startswith("long long") or decl.startswith("int64_t"):
+                return "i64"
+            if decl.startswith("int"):
+                return "int"
+            return decl
+
+        args = [] if params.strip() in ("", "void") else [cls(p) for p in params.split(",")]
+        protos[name] = (cls(ret) if ret != "void" else "void", args)
+    return protos
+
+
+def test_ctypes_signatures_match_header():
+    """Every signature the ctypes binding declares has the header's
+    parameter count and kinds (pointer, int, size_t, 64-bit int) and return
+    kind, so a change of the C ABI cannot leave the binding behind."""
+    from cuda_knn_aggregate import capi
+
+    kind = {ctypes.c_void_p: "ptr", ctypes.c_char_p: "ptr", ctypes.c_int: "int", ctypes.c_size_t: "size",
+            ctypes.c_longlong: "i64", None: "void"}
+    protos = _header_prototypes()
+    assert len(protos) >= len(capi._SIGS)
+    for name, (args, res) in capi._SIGS.items():
+        assert name in protos, name
+        ret, hargs = protos[name]
+        assert [kind[a] for a in args] == hargs, name
+        assert kind[res] == ret, name
