@@ -136,10 +136,24 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_inputs(rank, device):
-    from cuda_knn_aggregate import workloads as W
+def workloads_module():
+    """cuda_knn_aggregate/workloads.py loaded by file path: it needs only
+    torch, and importing it through the package would load the package's
+    CUDA extension (which the reference arm must not touch)."""
+    import importlib.util
 
-    shape, t = W.make(WORKLOAD["name"], seed=1001 + 7919 * rank)
+    name = "knnag_bench_workloads"
+    if name not in sys.modules:
+        path = os.path.join(PKG_DIR, "cuda_knn_aggregate", "workloads.py")
+        spec = importlib.util.spec_from_file_location(name, path)
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
+def make_inputs(rank, device):
+    shape, t = workloads_module().make(WORKLOAD["name"], seed=1001 + 7919 * rank)
     return shape, t
 
 
@@ -191,59 +205,57 @@ def cpu_baseline_block(seconds=12.0, q_per_batch=2048):
 
 # ------------------------------------------------------------ reference ext
 
+def ref_ext():
+    """The reference extension (compiled from its own sources) with the
+    reference package's autograd wiring: (module, op) or (None, reason)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_ext as RX
+
+    mod, why = RX.load()
+    if mod is None:
+        return None, why
+    return mod, RX.op(mod)
+
+
 def load_reference_ext():
-    import importlib.util
-
-    path = os.path.join(ROOT, "oracle", "_ref", "knn_ref_C.so")
-    if not os.path.exists(path):
-        return None, "reference extension not built (python oracle/build_ref.py needs the reference sources)"
-    spec = importlib.util.spec_from_file_location("knn_ref_C", path)
-    mod = importlib.util.module_from_spec(spec)
-    spec.loader.exec_module(mod)
-    return mod, None
+    mod, why = ref_ext()
+    return (mod, None) if mod is not None else (None, why)
 
 
-def reference_ext_op(ref):
-    """The reference package's autograd wiring (cuda_knn_aggregate/__init__.py:
-    64-117 and 216-289 of the reference) around the reference's own ops."""
-
-    class RefBackward(torch.autograd.Function):
-        @staticmethod
-        def forward(ctx, gfo, gwo, q, p, f, sigma, R, w_out, idxs):
-            outs = ref.knn_aggregate_aniso_backward(gfo, gwo, q, p, f, sigma, R, w_out, idxs)
-            ctx.save_for_backward(gfo, gwo, q, p, f, sigma, R, w_out, idxs)
-            return tuple(outs)
-
-        @staticmethod
-        def backward(ctx, ggq, ggp, ggf, ggs, ggR):
-            gfo, gwo, q, p, f, sigma, R, w_out, idxs = ctx.saved_tensors
-            o = ref.knn_aggregate_aniso_backward_2nd(ggq.contiguous(), gfo.contiguous(), gwo.contiguous(), q, p, f,
-                                                     sigma, R, w_out, idxs)
-            return o[0], None, o[1], o[2], o[3], o[4], o[5], None, None
-
-    class RefAgg(torch.autograd.Function):
-        @staticmethod
-        def forward(ctx, q, p, f, sigma, R, K):
-            f_out, w_out, dists, idxs = ref.knn_aggregate_aniso_forward(q, p, f, sigma, R, K)
-            ctx.save_for_backward(q, p, f, sigma, R, w_out, idxs)
-            return f_out, w_out, dists, idxs
-
-        @staticmethod
-        def backward(ctx, gfo, gwo, gd, gi):
-            q, p, f, sigma, R, w_out, idxs = ctx.saved_tensors
-            g = RefBackward.apply(gfo.contiguous(), gwo.contiguous(), q, p, f, sigma, R, w_out, idxs)
-            return (*g, None)
-
-    return RefAgg.apply
+def e2e_times(op, host, K, device, steps, warmup, flush):
+    """Per-step ms of the Eikonal step through `op` from pinned host inputs:
+    H2D copies, the step, and the D2H read of the loss inside each timed
+    region (CUDA events on the current stream)."""
+    loss_h = torch.empty((), dtype=torch.float32).pin_memory()
+    out = []
+    for i in range(warmup + steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dev_in = [x.to(device, non_blocking=True).requires_grad_(True) for x in host]
+        f_out = op(*dev_in, K)[0]
+        (gq,) = torch.autograd.grad(f_out.sum(), dev_in[0], create_graph=True)
+        loss = ((gq.norm(dim=-1) - 1.0) ** 2).mean()
+        loss.backward()
+        loss_h.copy_(loss.detach(), non_blocking=True)
+        e1.record()
+        e1.synchronize()
+        if i >= warmup:
+            out.append(e0.elapsed_time(e1))
+    return out, loss_h.element_size()
 
 
-def time_reference_ext(device, steps, warmup):
-    ref, why = load_reference_ext()
-    if ref is None:
-        return {"unavailable": why}
+def time_reference_ext(device, steps, warmup, host=None):
+    """The reference extension's Eikonal step on this GPU: device-resident
+    inputs (eager; it cannot be graph-captured: it launches on the legacy
+    default stream), and, when `host` inputs are given, end to end from
+    pinned host buffers as our e2e figure is taken."""
+    mod, op = ref_ext()
+    if mod is None:
+        return {"unavailable": op}
     shape, t = make_inputs(0, device)
     ins = [x.to(device).requires_grad_(True) for x in t]
-    step = eikonal_step_fn(reference_ext_op(ref), ins, shape.K)
+    step = eikonal_step_fn(op, ins, shape.K)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
     for _ in range(warmup):
         step()
@@ -258,8 +270,12 @@ def time_reference_ext(device, steps, warmup):
         e1.synchronize()
         times.append(e0.elapsed_time(e1))
     ms = statistics.mean(times)
-    return {"value": shape.B * shape.Q / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "steps": steps,
-            "how": "reference extension compiled from its own sources (sm_100), reference autograd wiring, eager"}
+    out = {"value": shape.B * shape.Q / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "steps": steps,
+           "how": "reference extension compiled from its own sources (sm_100), reference autograd wiring, eager"}
+    if host is not None:
+        e2e, _ = e2e_times(op, host, shape.K, device, steps, 1, flush)
+        out["e2e_ms_per_step"] = statistics.mean(e2e)
+    return out
 
 
 # ------------------------------------------------------------ ragged / served
@@ -432,11 +448,11 @@ def sphere_block(device, steps=5, ref_steps=1, with_reference=True, sample=256):
            "pairs": shape.B * shape.Q * shape.P, "idxs_dists_bit_exact_vs_oracle_sample": match,
            "oracle_sample_queries": sample}
     del g
-    ref, why = load_reference_ext() if with_reference else (None, "skipped (--no-reference-ext)")
+    ref, rop = ref_ext() if with_reference else (None, "skipped (--no-reference-ext)")
     if ref is None:
-        out["reference_ext"] = {"unavailable": why}
+        out["reference_ext"] = {"unavailable": rop}
     else:
-        rstep = eikonal_step_fn(reference_ext_op(ref), ins, shape.K)
+        rstep = eikonal_step_fn(rop, ins, shape.K)
         rstep()
         torch.cuda.synchronize()
         tr = []
@@ -559,16 +575,20 @@ def fp32_peak_tflops(device):
     return best
 
 
-def read_profile_traffic():
-    """Per-launch DRAM bytes of the search kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "search_f32_table.md")
-    try:
-        for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":", 1)[1])
-    except OSError:
-        pass
-    return None
+# DRAM bytes (read + write) of one search_f32_kernel<16,4> launch at the table
+# workload, from the ncu capture summarised in profiles/search_f32_table.md
+# (dram__bytes_read.sum + dram__bytes_write.sum of one launch); update it
+# with that summary whenever the search kernel changes.
+SEARCH_TRAFFIC_BYTES = 3588864
+SEARCH_TRAFFIC_SOURCE = "ncu capture of one search_f32_kernel<16,4> launch (profiles/search_f32_table.md)"
+
+CONFIG = {"workload": "table: B=2 Q=12288 P=4096 F=64 K=16, fwd + dq(create_graph) + Eikonal backward",
+          "l2": "flushed between timed steps (256 MiB write)"}
+
+
+def compact(block, keys):
+    """The named figures of a workload block (the full block: --workload NAME)."""
+    return {k: block[k] for k in keys if k in block}
 
 
 def run_ours(args):
@@ -647,23 +667,8 @@ def run_ours(args):
     # end to end through the public API: host inputs in pinned memory,
     # H2D copies + step + D2H of the loss inside the timed region
     host = [x.detach().cpu().pin_memory() for x in t]
-    loss_h = torch.empty((), dtype=torch.float32).pin_memory()
     h2d = sum(x.numel() * x.element_size() for x in host)
-    e2e = []
-    for i in range(args.warmup + args.steps):
-        flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        dev_in = [x.to(device, non_blocking=True).requires_grad_(True) for x in host]
-        f_out = knn_aggregate_aniso(*dev_in, K)[0]
-        (gq,) = torch.autograd.grad(f_out.sum(), dev_in[0], create_graph=True)
-        loss = ((gq.norm(dim=-1) - 1.0) ** 2).mean()
-        loss.backward()
-        loss_h.copy_(loss.detach(), non_blocking=True)
-        e1.record()
-        e1.synchronize()
-        if i >= args.warmup:
-            e2e.append(e0.elapsed_time(e1))
+    e2e, d2h = e2e_times(knn_aggregate_aniso, host, K, device, args.steps, args.warmup, flush)
     e2e_ms = max_over_ranks(statistics.mean(e2e), ws, device)
 
     if rank != 0:
@@ -678,16 +683,15 @@ def run_ours(args):
                 "unit": "TFLOP/s", "frac": achieved / peak,
                 "peak_source": "measured: FFMA-bound probe kernel in bench.py (MEASURED_PEAKS.json has no FP32 figure)",
                 "algorithmic": f"{FLOP_PER_PAIR} FLOP x {pairs} (q,p) pairs per launch",
-                "launch_ms": search_s * 1e3, "traffic": read_profile_traffic()}
+                "launch_ms": search_s * 1e3, "traffic": SEARCH_TRAFFIC_BYTES, "traffic_source": SEARCH_TRAFFIC_SOURCE}
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded uniform cube, README timing-table shape)",
-        "config": {"workload": "table: B=2 Q=12288 P=4096 F=64 K=16, fwd + dq(create_graph) + Eikonal backward",
-                   "queries_per_gpu": units, "parallelism": f"independent batches per rank x{ws}",
-                   "l2": "flushed between timed steps (256 MiB write)", "execution": "CUDA graph replay"},
+        "config": {**CONFIG, "queries_per_gpu": units, "parallelism": f"independent batches per rank x{ws}",
+                   "execution": "CUDA graph replay"},
         "e2e": {"value": ws * units / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms,
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": loss_h.element_size(),
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "how": "public API knn_aggregate_aniso + autograd, eager, pinned host inputs"},
         "roofline": roofline,
         "clocks": clocks,
@@ -695,21 +699,36 @@ def run_ours(args):
         "gpu_launches_per_step": launches_per_step,
         "eager_ms_per_step": statistics.mean(eager),
     }
-    if ws == 1 and not args.no_reference_ext:
-        out["reference_ext"] = time_reference_ext(device, min(args.steps, 10), 2)
-        if "ms_per_step" in out["reference_ext"]:
-            out["reference_ext"]["speedup_value"] = out["reference_ext"]["ms_per_step"] / ms
-            out["reference_ext"]["speedup_e2e"] = out["reference_ext"]["ms_per_step"] / e2e_ms
-    if ws == 1 and not args.no_ragged:
-        out["ragged"] = ragged_block(device, with_reference=not args.no_reference_ext)
-    if ws == 1 and not args.no_sphere:
-        out["sphere"] = sphere_block(device, with_reference=not args.no_reference_ext)
-    if ws == 1 and not args.no_served:
-        out["served"] = served_block(device)
-        out["served_p50_ms"] = out["served"].get("p50_ms")
-        out["served_p99_ms"] = out["served"].get("p99_ms")
     if ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_block()
+    if ws == 1 and not args.no_ragged:
+        rb = ragged_block(device, with_reference=not args.no_reference_ext)
+        out["ragged"] = compact(rb, ("clouds", "queries", "ms_per_step", "value", "speedup_vs_loop",
+                                     "f_out_identical_to_loop", "speedup_vs_reference_loop"))
+    if ws == 1 and not args.no_sphere:
+        sb = sphere_block(device, with_reference=not args.no_reference_ext)
+        out["sphere"] = compact(sb, ("ms_per_step", "value", "idxs_dists_bit_exact_vs_oracle_sample",
+                                     "speedup_vs_reference"))
+        if "reference_ext" in sb and "ms_per_step" in sb["reference_ext"]:
+            out["sphere"]["reference_ext_ms_per_step"] = sb["reference_ext"]["ms_per_step"]
+    if ws == 1 and not args.no_served:
+        sv = served_block(device)
+        out["served"] = {"saturated_qps": sv["saturated"]["throughput_qps"], "at_load": sv.get("at_load"),
+                         "speedup_vs_per_request_loop": sv.get("speedup_vs_loop")}
+        out["served_p50_ms"] = sv.get("p50_ms")
+        out["served_p99_ms"] = sv.get("p99_ms")
+    # the north-star comparator last, so it is in any tail of the line: the
+    # reference extension's step on this GPU, device-resident and end to end
+    if ws == 1 and not args.no_reference_ext:
+        r = time_reference_ext(device, min(args.steps, 10), 2, host=host)
+        if "ms_per_step" in r:
+            out["reference_ext_ms_per_step"] = r["ms_per_step"]
+            out["reference_ext_e2e_ms_per_step"] = r.get("e2e_ms_per_step")
+            out["speedup_vs_reference_ext"] = r["ms_per_step"] / ms
+            if r.get("e2e_ms_per_step"):
+                out["e2e_speedup_vs_reference_ext"] = r["e2e_ms_per_step"] / e2e_ms
+        else:
+            out["reference_ext"] = r
     print(json.dumps(out), flush=True)
     barrier(ws)
     return out
@@ -729,9 +748,9 @@ def run_reference_cpu(args):
     out = {"metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "impl": "reference", "data": "synthetic (seeded uniform cube, README timing-table shape)",
-           "config": {"workload": "table: B=2 Q=12288 P=4096 F=64 K=16 (bounded query sample per step)",
-                      "note": "the reference ships no CPU implementation; its op is timed as the plain-PyTorch "
-                              "formulation on all host threads"},
+           "config": {**CONFIG, "queries_per_gpu": 24576, "parallelism": "host cores",
+                      "execution": "plain-PyTorch CPU formulation (the reference ships no CPU implementation), "
+                                   "timed on a bounded query sample per step (see cpu_baseline.sample)"},
            "cpu_baseline": block,
            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)

@@ -21,6 +21,12 @@ void note_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); 
 static std::atomic<int> g_search_splits{0};
 int search_splits_setting() { return g_search_splits.load(std::memory_order_relaxed); }
 
+static std::atomic<int> g_stall_visit{-1}, g_wait_spins{kWaitSpinsDefault};
+void apply_search_debug(SearchParams& sp) {
+  sp.stall_visit = g_stall_visit.load(std::memory_order_relaxed);
+  sp.wait_spins = g_wait_spins.load(std::memory_order_relaxed);
+}
+
 // Record a profiling event on `st`: as an external event node while the
 // stream is being captured into a graph, as a plain record otherwise.  A
 // failed record is cleared so it cannot be mistaken for a launch error.
@@ -335,6 +341,13 @@ int knnag_set_search_splits(int splits) {
 }
 
 int knnag_get_search_splits(void) { return g_search_splits.load(std::memory_order_relaxed); }
+
+int knnag_debug_set_search_stall(int visit, int wait_spins) {
+  if (visit < -1 || wait_spins < 0) return KNNAG_ERR_ARG;
+  g_stall_visit.store(visit, std::memory_order_relaxed);
+  g_wait_spins.store(wait_spins > 0 ? wait_spins : kWaitSpinsDefault, std::memory_order_relaxed);
+  return KNNAG_OK;
+}
 
 int knnag_fp32_peak_probe(float* out, int blocks, int iters, void* stream) {
   if (!out || blocks < 1 || iters < 1) return KNNAG_ERR_ARG;

@@ -183,12 +183,16 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Wait for phase `parity` of `bar` to complete, giving up after roughly a
-// second; returns false on timeout (the caller latches the error and leaves).
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+// Default spin budget of mbar_wait_bounded: about a second of 256 ns sleeps.
+constexpr int kWaitSpinsDefault = 1 << 22;
+
+// Wait for phase `parity` of `bar` to complete, giving up after `spins`
+// sleeps of 256 ns (after 256 hardware-suspended tries); returns false on
+// timeout (the caller latches the error and leaves).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int spins = kWaitSpinsDefault) {
   for (int spin = 0; spin < 256; ++spin)
     if (mbar_try_wait(bar, parity)) return true;
-  for (int spin = 0; spin < (1 << 22); ++spin) {
+  for (int spin = 0; spin < spins; ++spin) {
     if (mbar_test_wait(bar, parity)) return true;
     __nanosleep(256);
   }

@@ -62,6 +62,12 @@ struct SearchParams {
   const char* cs;
   const void* segs;
   int* item_counter;
+  // Test hook of the timeout path (knnag_debug_set_search_stall): the tile
+  // copy of visit `stall_visit` is armed on its mbarrier but never issued,
+  // so the waits on it run out after `wait_spins` sleeps; -1 (no stall)
+  // and the default budget otherwise.
+  int stall_visit;
+  int wait_spins;
 };
 
 // Search CTA: 4 warps; G warps split the points of one 32-query group.
@@ -163,6 +169,10 @@ AdjLayout adj_layout(int B, int Q, int P, int K);
 // Process-wide split count of the uniform search (0: automatic), set by
 // knnag_set_search_splits (defined in knn_capi.cu).
 int search_splits_setting();
+// Process-wide test hook of the search's bounded waits, set by
+// knnag_debug_set_search_stall (defined in knn_capi.cu): writes the
+// stall_visit / wait_spins fields of a SearchParams.
+void apply_search_debug(SearchParams& sp);
 
 // Instrumentation shared by the .cu files (defined in knn_capi.cu).
 void note_launches(int n);

@@ -17,6 +17,12 @@
 // array: the forward clears what must start at zero (status word and flag
 // count) at the start of every call, and two calls that overlap on the GPU
 // (different streams, or different threads without ordering) race on it.
+// Errors latched on the device (a bounded wait that gave up, an internal
+// index out of range) land in the array's first word, which
+// knnag_noalloc_read_device_status copies back and clears; the next
+// forward call clears it too, so it must be read before that call.  The
+// cached address assumes the device's primary context lives as long as the
+// process (a cudaDeviceReset would leave it stale).
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -78,4 +84,11 @@ extern "C" int knnag_forward_noalloc(const void* q, const void* p, const void* f
   if (!scratch) return KNNAG_ERR_CUDA;
   return forward_impl(q, p, f, sigma, R, B, Q, P, F, K, dtype, f_out, w_out, dists, idxs, nullptr, scratch,
                       static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int knnag_noalloc_read_device_status(void* stream) {
+  void* scratch = noalloc_scratch_on_current_device();
+  if (!scratch) return KNNAG_ERR_CUDA;
+  // the forward's status word is the first word of its layout
+  return knnag_read_device_status(scratch, stream);
 }

@@ -629,6 +629,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   auto issue = [&](int v) {
     const int buf = v % kTileBufs;
     mbar_arrive_expect_tx(&full[buf], kTileBytes);
+    if (v == a.stall_visit) return;  // test hook: this phase never completes
     bulk_copy_g2s(regA + buf * kTileBytes, pairs_b + (int64_t)lbt[v] * PPT * kPairFloats, kTileBytes, &full[buf]);
   };
   // Issue position v unless its bound exceeds every threshold (the order is
@@ -679,7 +680,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   int t = 0;
   for (;; ++t) {
     const int buf = t % kTileBufs;
-    const bool ok = mbar_wait_bounded(&full[buf], (uses[buf] + t / kTileBufs) & 1);
+    const bool ok = mbar_wait_bounded(&full[buf], (uses[buf] + t / kTileBufs) & 1, a.wait_spins);
     if (!ok) {
       if (lane == 0) {
         atomicOr(a.status, kStatusWaitTimeout);
@@ -772,7 +773,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     if (tid == 0) {
       // best effort: let the copies of the last issued visits land
       for (int v = *s_nvisit - kTileBufs; v < *s_nvisit; ++v)
-        if (v >= 0) mbar_wait_bounded(&full[v % kTileBufs], (uses[v % kTileBufs] + v / kTileBufs) & 1);
+        if (v >= 0) mbar_wait_bounded(&full[v % kTileBufs], (uses[v % kTileBufs] + v / kTileBufs) & 1, a.wait_spins);
     }
     return false;
   }
@@ -1216,6 +1217,7 @@ int forward_impl(const void* q, const void* p, const void* f, const void* sigma,
   sp.status = status;
   sp.flag_count = flag_count;
   sp.flag_list = flag_list;
+  apply_search_debug(sp);
   const int G = choose_splits(B, Q, dev);
   if (K <= 8)
     rc = launch_search_k<8>(sp, G, st);
@@ -1289,6 +1291,7 @@ int ragged_forward_impl(const char* cs, const void* segs, const float* q, const 
   sp.cs = cs;
   sp.segs = segs;
   sp.item_counter = item_counter;
+  apply_search_debug(sp);
   const int64_t cap_items = cap_q / qpc + cap_segs;
   if (ks <= 8)
     rc = launch_search_ragged_k<8>(sp, G, cap_items, st);

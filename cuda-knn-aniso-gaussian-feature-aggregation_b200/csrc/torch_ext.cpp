@@ -12,6 +12,7 @@
 #include <c10/cuda/CUDAGuard.h>
 #include <torch/extension.h>
 
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -27,6 +28,24 @@ namespace {
 
 void check_status(int rc, const char* what) {
   TORCH_CHECK(rc == KNNAG_OK, what, " failed: ", knnag_status_string(rc));
+}
+
+// Opt-in check of the errors the kernels latch on the device (a bounded
+// wait that gave up, an internal index out of range): with the environment
+// variable KNNAG_CHECK_DEVICE_STATUS set to a value other than "0", every op
+// reads its workspace's status word after its launches (which synchronises
+// the stream, so such a process cannot capture the ops into a CUDA graph)
+// and raises if an error was latched.  Off by default: the ops then neither
+// synchronise nor report device-latched errors.
+bool device_status_checks() {
+  const char* e = std::getenv("KNNAG_CHECK_DEVICE_STATUS");
+  return e && e[0] && !(e[0] == '0' && e[1] == 0);
+}
+
+void check_device_status(const torch::Tensor& ws, void* stream, const char* what) {
+  if (!device_status_checks()) return;
+  TORCH_CHECK(knnag_read_device_status(ws.data_ptr(), stream) == KNNAG_OK, what,
+              ": an error was latched on the device (", knnag_status_string(KNNAG_ERR_DEVICE), ")");
 }
 
 int dtype_code(const torch::Tensor& t) {
@@ -97,6 +116,7 @@ std::vector<torch::Tensor> forward_impl(const torch::Tensor& q, const torch::Ten
                                idxs.data_ptr<int64_t>(), want_points ? points.data_ptr() : nullptr, ws.data_ptr(),
                                ws_bytes, stream_of(q));
   check_status(rc, "knn_aggregate_aniso_forward");
+  check_device_status(ws, stream_of(q), "knn_aggregate_aniso_forward");
   if (want_points) return {f_out, w_out, dists, idxs, points};
   return {f_out, w_out, dists, idxs};
 }
@@ -161,6 +181,7 @@ std::vector<torch::Tensor> backward_impl(int order, const c10::optional<torch::T
                         (int)needs, ptr_or_null(points), ptr_or_null(adjacency), P_(dq), P_(dp), P_(df), P_(ds),
                         P_(dR), P_(cf), ws.data_ptr(), ws_bytes, stream_of(q));
     check_status(rc, "knn_aggregate_aniso_backward");
+    check_device_status(ws, stream_of(q), "knn_aggregate_aniso_backward");
     return {dq, dp, df, ds, dR, cf};
   }
   rc = knnag_backward_2nd(ggq->data_ptr(), gfo.data_ptr(), nullptr, q.data_ptr(), p.data_ptr(), f.data_ptr(),
@@ -169,6 +190,7 @@ std::vector<torch::Tensor> backward_impl(int order, const c10::optional<torch::T
                           ptr_or_null(coef), P_(dgfo), P_(dq), P_(dp), P_(df), P_(ds), P_(dR), ws.data_ptr(),
                           ws_bytes, stream_of(q));
   check_status(rc, "knn_aggregate_aniso_backward_2nd");
+  check_device_status(ws, stream_of(q), "knn_aggregate_aniso_backward_2nd");
   return {dgfo, dq, dp, df, ds, dR};
 }
 

@@ -99,65 +99,76 @@ def _mask(flags):
     return m
 
 
-class KNNAnisotropicAggregate:
+class KNNAnisotropicAggregate(torch.autograd.Function):
     """Fused kNN search and aggregation (reference
     ``cuda_knn_aggregate/__init__.py:64-117``):
     ``KNNAnisotropicAggregate.apply(q, p, f, sigma, R, K)`` returns
     ``(f_out, w_out, dists, idxs)``.
 
-    The autograd nodes are C++ Functions of the extension: their backward
-    asks the running graph task which input gradients are used, so e.g.
+    A ``torch.autograd.Function`` with the reference's ``forward`` /
+    ``backward`` and saved-tensor list ``(q, p, f, sigma, R, w_out, idxs)``,
+    so subclasses written against the reference (a new ``forward`` reusing
+    this ``backward``, as its lookup and precomputed variants do) work
+    unchanged.  ``apply`` on this class itself runs the extension's C++
+    autograd nodes instead: their backward asks the running graph task
+    which input gradients are used, so e.g.
     ``autograd.grad(f_out.sum(), q, create_graph=True)`` (the first step of
     an Eikonal loss) computes dq only, and the following ``backward()``
     computes the second-order gradients only for inputs that need them.
+    Both routes give identical values.
     """
 
-    @staticmethod
-    def apply(q, p, f, sigma, R, K):
-        return tuple(_C.knn_aggregate_aniso_autograd(q, p, f, sigma, R, int(K)))
-
-
-class _AggregatePy(torch.autograd.Function):
-    """Python autograd Function of the fused op; base of the lookup and
-    precomputed variants (whose backward is the same adjoint at their
-    indices)."""
+    @classmethod
+    def apply(cls, *args, **kwargs):
+        if cls is KNNAnisotropicAggregate and not kwargs and len(args) == 6:
+            q, p, f, sigma, R, K = args
+            return tuple(_C.knn_aggregate_aniso_autograd(q, p, f, sigma, R, int(K)))
+        return super().apply(*args, **kwargs)
 
     @staticmethod
     def forward(ctx, q, p, f, sigma, R, K):
         f_out, w_out, dists, idxs, points = _C.forward_ex(q, p, f, sigma, R, int(K))
-        ctx.save_for_backward(q, p, f, sigma, R, idxs)
+        ctx.save_for_backward(q, p, f, sigma, R, w_out, idxs)
         ctx.set_materialize_grads(False)  # unused output grads arrive as None, not zero tensors
         ctx.aux = _Aux(points, p.shape[1], tuple(bool(x) for x in ctx.needs_input_grad[:5]))
         return f_out, w_out, dists, idxs
 
     @staticmethod
     def backward(ctx, grad_f_out, grad_w_out, grad_dists, grad_idxs):
-        q, p, f, sigma, R, idxs = ctx.saved_tensors
+        q, p, f, sigma, R, w_out, idxs = ctx.saved_tensors
         if grad_f_out is None:
             return None, None, None, None, None, None
-        grads = KNNAnisotropicAggregateBackward.apply(
-            grad_f_out.contiguous(), grad_w_out, q, p, f, sigma, R, None, idxs, ctx.aux)
+        aux = getattr(ctx, "aux", None)
+        if aux is None:
+            # a subclass's forward (reference style): the weights it saved are used as given
+            gwo = grad_w_out if grad_w_out is not None else torch.zeros_like(w_out)
+            grads = KNNAnisotropicAggregateBackward.apply(grad_f_out.contiguous(), gwo.contiguous(), q, p, f, sigma,
+                                                          R, w_out, idxs)
+        else:
+            # weights recomputed from idxs (bit-identical to the forward's), packed records reused
+            grads = KNNAnisotropicAggregateBackward.apply(grad_f_out.contiguous(), grad_w_out, q, p, f, sigma, R,
+                                                          None, idxs, aux)
         return (*grads, None)
 
 
-class KNNLookupAnisotropicAggregate(_AggregatePy):
+class KNNLookupAnisotropicAggregate(KNNAnisotropicAggregate):
     """Lookup variant (reference ``__init__.py:120-165``); gradients as the
     fused op's at the looked-up indices, none for the table."""
 
     @staticmethod
     def forward(ctx, q, p, f, sigma, R, knn_table, K):
         f_out, w_out, dists, idxs = _C.knn_lookup_aggregate_aniso_forward(q, p, f, sigma, R, knn_table, int(K))
-        ctx.save_for_backward(q, p, f, sigma, R, idxs)
+        ctx.save_for_backward(q, p, f, sigma, R, w_out, idxs)
         ctx.set_materialize_grads(False)
         ctx.aux = _Aux(None, p.shape[1], tuple(bool(x) for x in ctx.needs_input_grad[:5]))
         return f_out, w_out, dists, idxs
 
     @staticmethod
     def backward(ctx, grad_f_out, grad_w_out, grad_dists, grad_idxs):
-        return _AggregatePy.backward(ctx, grad_f_out, grad_w_out, grad_dists, grad_idxs) + (None,)
+        return KNNAnisotropicAggregate.backward(ctx, grad_f_out, grad_w_out, grad_dists, grad_idxs) + (None,)
 
 
-class KNNPrecomputedAnisotropicAggregate(_AggregatePy):
+class KNNPrecomputedAnisotropicAggregate(KNNAnisotropicAggregate):
     """Aggregation at caller-given neighbour indices (reference
     ``__init__.py:167-213``): returns f_out, w_out, dists; gradients as
     KNNAnisotropicAggregate, none for the indices.  (The reference's backward
@@ -167,14 +178,14 @@ class KNNPrecomputedAnisotropicAggregate(_AggregatePy):
     @staticmethod
     def forward(ctx, q, p, f, sigma, R, knn_idxs, K):
         f_out, w_out, dists = _C.knn_precomputed_aggregate_aniso_forward(q, p, f, sigma, R, knn_idxs, int(K))
-        ctx.save_for_backward(q, p, f, sigma, R, knn_idxs)
+        ctx.save_for_backward(q, p, f, sigma, R, w_out, knn_idxs)
         ctx.set_materialize_grads(False)
         ctx.aux = _Aux(None, p.shape[1], tuple(bool(x) for x in ctx.needs_input_grad[:5]))
         return f_out, w_out, dists
 
     @staticmethod
     def backward(ctx, grad_f_out, grad_w_out, grad_dists):
-        return _AggregatePy.backward(ctx, grad_f_out, grad_w_out, grad_dists, None) + (None,)
+        return KNNAnisotropicAggregate.backward(ctx, grad_f_out, grad_w_out, grad_dists, None) + (None,)
 
 
 class KNNAnisotropicAggregateBackward(torch.autograd.Function):

@@ -31,6 +31,8 @@ _SIGS = {
     "knnag_version": ([], _I),
     "knnag_forward_workspace_bytes": ([_I, _I, _I, _I, _I, _I], _S),
     "knnag_forward": ([_V] * 5 + [_I] * 6 + [_V] * 4 + [_V, _V, _S, _V], _I),
+    "knnag_forward_noalloc": ([_V] * 5 + [_I] * 6 + [_V] * 4 + [_V], _I),
+    "knnag_noalloc_read_device_status": ([_V], _I),
     "knnag_variant_workspace_bytes": ([_I, _I, _I, _I], _S),
     "knnag_forward_precomputed": ([_V] * 6 + [_I] * 6 + [_V] * 3 + [_V, _S, _V], _I),
     "knnag_forward_lookup": ([_V] * 6 + [_I] * 7 + [_V] * 4 + [_V, _S, _V], _I),
@@ -60,6 +62,7 @@ _SIGS = {
     "knnag_fp32_peak_probe": ([_V, _I, _I, _V], _I),
     "knnag_set_search_splits": ([_I], _I),
     "knnag_get_search_splits": ([], _I),
+    "knnag_debug_set_search_stall": ([_I, _I], _I),
 }
 
 _lib = None
@@ -125,6 +128,26 @@ def forward(q, p, f, sigma, R, K, points=None):
     _check(lib().knnag_forward(_p(q), _p(p), _p(f), _p(sigma), _p(R), B, Q, P, F, K, dt, _p(f_out), _p(w_out),
                                _p(dists), _p(idxs), _p(points), _p(ws), nb, _stream(q.device)))
     return f_out, w_out, dists, idxs
+
+
+def forward_noalloc(q, p, f, sigma, R, K):
+    """knnag_forward_noalloc (scratch in the library's fixed device array):
+    returns (f_out, w_out, dists, idxs).  Read its device status with
+    noalloc_device_status() before the next call."""
+    B, Q, P, F = q.shape[0], q.shape[1], p.shape[1], f.shape[2]
+    o = dict(dtype=q.dtype, device=q.device)
+    f_out, w_out, dists = torch.empty(B, Q, F, **o), torch.empty(B, Q, K, **o), torch.empty(B, Q, K, **o)
+    idxs = torch.empty(B, Q, K, dtype=torch.int64, device=q.device)
+    _check(lib().knnag_forward_noalloc(_p(q), _p(p), _p(f), _p(sigma), _p(R), B, Q, P, F, K, _dtype(q), _p(f_out),
+                                       _p(w_out), _p(dists), _p(idxs), _stream(q.device)))
+    return f_out, w_out, dists, idxs
+
+
+def noalloc_device_status(device):
+    """knnag_noalloc_read_device_status on `device`: 0 (ok) or 7 (an error
+    latched on the device); synchronises the current stream."""
+    with torch.cuda.device(device):
+        return int(lib().knnag_noalloc_read_device_status(_stream(device)))
 
 
 def forward_precomputed(q, p, f, sigma, R, knn_idxs):
@@ -248,3 +271,16 @@ def set_search_splits(splits):
 
 def search_splits():
     return int(lib().knnag_get_search_splits())
+
+
+def debug_set_search_stall(visit, wait_spins=0):
+    """Test hook of the search's bounded waits (knnag_debug_set_search_stall):
+    visit >= 0 never issues that visit's tile copy, so the waits time out;
+    (-1, 0) restores normal operation."""
+    _check(lib().knnag_debug_set_search_stall(int(visit), int(wait_spins)))
+
+
+def read_device_status(workspace, device):
+    """knnag_read_device_status of a workspace: 0 or 7 (KNNAG_ERR_DEVICE)."""
+    with torch.cuda.device(device):
+        return int(lib().knnag_read_device_status(_p(workspace), _stream(device)))

@@ -113,6 +113,14 @@ int knnag_forward_noalloc(const void* q, const void* p, const void* f, const voi
                           int B, int Q, int P, int F, int K, int dtype,
                           void* f_out, void* w_out, void* dists, int64_t* idxs, void* stream);
 
+/* The device status word of knnag_forward_noalloc's fixed scratch on the
+ * current device, read and cleared as knnag_read_device_status does for a
+ * workspace (synchronises `stream`).  Read it after a call and before the
+ * next one, which clears it.  The scratch address is cached per device for
+ * the life of the device's primary context.  No counterpart in the
+ * reference. */
+int knnag_noalloc_read_device_status(void* stream);
+
 /* ----------------------------------------------------- forward variants */
 
 /* Bytes of scratch the variant entry points below need. */
@@ -325,6 +333,17 @@ long long knnag_launch_count(void);
  * reference counterpart. */
 int knnag_set_search_splits(int splits);
 int knnag_get_search_splits(void);
+
+/* Test hook of the search kernels' bounded waits (process-wide; affects
+ * every later FP32 search launch).  visit >= 0: the tile copy of that
+ * visit position of every search CTA is armed on its mbarrier but never
+ * issued, so the waits on it give up after wait_spins sleeps of 256 ns
+ * (0: the default budget, about a second), the kernel latches
+ * KNNAG_ERR_DEVICE in the workspace status word and returns without writing
+ * that CTA's outputs.  knnag_debug_set_search_stall(-1, 0) restores normal
+ * operation.  Returns KNNAG_ERR_ARG for visit < -1 or wait_spins < 0.  No
+ * reference counterpart (the reference has no bounded waits). */
+int knnag_debug_set_search_stall(int visit, int wait_spins);
 
 /* Launch an FFMA-bound kernel (blocks x 256 threads, `iters` iterations of 16
  * independent FMA chains per thread, 32*iters FLOP per thread) writing one

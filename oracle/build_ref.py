@@ -15,8 +15,10 @@ pick on a B200.  The module is used on the GPU box as the bit-exact reference
 for ``idxs``/``dists`` and as the timed reference extension.  Nothing here is
 imported by the product.
 
-Usage: ``python oracle/build_ref.py [--src DIR]``; exits 0 without building
-when the reference checkout is absent.
+Usage: ``python oracle/build_ref.py [--src DIR]``.  The checkout is ``--src``,
+else the ``KNN_REFERENCE_SRC`` environment variable, else a directory named
+``reference`` beside this repository's root.  Exits 0 without building when
+the checkout is absent (as on a machine that only runs the prebuilt module).
 """
 from __future__ import annotations
 
@@ -29,7 +31,16 @@ import sysconfig
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_ref")
 MODULE = "knn_ref_C"
-DEFAULT_SRC = "/root/reference"
+REPO_ROOT = os.path.dirname(HERE)
+
+
+def default_src() -> str:
+    """Location of the reference checkout: $KNN_REFERENCE_SRC, else
+    ``<parent of the repository root>/reference``."""
+    env = os.environ.get("KNN_REFERENCE_SRC")
+    if env:
+        return env
+    return os.path.join(os.path.dirname(REPO_ROOT), "reference")
 
 
 def _torch_paths():
@@ -42,8 +53,8 @@ def _torch_paths():
     return incs, libs, abi
 
 
-def build(src_root: str = DEFAULT_SRC, verbose: bool = True) -> str | None:
-    csrc = os.path.join(src_root, "csrc")
+def build(src_root: str | None = None, verbose: bool = True) -> str | None:
+    csrc = os.path.join(src_root or default_src(), "csrc")
     if not os.path.isdir(csrc):
         if verbose:
             print(f"[build_ref] reference sources not found at {csrc}; skipping")
@@ -91,7 +102,7 @@ def build(src_root: str = DEFAULT_SRC, verbose: bool = True) -> str | None:
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--src", default=DEFAULT_SRC)
+    ap.add_argument("--src", default=None, help="reference checkout (default: $KNN_REFERENCE_SRC or ../reference)")
     a = ap.parse_args()
     build(a.src)
     sys.exit(0)

@@ -184,6 +184,30 @@ def eikonal_step(q, p, f, sigma, R, K, forward=plain_forward):
     return loss.detach(), f_out.detach(), idxs
 
 
+def eikonal_grads64(q, p, f, sigma, R, idxs, chunk=2048):
+    """The timed step's gradients in FP64 at fixed idxs, chunked over the
+    queries so that full-size workloads fit in host memory: dq = d(sum
+    f_out)/dq per query, loss = mean((|dq| - 1)^2) over all B*Q queries, and
+    d loss / d(q, p, f, sigma, R) -- each chunk's share of the loss is
+    back-propagated on its own and the point-side gradients accumulate.
+    Returns (loss, dq [B,Q,3], (grad_q, grad_p, grad_f, grad_sigma, grad_R))."""
+    B, Q = q.shape[0], q.shape[1]
+    pp, ff, ss, RR = [x.detach().double().clone().requires_grad_(True) for x in (p, f, sigma, R)]
+    dq = torch.empty(B, Q, 3, dtype=torch.float64)
+    gq = torch.empty(B, Q, 3, dtype=torch.float64)
+    loss = 0.0
+    for s0 in range(0, Q, chunk):
+        qc = q[:, s0:s0 + chunk].detach().double().clone().requires_grad_(True)
+        fo, _ = aggregate64(qc, pp, ff, ss, RR, idxs[:, s0:s0 + chunk])
+        (g,) = torch.autograd.grad(fo.sum(), qc, create_graph=True)
+        lc = ((g.norm(dim=-1) - 1.0) ** 2).sum() / (B * Q)
+        lc.backward()
+        dq[:, s0:s0 + chunk] = g.detach()
+        gq[:, s0:s0 + chunk] = qc.grad
+        loss += float(lc.detach())
+    return loss, dq, (gq, pp.grad, ff.grad, ss.grad, RR.grad)
+
+
 # ----------------------------------------------------------------------------
 # Variants of the forward (reference csrc/forward.cu:5-53, 113-183, 186-230)
 # ----------------------------------------------------------------------------

@@ -117,6 +117,41 @@ def test_reference_compatible_ops():
         assert rel_err(a.cpu().numpy(), r.numpy()) < 1e-4
 
 
+def test_function_subclass_written_against_the_reference():
+    """KNNAnisotropicAggregate is a torch.autograd.Function: a subclass in the
+    reference's style (its own forward saving (q, p, f, sigma, R, w_out,
+    idxs), the base class's backward) trains to the same gradients as the
+    C++ autograd route of the base class, through both orders."""
+    import cuda_knn_aggregate as C
+
+    assert issubclass(C.KNNAnisotropicAggregate, torch.autograd.Function)
+    assert issubclass(C.KNNLookupAnisotropicAggregate, C.KNNAnisotropicAggregate)
+    assert issubclass(C.KNNPrecomputedAnisotropicAggregate, C.KNNAnisotropicAggregate)
+
+    class Mine(C.KNNAnisotropicAggregate):
+        @staticmethod
+        def forward(ctx, q, p, f, sigma, R, K):
+            f_out, w_out, dists, idxs = C._C.knn_aggregate_aniso_forward(q, p, f, sigma, R, K)
+            ctx.save_for_backward(q, p, f, sigma, R, w_out, idxs)
+            return f_out, w_out, dists, idxs
+
+    shape, t = make(B=2, Q=300, P=400, F=8, K=8, seed=21)
+    results = []
+    for op in (C.KNNAnisotropicAggregate.apply, Mine.apply, C.KNNPrecomputedAnisotropicAggregate.apply):
+        ins = [x.to(DEV).requires_grad_(True) for x in t]
+        if op is C.KNNPrecomputedAnisotropicAggregate.apply:
+            idxs = C.knn_aggregate_aniso(*[x.detach() for x in ins], shape.K)[3]
+            f_out = op(*ins, idxs, shape.K)[0]
+        else:
+            f_out = op(*ins, shape.K)[0]
+        (gq,) = torch.autograd.grad(f_out.sum(), ins[0], create_graph=True)
+        ((gq.norm(dim=-1) - 1.0) ** 2).mean().backward()
+        results.append([f_out.detach(), gq.detach()] + [x.grad for x in ins])
+    for other in results[1:]:
+        for a, b in zip(results[0], other):
+            assert rel_err(b.cpu().numpy(), a.cpu().numpy()) < 1e-5
+
+
 def test_errors_follow_reference_wording():
     from cuda_knn_aggregate import knn_aggregate_aniso
 

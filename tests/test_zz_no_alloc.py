@@ -5,8 +5,13 @@ so it must give the same results as knnag_forward -- on consecutive calls,
 whatever the previous call left in that shared array.
 
 Tolerances as in the other parity tests: idxs and dists exact, w_out and
-f_out within 1e-5 relative to the tensor's max.  The file name sorts last so
-a run that stops at the first failure has run every other test first.
+f_out within 1e-5 relative to the tensor's max.  After every call the
+array's device status word is read back (knnag_noalloc_read_device_status)
+and must be clear.  The cases cover each layout the array can hold: FP32
+with the spatial search index (K <= 32), FP32 with K > 32 (exact kernel
+only), FP64 (larger records, no index), and an FP32 shape whose scratch is
+just under the array's size.  The file name sorts last so a run that stops
+at the first failure has run every other test first.
 """
 import ctypes
 
@@ -45,7 +50,7 @@ def assert_same(a, b):
     f0, w0, d0, i0 = [x.cpu().numpy() for x in a]
     f1, w1, d1, i1 = [x.cpu().numpy() for x in b]
     assert np.array_equal(i0, i1)
-    assert np.array_equal(d0.view(np.int32), d1.view(np.int32))
+    assert np.array_equal(d0.view(np.uint8), d1.view(np.uint8))
     assert rel_err(w0, w1) < FWD_TOL
     assert rel_err(f0, f1) < FWD_TOL
 
@@ -63,9 +68,39 @@ def test_noalloc_matches_forward_on_consecutive_calls():
     for shape, t in cases + cases:
         x = [a.to(dev) for a in t]
         got = run_noalloc(fn, capi, *x, shape.K)
+        assert capi.noalloc_device_status(dev) == 0
         want = capi.forward(*x, shape.K)
         torch.cuda.synchronize()
         assert_same(got, want)
+
+
+@pytest.mark.gpu
+def test_noalloc_other_layouts_and_the_size_limit():
+    """FP64, K > 32 and a shape whose scratch is just under the fixed array
+    (and one point more, which must be refused), each twice in a row."""
+    from cuda_knn_aggregate import workloads as W
+
+    fn, capi = lib_and_capi()
+    dev = torch.device("cuda:0")
+    lim = 8 << 20
+    near_P = 59392  # FP32, K=16, Q=512: the largest P whose scratch fits
+    L = capi.lib()
+    assert L.knnag_forward_workspace_bytes(1, 512, near_P, 8, 16, capi.F32) <= lim
+    assert L.knnag_forward_workspace_bytes(1, 512, near_P + 1, 8, 16, capi.F32) > lim
+    cases = [W.make("small", B=2, Q=300, P=400, F=6, K=9, seed=33, dtype=torch.float64),
+             W.make("small", B=1, Q=200, P=300, F=8, K=40, seed=34),
+             W.make("small", B=1, Q=512, P=near_P, F=8, K=16, seed=35)]
+    for shape, t in cases + cases:
+        x = [a.to(dev) for a in t]
+        got = run_noalloc(fn, capi, *x, shape.K)
+        assert capi.noalloc_device_status(dev) == 0
+        want = capi.forward(*x, shape.K)
+        torch.cuda.synchronize()
+        assert_same(got, want)
+    _, t = W.make("small", B=1, Q=512, P=near_P + 1, F=8, K=16, seed=36)
+    x = [a.to(dev) for a in t]
+    with pytest.raises(RuntimeError, match="scratch"):
+        capi.forward_noalloc(*x, 16)
 
 
 @pytest.mark.gpu
