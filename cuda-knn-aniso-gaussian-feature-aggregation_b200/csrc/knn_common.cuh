@@ -32,9 +32,10 @@ enum RecField {
   kRecLen = 16
 };
 
-// Points per search tile (8 KB) and the pair-interleaved tile layout: a pair of
-// points (2m, 2m+1) is 16 float2 = 128 bytes, field f of the pair at float2
-// slot f, so packed f32x2 arithmetic reads both points' field with one load.
+// Points per search tile (8 KB) and the floats of one point pair (2m, 2m+1)
+// in it: 16 fields x float2.  Tiles are field-major (field f of pair m at
+// float2 f * 64 + m), so packed f32x2 arithmetic reads both points' field
+// with one load and a warp reads 32 pairs' field with one conflict-free load.
 constexpr int kTilePoints = 128;
 constexpr int kPairFloats = 32;
 

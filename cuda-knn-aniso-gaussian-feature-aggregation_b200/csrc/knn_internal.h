@@ -70,49 +70,47 @@ struct SearchParams {
   int wait_spins;
 };
 
-// Search CTA: 4 warps; G warps split the points of one 32-query group.
-constexpr int kSearchThreads = 128;
-constexpr int kQueueCap = 8;
+// Search CTA: WPC warps (1, 2 or 4), each owning 32 queries (one per lane)
+// and sharing the CTA's tile ring; a work item is the CTA's 32 * WPC
+// queries.  The C ABI's `splits` setting s (1, 2, 4) selects WPC = 4 / s,
+// i.e. 128 / s queries per work item.
+constexpr int kSearchMaxThreads = 128;
+// Candidate queue entries per query: one half tile (64 points) always fits.
+constexpr int kQCap = 64;
 // Tile buffers of the search ring: visit v lands in buffer v % kTileBufs,
 // so kTileBufs - 1 copies are in flight while a tile is being read.
 constexpr int kTileBufs = 2;
-// the tail of region B holds kTileBufs mbarriers (8 B), kTileBufs counters
-// (4 B) and two flags (4 B each)
+constexpr size_t kSearchTileBytes = 8192;                  // 128 points x 16 floats
+constexpr size_t kWarpQueueBytes = (size_t)32 * kQCap * 8;  // keys + point indices
 static_assert(kTileBufs * 12 + 8 <= 64, "search ring bookkeeping exceeds its 64 bytes");
 
-// Shared-memory bytes of the search kernel for (KMAX, G).
-__host__ __device__ inline constexpr size_t search_merge_bytes(int kmax, int g) {
-  return (g > 1) ? (size_t)kSearchThreads * (kmax + 1) * 8 + (size_t)kSearchThreads * 4 : 0;
+// Shared-memory layout of the search kernel with `wpc` warps:
+//   ring      kTileBufs tiles
+//   queues    wpc x [32 queries][kQCap] keys, then indices (after the tile
+//             loop: the CTA's sorted lists, weights and flags)
+//   qtab      [32 wpc] float4 (x, y, z, threshold) of the CTA's queries
+//   misc      [32 wpc] original query index, [wpc][6] warp query boxes,
+//             64 bytes of mbarriers / counters / flags
+//   region C  tile bounds and visit order [NTP x 8 B] + visit counter
+__host__ __device__ inline constexpr size_t search_queue_off() { return (size_t)kTileBufs * kSearchTileBytes; }
+__host__ __device__ inline constexpr size_t search_qtab_off(int wpc) {
+  return search_queue_off() + (size_t)wpc * kWarpQueueBytes;
 }
-__host__ __device__ inline constexpr size_t search_region_a_bytes(int kmax, int g) {
-  // phase 1: kTileBufs tiles of 64 pairs x 128 B
-  size_t tiles = (size_t)kTileBufs * 64 * 128;
-  int qpc = 32 * (4 / g);
-  int L = kmax + 1;
-  size_t merge = (g > 1) ? (size_t)kSearchThreads * L * 8 + (size_t)kSearchThreads * 4 : 0;
-  size_t out = (size_t)qpc * ((size_t)L * 12 + 4);
-  size_t phase2 = merge + out;
-  return tiles > phase2 ? tiles : phase2;
+__host__ __device__ inline constexpr size_t search_misc_off(int wpc) { return search_qtab_off(wpc) + (size_t)wpc * 32 * 16; }
+__host__ __device__ inline constexpr size_t search_bars_off(int wpc) {
+  return search_misc_off(wpc) + (size_t)wpc * 32 * 4 + (size_t)wpc * 6 * 4;
 }
-__host__ __device__ inline constexpr size_t search_region_b_bytes() {
-  // candidate queues (keys + idx), shared thresholds, then 64 bytes for the
-  // kTileBufs mbarriers, their counters and two flags
-  return (size_t)kQueueCap * kSearchThreads * 8 + 2 * (size_t)kSearchThreads * 4 + 64;
-}
-__host__ __device__ inline constexpr size_t search_smem_bytes(int kmax, int g) {
-  return search_region_a_bytes(kmax, g) + search_region_b_bytes();
-}
-// Tiles per batch element rounded up to a power of two (the visit-order sort).
+__host__ __device__ inline constexpr size_t search_smem_bytes(int wpc) { return search_bars_off(wpc) + 64; }
+// Tiles per cloud rounded up to a power of two (the visit-order sort).
 __host__ __device__ inline int search_tiles_pow2(int ntile) {
   int n = 1;
   while (n < ntile) n <<= 1;
   return n;
 }
-// Region C: tile bounds + order [NTP x 8 B], original query index [QPC],
-// query boxes [4 x 6 floats], visit counter.
-__host__ __device__ inline size_t search_region_c_bytes(int ntile, int g) {
-  return (size_t)search_tiles_pow2(ntile) * 8 + (size_t)32 * (4 / g) * 4 + 24 * 4 + 16;
-}
+__host__ __device__ inline size_t search_region_c_bytes(int ntile) { return (size_t)search_tiles_pow2(ntile) * 8 + 16; }
+// The sorted lists of the CTA's queries (keys, indices, weights) staged for
+// the epilogue must fit the queue region.
+static_assert((size_t)32 * 33 * 12 + 32 * 4 <= kWarpQueueBytes, "epilogue staging exceeds the queue region");
 
 // ------------------------------------------------------------- workspace
 // Forward workspace: [status, flag_count] | flag_list [B*Q] | records (when

@@ -294,39 +294,37 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
 
 // ------------------------------------------------------- fused FP32 search
 //
-// CTA = 4 warps.  Each thread owns one query; G warps of the CTA share one
-// 32-query group and split every point tile between them (G = 1, 2, 4), so
-// small query counts still fill the GPU.  Point tiles (128 points, 8 KB, in
-// the pair-interleaved layout) are streamed into shared memory by one-
-// dimensional bulk copies (TMA), double-buffered on two mbarriers; all lanes
-// read the same pair at a time (broadcast), and both keys of a pair come out
-// of one packed f32x2 key evaluation.
+// CTA = WPC warps (1, 2 or 4).  Each warp owns 32 queries -- lane j keeps
+// query j's sorted register list -- and all warps share the CTA's ring of
+// point tiles (128 points, 8 KB, field-major: field f of pair m at float2
+// f * 64 + m), streamed into shared memory by one-dimensional bulk copies
+// (TMA, no multicast), double-buffered on mbarriers.
 //
-// Selection.  Each thread keeps the K+1 smallest keys it has accepted in a
-// sorted register list of KMAX+1 slots whose lowest KMAX-K slots hold -inf
-// sentinels, so the (K+1)-th smallest real key is always the last slot.  A
-// key is a candidate when key <= tau (the tightest list top known to the
-// group); candidates are appended to a per-thread queue in shared memory and
-// folded into the list when any lane's queue is nearly full and at every
-// tile end.  At every tile end each split also publishes two bounds on the
-// (K+1)-th smallest key of the union of the G lists of its query: its own
-// list top (the union holds K+1 keys at or below it) and its c-th smallest
-// key, c = ceil((K+1)/G) (the G splits together hold G*c >= K+1 keys at or
-// below the largest of those).  tau is the smallest of these bounds; any
-// published value, however stale, is a valid bound because a list only ever
-// gets smaller keys.  The G lists are merged once, after the last tile.
+// Keys are computed with lanes over POINTS: for each half tile a lane holds
+// one point pair (16 float2 registers) and the warp loops over its queries
+// that the tile may matter to, each broadcast from a shared table
+// (x, y, z, threshold); one packed f32x2 evaluation gives the lane both of
+// its points' keys, so a warp instruction covers 64 (query, point) pairs.
+// Keys at or below the query's threshold are appended (ballot + popc
+// positions) to the query's candidate queue in shared memory, and after
+// every half tile each lane folds its own query's queue into its list.  A
+// query skips a tile whose lower bound against the query point exceeds its
+// threshold.
+//
+// Selection.  Each list holds the K+1 smallest keys accepted so far in
+// KMAX+1 slots whose lowest KMAX-K slots are -inf sentinels, so the
+// (K+1)-th smallest real key is always the last slot; the threshold is that
+// slot (stale values are still valid: lists only gain smaller keys).
 //
 // Exactness.  The result equals the reference's MinK selection whenever the
 // K+1 smallest keys are pairwise distinct (then the top-K set and its order
 // are unique) and no NaN key falls in MinK's fill phase (points 0..K-1).
-// Every key that leaves the lists is either strictly above a threshold that
-// is >= the global (K+1)-th key, or equal to the threshold it was compared
-// with; the smallest such "equal" key is tracked (tie_key).  A query is
-// flagged for the exact replay kernel when its merged top-(K+1) holds equal
-// keys or an empty slot, when tie_key <= its merged (K+1)-th key, or when a
+// Every key that leaves a list or is not queued is either strictly above a
+// threshold that is >= the (K+1)-th key, or equal to the threshold it was
+// compared with; the smallest such "equal" key is tracked (tie_key).  A
+// query is flagged for the exact replay kernel when its top-(K+1) holds
+// equal keys or an empty slot, when tie_key <= its (K+1)-th key, or when a
 // fill-phase key is NaN.
-
-constexpr unsigned kTileBytes = (kTilePoints / 2) * kPairFloats * 4;
 
 template <int L>
 __device__ __forceinline__ void list_insert(float (&keys)[L], int (&vals)[L], float k, int i, float& tie_key) {
@@ -346,62 +344,31 @@ __device__ __forceinline__ void list_insert(float (&keys)[L], int (&vals)[L], fl
   if (i >= 0 && k == keys[L - 1]) tie_key = fminf(tie_key, k);
 }
 
+// Queue slot of entry e of query (lane) j: rows are rotated by j so that
+// appends (one query, consecutive entries) and drains (every lane its own
+// query, the same entry) are both free of bank conflicts.
+__device__ __forceinline__ int queue_slot(int j, int e) { return j * kQCap + ((e + j) & (kQCap - 1)); }
+
+// Lane `lane` folds its query's n queued candidates into its list and
+// refreshes its threshold; the caller resets the counts.
 template <int L>
-__device__ __forceinline__ void flush_queue(float (&keys)[L], int (&vals)[L], int& qn, float& tie_key, float& tau,
-                                            const float* qk, const int* qv, int tid) {
-  for (int e = 0; e < qn; ++e) {
-    const float k = qk[e * kSearchThreads + tid];
-    const int i = qv[e * kSearchThreads + tid];
+__device__ __forceinline__ void drain_queue(float (&keys)[L], int (&vals)[L], float& tie_key, float& tau, int n,
+                                            const float* qk, const int* qv, int lane) {
+  for (int e = 0; e < n; ++e) {
+    const int s = queue_slot(lane, e);
+    const float k = qk[s];
     const float top = keys[L - 1];
     if (k < top) {
-      list_insert<L>(keys, vals, k, i, tie_key);
+      list_insert<L>(keys, vals, k, qv[s], tie_key);
     } else if (k == top) {
       tie_key = fminf(tie_key, k);
     }
   }
-  qn = 0;
   tau = fminf(tau, keys[L - 1]);
 }
 
-// Merge the sorted lists of the G splits of query lq (slots [start, L) of
-// each; entries with a negative index count as +inf) and write the `count`
-// smallest to ok/oi.  Returns the next key after them (+inf if none).
-template <int G, int L>
-__device__ __forceinline__ float merge_splits(const float* mk, const int* mv, int qpc, int lq, int start, int count,
-                                              float* ok, int* oi) {
-  int h[G];
-#pragma unroll
-  for (int g = 0; g < G; ++g) h[g] = start;
-  float next = INFINITY;
-  for (int j = 0; j <= count; ++j) {
-    float bk = INFINITY;
-    int bi = -1, bg = -1;
-#pragma unroll
-    for (int g = 0; g < G; ++g) {
-      if (h[g] < L) {
-        const int v = mv[(g * qpc + lq) * L + h[g]];
-        const float kk = v >= 0 ? mk[(g * qpc + lq) * L + h[g]] : INFINITY;
-        if (bg < 0 || kk < bk) {
-          bk = kk;
-          bi = v;
-          bg = g;
-        }
-      }
-    }
-#pragma unroll
-    for (int g = 0; g < G; ++g) h[g] += (g == bg) ? 1 : 0;
-    if (j < count) {
-      ok[j] = bk;
-      oi[j] = bi >= 0 ? bi : -1;
-    } else {
-      next = bk;
-    }
-  }
-  return next;
-}
-
-// One search work item: up to QPC queries of one batch element or segment,
-// all against one cloud.  Pointers are offset to the group already.
+// One search work item: up to 32 * WPC queries of one batch element or
+// segment, all against one cloud.  Pointers are offset to the group already.
 struct SearchItem {
   const float* q;      // query rows (group-local index)
   const int* perm_q;   // sorted position -> group-local query index
@@ -434,71 +401,49 @@ __device__ __forceinline__ float tile_lower_bound(const float* ti, const float* 
   return lb >= 0.f ? lb : 0.f;  // NaN: 0 (keys are >= 0 when mu >= 0)
 }
 
-// Bound on the (K+1)-th smallest key of query lq's G split lists, from the
-// published list tops (any one split's top) and c-th keys (the largest of
-// the G).
-template <int G, int QPC>
-__device__ __forceinline__ float query_bound(const float* tops, const float* cths, int lq) {
-  float tm = tops[lq], tc = cths[lq];
-#pragma unroll
-  for (int g = 1; g < G; ++g) {
-    tm = fminf(tm, tops[g * QPC + lq]);
-    tc = fmaxf(tc, cths[g * QPC + lq]);
-  }
-  return G > 1 ? fminf(tm, tc) : tm;
-}
-
-// The two tile-buffer mbarriers of a search CTA.
-__device__ __forceinline__ uint64_t* search_barriers(unsigned char* smem, size_t region_a) {
-  return reinterpret_cast<uint64_t*>(smem + region_a + (size_t)kQueueCap * kSearchThreads * 8 +
-                                     2 * (size_t)kSearchThreads * 4);
+// The tile-ring mbarriers of a search CTA.
+template <int WPC>
+__device__ __forceinline__ uint64_t* search_barriers(unsigned char* smem) {
+  return reinterpret_cast<uint64_t*>(smem + search_bars_off(WPC));
 }
 
 // Search + aggregation of one work item.  The mbarriers are initialised by
 // the kernel; uses[buf] counts the phases buffer buf has completed so far
 // (a persistent CTA runs many items on the same barriers).  Returns false
 // when a tile copy timed out (status flagged; the CTA must stop).
-template <int KMAX, int G>
+template <int KMAX, int WPC>
 __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchItem& it, unsigned char* smem,
                                             int ntp_cap, uint32_t (&uses)[kTileBufs]) {
   constexpr int L = KMAX + 1;
-  constexpr int QPC = 32 * (4 / G);
+  constexpr int NT = 32 * WPC;          // threads = queries of the item
   constexpr int PPT = kTilePoints / 2;  // pairs per tile
-  constexpr int PPS = PPT / G;          // pairs per split per tile
-  constexpr size_t RA = search_region_a_bytes(KMAX, G);
-  constexpr size_t RB = search_region_b_bytes();
-  constexpr size_t kMerge = search_merge_bytes(KMAX, G);
+  constexpr unsigned FULL = 0xffffffffu;
+  static_assert((size_t)NT * L * 12 + NT * 4 <= (size_t)WPC * kWarpQueueBytes, "epilogue staging");
 
-  unsigned char* regA = smem;
-  float* qk = reinterpret_cast<float*>(smem + RA);
-  int* qv = reinterpret_cast<int*>(qk + kQueueCap * kSearchThreads);
-  // per split and query: list top, and c-th smallest key (G > 1)
-  float* tau_share = reinterpret_cast<float*>(qv + kQueueCap * kSearchThreads);  // [128]
-  float* cth_share = tau_share + kSearchThreads;                                 // [128]
-  uint64_t* full = reinterpret_cast<uint64_t*>(tau_share + 2 * kSearchThreads);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  unsigned char* ring = smem;
+  float* qk = reinterpret_cast<float*>(smem + search_queue_off() + (size_t)warp * kWarpQueueBytes);
+  int* qv = reinterpret_cast<int*>(qk + 32 * kQCap);
+  float4* qtab = reinterpret_cast<float4*>(smem + search_qtab_off(WPC));  // [NT]
+  int* qorig = reinterpret_cast<int*>(smem + search_misc_off(WPC));       // [NT] original query index (-1: none)
+  float* qbox = reinterpret_cast<float*>(qorig + NT);                     // [WPC][6]
+  uint64_t* full = search_barriers<WPC>(smem);
   int* cnt = reinterpret_cast<int*>(full + kTileBufs);               // warps done per buffer
   volatile int* s_final = reinterpret_cast<volatile int*>(cnt + kTileBufs);  // visit count once stopped
   volatile int* s_abort = s_final + 1;                               // a wait gave up
-  // region C: per-tile lower bounds (sorted), visit order, query bookkeeping
+  // region C: per-tile lower bounds (sorted), visit order, visit counter
   const int NTP = search_tiles_pow2(it.ntile);
-  float* lbk = reinterpret_cast<float*>(smem + RA + RB);
+  float* lbk = reinterpret_cast<float*>(smem + search_smem_bytes(WPC));
   int* lbt = reinterpret_cast<int*>(lbk + ntp_cap);
-  int* qorig = lbt + ntp_cap;                                // [QPC] original query index (-1: none)
-  float* qbox = reinterpret_cast<float*>(qorig + QPC);       // [4 warps][6]
-  volatile int* s_nvisit = reinterpret_cast<volatile int*>(qbox + 24);
-  // phase-2 views of region A
-  float* mk = reinterpret_cast<float*>(regA);
-  int* mv = reinterpret_cast<int*>(regA + (size_t)kSearchThreads * L * 4);
-  float* mf = reinterpret_cast<float*>(regA + (size_t)kSearchThreads * L * 8);
-  float* out_k = reinterpret_cast<float*>(regA + kMerge);
-  int* out_i = reinterpret_cast<int*>(out_k + QPC * L);
-  float* out_w = reinterpret_cast<float*>(out_i + QPC * L);
-  int* out_f = reinterpret_cast<int*>(out_w + QPC * L);
+  volatile int* s_nvisit = reinterpret_cast<volatile int*>(lbt + ntp_cap);
+  // epilogue views of the queue region (after the tile loop)
+  float* out_k = reinterpret_cast<float*>(smem + search_queue_off());
+  int* out_i = reinterpret_cast<int*>(out_k + NT * L);
+  float* out_w = reinterpret_cast<float*>(out_i + NT * L);
+  int* out_f = reinterpret_cast<int*>(out_w + NT * L);
 
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int split = warp % G, grp = warp / G;
-  const int lq = grp * 32 + lane;
-  const int sp = it.qblock * QPC + lq;  // position in the spatial order
+  const int lq = tid;                   // query of this lane within the item
+  const int sp = it.qblock * NT + lq;   // position in the spatial order
   bool valid = sp < it.Q;
   int qi = it.perm_q[valid ? sp : it.Q - 1];
   if ((unsigned)qi >= (unsigned)it.Q) {  // the query order is a permutation: never taken
@@ -507,25 +452,18 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     valid = false;
   }
   const int K = it.K, P = it.P;
-
   const float qx = it.q[(int64_t)qi * 3 + 0], qy = it.q[(int64_t)qi * 3 + 1], qz = it.q[(int64_t)qi * 3 + 2];
-  const float2 qx2 = make_float2(qx, qx), qy2 = make_float2(qy, qy), qz2 = make_float2(qz, qz);
   const float* recb = it.rec;
-  if (split == 0) qorig[lq] = valid ? qi : -1;
-  // thresholds published by the warps of this item (read without barriers:
-  // any value written here is a valid bound, so it must not be a stale one
-  // from the previous item)
-  tau_share[split * QPC + lq] = INFINITY;
-  cth_share[split * QPC + lq] = INFINITY;
+  qorig[lq] = valid ? qi : -1;
+  qtab[lq] = make_float4(qx, qy, qz, valid ? INFINITY : -INFINITY);
 
   // MinK's fill phase stores points 0..K-1 whatever their key: a NaN there
   // changes the result in ways only the replay reproduces.
   bool nan_fill = false;
-  if (split == 0)
-    for (int i = 0; i < K; ++i) {
-      const float s = key_rec<float>(qx, qy, qz, recb + (int64_t)i * kRecLen);
-      if (s != s) nan_fill = true;
-    }
+  for (int i = 0; i < K; ++i) {
+    const float s = key_rec<float>(qx, qy, qz, recb + (int64_t)i * kRecLen);
+    if (s != s) nan_fill = true;
+  }
 
   // ---- box of this CTA's queries and the tile visit order
   {
@@ -534,8 +472,8 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        bx[c] = fminf(bx[c], __shfl_xor_sync(0xffffffffu, bx[c], o));
-        bx[3 + c] = fmaxf(bx[3 + c], __shfl_xor_sync(0xffffffffu, bx[3 + c], o));
+        bx[c] = fminf(bx[c], __shfl_xor_sync(FULL, bx[c], o));
+        bx[3 + c] = fmaxf(bx[3 + c], __shfl_xor_sync(FULL, bx[3 + c], o));
       }
     }
     if (lane == 0)
@@ -546,8 +484,13 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   float bmin[3], bmax[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    bmin[c] = fminf(fminf(qbox[c], qbox[6 + c]), fminf(qbox[12 + c], qbox[18 + c]));
-    bmax[c] = fmaxf(fmaxf(qbox[3 + c], qbox[9 + c]), fmaxf(qbox[15 + c], qbox[21 + c]));
+    bmin[c] = qbox[c];
+    bmax[c] = qbox[3 + c];
+#pragma unroll
+    for (int w = 1; w < WPC; ++w) {
+      bmin[c] = fminf(bmin[c], qbox[w * 6 + c]);
+      bmax[c] = fmaxf(bmax[c], qbox[w * 6 + 3 + c]);
+    }
   }
   const float* tinfo_b = it.tinfo;
   if (NTP <= 32) {
@@ -561,8 +504,8 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
       for (int kk = 2; kk <= 32; kk <<= 1) {
 #pragma unroll
         for (int j = kk >> 1; j > 0; j >>= 1) {
-          const float ok = __shfl_xor_sync(0xffffffffu, lb, j);
-          const int oi = __shfl_xor_sync(0xffffffffu, ti, j);
+          const float ok = __shfl_xor_sync(FULL, lb, j);
+          const int oi = __shfl_xor_sync(FULL, ti, j);
           const bool up = (lane & kk) == 0;
           const bool lower = (lane & j) == 0;
           const bool other_less = ok < lb || (ok == lb && oi < ti);
@@ -579,11 +522,10 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     }
     __syncthreads();
   } else {
-    for (int t = tid; t < NTP; t += kSearchThreads) {
+    for (int t = tid; t < NTP; t += NT) {
       float lb = INFINITY;
       if (t < it.ntile) {
-        const float* ti = tinfo_b + t * 8;
-        lb = tile_lower_bound(ti, bmin, bmax);
+        lb = tile_lower_bound(tinfo_b + t * 8, bmin, bmax);
         lb = fminf(lb, 3.4e38f);  // real tiles sort before the +inf padding entries
       }
       lbk[t] = lb;
@@ -592,7 +534,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     __syncthreads();
     for (int kk = 2; kk <= NTP; kk <<= 1) {  // bitonic sort of (bound, tile) ascending
       for (int j = kk >> 1; j > 0; j >>= 1) {
-        for (int i = tid; i < NTP; i += kSearchThreads) {
+        for (int i = tid; i < NTP; i += NT) {
           const int ixj = i ^ j;
           if (ixj > i) {
             const bool up = (i & kk) == 0;
@@ -618,19 +560,19 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     keys[s] = (s < KMAX - K) ? -INFINITY : INFINITY;
     vals[s] = -1;
   }
-  float tau = INFINITY, tie_key = INFINITY;
-  int qn = 0;
+  float tau = valid ? INFINITY : -INFINITY, tie_key = INFINITY;
+  int my_cnt = 0;  // queued candidates of this lane's query
+  const float qpt[3] = {qx, qy, qz};
 
   const int ntile = it.ntile;
-  // slot of this list's c-th smallest real key, c = ceil((K+1)/G)
-  const int cslot = (KMAX - K) + (K + G) / G - 1;
   const float* pairs_b = it.pairs;
   // visit position v reads tile lbt[v] into buffer v % kTileBufs
   auto issue = [&](int v) {
     const int buf = v % kTileBufs;
-    mbar_arrive_expect_tx(&full[buf], kTileBytes);
+    mbar_arrive_expect_tx(&full[buf], (uint32_t)kSearchTileBytes);
     if (v == a.stall_visit) return;  // test hook: this phase never completes
-    bulk_copy_g2s(regA + buf * kTileBytes, pairs_b + (int64_t)lbt[v] * PPT * kPairFloats, kTileBytes, &full[buf]);
+    bulk_copy_g2s(ring + buf * kSearchTileBytes, pairs_b + (int64_t)lbt[v] * PPT * kPairFloats,
+                  (uint32_t)kSearchTileBytes, &full[buf]);
   };
   // Issue position v unless its bound exceeds every threshold (the order is
   // ascending, so nothing after it is needed either).  Decisions are made
@@ -657,7 +599,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     *s_final = 0x7fffffff;
     *s_abort = 0;
     for (int b = 0; b < kTileBufs; ++b) cnt[b] = 0;
-    fence_proxy_async_smem();  // region A was last written by generic stores
+    fence_proxy_async_smem();  // the ring was last written by generic stores
     for (int v = 0; v < kTileBufs; ++v) {
       if (decide(v, INFINITY)) {
         issue(v);
@@ -669,14 +611,14 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   }
   __syncthreads();
 
-  // Tile loop without CTA barriers.  Visit t sits in buffer t % kTileBufs; each warp
-  // waits for its copy, reads its split of the pairs, publishes its list top
-  // in tau_share and counts itself out of the tile.  The warp that counts
-  // out last knows every warp is done with the buffer: it re-arms the counter
-  // and decides (and issues) visit t + kTileBufs into the same buffer.  A warp
-  // does that duty before it starts its next tile, so the decision for
-  // t + kTileBufs - 1 is complete before any warp can be last for tile t:
-  // decisions stay in order.
+  // Tile loop without CTA barriers.  Visit t sits in buffer t % kTileBufs;
+  // each warp waits for its copy, evaluates the tile for its queries that
+  // need it, publishes its thresholds and counts itself out of the tile.
+  // The warp that counts out last knows every warp is done with the
+  // buffer: it re-arms the counter and decides (and issues) visit
+  // t + kTileBufs into the same buffer.  A warp does that duty before it
+  // starts its next tile, so the decision for t + kTileBufs - 1 is complete
+  // before any warp can be last for tile t: decisions stay in order.
   int t = 0;
   for (;; ++t) {
     const int buf = t % kTileBufs;
@@ -689,69 +631,88 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
       break;
     }
     if (*s_abort || t >= *s_final) break;
-    const float4* tp = reinterpret_cast<const float4*>(regA + buf * kTileBytes) + split * PPS * 8;
-    // Per-warp culling: the CTA visits a tile when it may matter to any of
-    // its query groups; a warp whose own query box bounds every key of the
-    // tile above all of its lanes' thresholds skips it (it could add no
-    // candidate: keys above a lane's threshold are dropped anyway).
-    bool run = true;
-    if (G < 4) {
-      const float lbw = tile_lower_bound(tinfo_b + (int64_t)lbt[t] * 8, qbox + warp * 6, qbox + warp * 6 + 3);
-      float tw = valid ? tau : -INFINITY;
+    const float2* tile = reinterpret_cast<const float2*>(ring + buf * kSearchTileBytes);
+    // queries of this warp the tile may matter to: bound against the query
+    // point itself not above its threshold
+    const float lbq = tile_lower_bound(tinfo_b + (int64_t)lbt[t] * 8, qpt, qpt);
+    const unsigned need = __ballot_sync(FULL, valid && !(lbq > tau));
+    if (need) {
+#pragma unroll 1
+      for (int h = 0; h < 2; ++h) {
+        float2 pr[kRecLen];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) tw = fmaxf(tw, __shfl_xor_sync(0xffffffffu, tw, o));
-      run = !(lbw > tw);
-    }
-#pragma unroll 2
-    for (int m = 0; run && m < PPS; ++m) {
-      float2 pr[16];
+        for (int f = 0; f < kRecLen; ++f) pr[f] = tile[f * PPT + h * 32 + lane];
+        const int i0 = __float_as_int(pr[kRecPad].x), i1 = __float_as_int(pr[kRecPad].y);
+        const unsigned lt_mask = (1u << lane) - 1u;
+        unsigned rem = need;
+        while (rem) {
+          const int j0 = __ffs(rem) - 1;
+          rem &= rem - 1;
+          const bool two = rem != 0;
+          const int j1 = two ? __ffs(rem) - 1 : j0;
+          if (two) rem &= rem - 1;
+          const float4 q0 = qtab[warp * 32 + j0], q1 = qtab[warp * 32 + j1];
+          const float2 s0 = key_pair(make_float2(q0.x, q0.x), make_float2(q0.y, q0.y), make_float2(q0.z, q0.z), pr);
+          const float2 s1 = key_pair(make_float2(q1.x, q1.x), make_float2(q1.y, q1.y), make_float2(q1.z, q1.z), pr);
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const float4 v = tp[m * 8 + u];
-        pr[2 * u] = make_float2(v.x, v.y);
-        pr[2 * u + 1] = make_float2(v.z, v.w);
+          for (int u = 0; u < 2; ++u) {
+            if (u == 1 && !two) break;
+            const int j = u ? j1 : j0;
+            const float th = u ? q1.w : q0.w;
+            const float2 s2 = u ? s1 : s0;
+            const bool c0 = s2.x <= th, c1 = s2.y <= th;
+            const unsigned b0 = __ballot_sync(FULL, c0), b1 = __ballot_sync(FULL, c1);
+            if (b0 | b1) {
+              const int n = __popc(b0) + __popc(b1);
+              int c = __shfl_sync(FULL, my_cnt, j);
+              if (c + n > kQCap) {  // the queue of query j would overflow: fold every queue first
+                __syncwarp();
+                drain_queue<L>(keys, vals, tie_key, tau, my_cnt, qk, qv, lane);
+                my_cnt = 0;
+                qtab[warp * 32 + lane].w = tau;
+                __syncwarp();
+                c = 0;
+              }
+              if (c0) {
+                const int s = queue_slot(j, c + __popc(b0 & lt_mask));
+                qk[s] = s2.x;
+                qv[s] = i0;
+              }
+              if (c1) {
+                const int s = queue_slot(j, c + __popc(b0) + __popc(b1 & lt_mask));
+                qk[s] = s2.y;
+                qv[s] = i1;
+              }
+              if (lane == j) my_cnt = c + n;
+            }
+          }
+        }
+        __syncwarp();
+        drain_queue<L>(keys, vals, tie_key, tau, my_cnt, qk, qv, lane);
+        my_cnt = 0;
+        qtab[warp * 32 + lane].w = tau;
+        __syncwarp();
       }
-      const float2 s2 = key_pair(qx2, qy2, qz2, pr);
-      if (s2.x <= tau) {
-        qk[qn * kSearchThreads + tid] = s2.x;
-        qv[qn * kSearchThreads + tid] = __float_as_int(pr[kRecPad].x);
-        ++qn;
-      }
-      if (s2.y <= tau) {
-        qk[qn * kSearchThreads + tid] = s2.y;
-        qv[qn * kSearchThreads + tid] = __float_as_int(pr[kRecPad].y);
-        ++qn;
-      }
-      if (__any_sync(0xffffffffu, qn > kQueueCap - 2)) flush_queue<L>(keys, vals, qn, tie_key, tau, qk, qv, tid);
-    }
-    flush_queue<L>(keys, vals, qn, tie_key, tau, qk, qv, tid);
-    tau_share[split * QPC + lq] = keys[L - 1];
-    if (G > 1) {
-      float cth = keys[0];  // keys[cslot] without a dynamic register index
-#pragma unroll
-      for (int s = 1; s < L; ++s) cth = (s == cslot) ? keys[s] : cth;
-      cth_share[split * QPC + lq] = cth;
     }
     // count this warp out of the tile (release: its reads of the buffer and
-    // its bound writes come first)
+    // its threshold writes come first)
     __syncwarp();
     int last = 0;
     if (lane == 0) {
       __threadfence_block();
-      last = atomicAdd(&cnt[buf], 1) == kSearchThreads / 32 - 1;
+      last = atomicAdd(&cnt[buf], 1) == WPC - 1;
       if (last) __threadfence_block();
     }
-    last = __shfl_sync(0xffffffffu, last, 0);
-    tau = fminf(tau, query_bound<G, QPC>(tau_share, cth_share, lq));
+    last = __shfl_sync(FULL, last, 0);
     if (last) {
       // every warp is done with this buffer: re-arm its counter, then decide
       // visit t + kTileBufs unless a stop was made; a tile is needed while
-      // its bound is below some query's bound
+      // its bound is below some query's threshold
       float tmax = -INFINITY;
 #pragma unroll
-      for (int i = lane; i < QPC; i += 32) tmax = fmaxf(tmax, query_bound<G, QPC>(tau_share, cth_share, i));
+      for (int i = lane; i < NT; i += 32) tmax = fmaxf(tmax, qtab[i].w);
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) tmax = fmaxf(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
+      for (int o = 16; o > 0; o >>= 1) tmax = fmaxf(tmax, __shfl_xor_sync(FULL, tmax, o));
       if (lane == 0) {
         cnt[buf] = 0;
         if (*s_final == 0x7fffffff && !*s_abort) {
@@ -783,34 +744,17 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     for (int b = 0; b < kTileBufs; ++b) uses[b] += n > b ? (n - b + kTileBufs - 1) / kTileBufs : 0;
   }
 
-  // ---- merge the G split lists; region A is free (no copy in flight, all
-  // tile reads ended before the last barrier).
-  float fl_tie = tie_key;
-  if (G > 1) {
-    const int slot = split * QPC + lq;
+  // ---- flags and staging; the queue region is free (every drain ended
+  // before the last barrier)
 #pragma unroll
-    for (int s = 0; s < L; ++s) {
-      mk[slot * L + s] = keys[s];
-      mv[slot * L + s] = vals[s];
-    }
-    mf[slot] = tie_key;
-    __syncthreads();
-    if (split == 0) {
-#pragma unroll
-      for (int g = 0; g < G; ++g) fl_tie = fminf(fl_tie, mf[g * QPC + lq]);
-      merge_splits<G, L>(mk, mv, QPC, lq, KMAX - K, K + 1, out_k + lq * L, out_i + lq * L);
-    }
-  } else {
-#pragma unroll
-    for (int s = 0; s < L; ++s) {
-      const int j = s - (KMAX - K);
-      if (j >= 0) {
-        out_k[lq * L + j] = keys[s];
-        out_i[lq * L + j] = vals[s];
-      }
+  for (int s = 0; s < L; ++s) {
+    const int j = s - (KMAX - K);
+    if (j >= 0) {
+      out_k[lq * L + j] = keys[s];
+      out_i[lq * L + j] = vals[s];
     }
   }
-  if (split == 0) {
+  {
     const int nneed = (P > K) ? K + 1 : K;
     bool fl = nan_fill, bad = false;
     for (int j = 0; j < nneed; ++j) {
@@ -822,7 +766,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     for (int j = 0; j + 1 < nneed; ++j)
       if (out_k[lq * L + j] == out_k[lq * L + j + 1]) fl = true;
     const float m = (P > K) ? out_k[lq * L + K] : INFINITY;
-    if (fl_tie <= m) fl = true;
+    if (tie_key <= m) fl = true;
     for (int j = 0; j < K; ++j) out_w[lq * L + j] = weight_of(out_k[lq * L + j]);
     out_f[lq] = (fl || bad || !valid) ? 1 : 0;
     if (valid && fl && !bad) {
@@ -835,7 +779,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   // ---- epilogue: dists / idxs / w_out, then f_out = sum_k w_k f[idx_k]
   // accumulated in k order with fma, 128-bit gathers of f rows.  Rows go to
   // the queries' original positions.
-  for (int x = tid; x < QPC * K; x += kSearchThreads) {
+  for (int x = tid; x < NT * K; x += NT) {
     const int l = x / K, k = x - l * K;
     if (out_f[l]) continue;
     const int64_t e = (int64_t)qorig[l] * K + k;
@@ -847,13 +791,12 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   const float* fb = it.f;
   if (a.vec4) {
     const int C4 = F >> 2;
-    for (int x = tid; x < QPC * C4; x += kSearchThreads) {
+    for (int x = tid; x < NT * C4; x += NT) {
       const int l = x / C4, c = x - l * C4;
       if (out_f[l]) continue;
       float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-      // KMAX <= 16: eight rows in flight, summed in k order (the KMAX = 32
-      // kernels, at 128 registers, run the plain loop: measured faster there)
-      constexpr int RB = KMAX <= 16 ? 8 : 1;
+      // eight rows in flight, summed in k order
+      constexpr int RB = 8;
       for (int k0 = 0; k0 < K; k0 += RB) {
         float4 v[RB];
         float w[RB];
@@ -877,7 +820,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
       reinterpret_cast<float4*>(it.f_out + (int64_t)qorig[l] * F)[c] = acc;
     }
   } else {
-    for (int x = tid; x < QPC * F; x += kSearchThreads) {
+    for (int x = tid; x < NT * F; x += NT) {
       const int l = x / F, c = x - l * F;
       if (out_f[l]) continue;
       float acc = 0.f;
@@ -889,10 +832,10 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   return true;
 }
 
-template <int KMAX, int G>
-__global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f32_kernel(SearchParams a) {
+template <int KMAX, int WPC>
+__global__ void __launch_bounds__(32 * WPC) search_f32_kernel(SearchParams a) {
   extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t* full = search_barriers(smem, search_region_a_bytes(KMAX, G));
+  uint64_t* full = search_barriers<WPC>(smem);
   if (threadIdx.x == 0) {
     for (int b = 0; b < kTileBufs; ++b) mbar_init(&full[b], 1);
     fence_mbar_init();
@@ -917,19 +860,21 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_f
   it.ntile = a.ntile;
   it.qblock = blockIdx.x;
   uint32_t uses[kTileBufs] = {};
-  search_item<KMAX, G>(a, it, smem, search_tiles_pow2(a.ntile), uses);
+  search_item<KMAX, WPC>(a, it, smem, search_tiles_pow2(a.ntile), uses);
 }
 
 // Ragged search: a persistent CTA takes work items in order from a counter
 // until the segment table's items run out.  Item i belongs to the last
 // segment whose item_off <= i; its queries are that segment's sorted
-// positions [(i - item_off) * QPC, ...).
-template <int KMAX, int G>
-__global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_ragged_kernel(SearchParams a) {
+// positions [(i - item_off) * 32 * WPC, ...).  Each item runs with the
+// register list of its own segment's K (8, 16 or 32 slots + 1), up to the
+// launch's KMAX.
+template <int KMAX, int WPC>
+__global__ void __launch_bounds__(32 * WPC) search_ragged_kernel(SearchParams a) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ int s_item;
   if (*a.status) return;  // the table failed validation
-  uint64_t* full = search_barriers(smem, search_region_a_bytes(KMAX, G));
+  uint64_t* full = search_barriers<WPC>(smem);
   if (threadIdx.x == 0) {
     for (int b = 0; b < kTileBufs; ++b) mbar_init(&full[b], 1);
     fence_mbar_init();
@@ -944,7 +889,7 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_r
   const float* ctinfo = reinterpret_cast<const float*>(a.cs + ch->tinfo_off);
   const int nseg = sh->nseg, n_items = sh->n_items;
   const int ntp_cap = search_tiles_pow2(a.ntile);
-  constexpr int QPC = 32 * (4 / G);
+  constexpr int QPC = 32 * WPC;
   uint32_t uses[kTileBufs] = {};
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(a.item_counter, 1);
@@ -977,7 +922,14 @@ __global__ void __launch_bounds__(kSearchThreads, (KMAX <= 16 ? 6 : 4)) search_r
       it.K = g.K;
       it.ntile = c.ntile;
       it.qblock = item - g.item_off;
-      if (!search_item<KMAX, G>(a, it, smem, ntp_cap, uses)) break;
+      bool ok;
+      if (KMAX > 8 && g.K <= 8)
+        ok = search_item<8, WPC>(a, it, smem, ntp_cap, uses);
+      else if (KMAX > 16 && g.K <= 16)
+        ok = search_item<(KMAX > 16 ? 16 : KMAX), WPC>(a, it, smem, ntp_cap, uses);
+      else
+        ok = search_item<KMAX, WPC>(a, it, smem, ntp_cap, uses);
+      if (!ok) break;
     }
     __syncthreads();  // the next item reuses shared memory (and s_item)
   }
@@ -998,43 +950,43 @@ int num_sms(int dev) {
   return cache[dev];
 }
 
-template <int KMAX, int G>
+template <int KMAX, int WPC>
 int launch_search_t(const SearchParams& a, cudaStream_t st) {
-  const size_t smem = search_smem_bytes(KMAX, G) + search_region_c_bytes(a.ntile, G);
+  const size_t smem = search_smem_bytes(WPC) + search_region_c_bytes(a.ntile);
   if (smem > 227 * 1024) return KNNAG_ERR_TOO_LARGE;
   static int attr_set[64] = {0};  // largest size already allowed, per device
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 0 && dev < 64 && attr_set[dev] < (int)smem) {
-    if (cudaFuncSetAttribute(search_f32_kernel<KMAX, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+    if (cudaFuncSetAttribute(search_f32_kernel<KMAX, WPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
       return KNNAG_ERR_CUDA;
     attr_set[dev] = (int)smem;
   }
-  constexpr int QPC = 32 * (4 / G);
+  constexpr int QPC = 32 * WPC;
   dim3 grid((a.Q + QPC - 1) / QPC, a.B);
   profile_begin(st);
-  search_f32_kernel<KMAX, G><<<grid, kSearchThreads, smem, st>>>(a);
+  search_f32_kernel<KMAX, WPC><<<grid, 32 * WPC, smem, st>>>(a);
   profile_end(st);
   note_launches(1);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 
-template <int KMAX, int G>
+template <int KMAX, int WPC>
 int launch_search_ragged_t(const SearchParams& a, int64_t cap_items, cudaStream_t st) {
-  const size_t smem = search_smem_bytes(KMAX, G) + search_region_c_bytes(a.ntile, G);
+  const size_t smem = search_smem_bytes(WPC) + search_region_c_bytes(a.ntile);
   if (smem > 227 * 1024) return KNNAG_ERR_TOO_LARGE;
   int dev = 0;
   cudaGetDevice(&dev);
   static int attr_set[64] = {0};
   if (dev >= 0 && dev < 64 && attr_set[dev] < (int)smem) {
-    if (cudaFuncSetAttribute(search_ragged_kernel<KMAX, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(search_ragged_kernel<KMAX, WPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem) != cudaSuccess)
       return KNNAG_ERR_CUDA;
     attr_set[dev] = (int)smem;
   }
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_ragged_kernel<KMAX, G>, kSearchThreads, smem) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_ragged_kernel<KMAX, WPC>, 32 * WPC, smem) !=
           cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
@@ -1042,24 +994,25 @@ int launch_search_ragged_t(const SearchParams& a, int64_t cap_items, cudaStream_
   if (grid > cap_items) grid = cap_items;
   if (grid < 1) grid = 1;
   profile_begin(st);
-  search_ragged_kernel<KMAX, G><<<(unsigned)grid, kSearchThreads, smem, st>>>(a);
+  search_ragged_kernel<KMAX, WPC><<<(unsigned)grid, 32 * WPC, smem, st>>>(a);
   profile_end(st);
   note_launches(1);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 
+// splits s (1, 2, 4) -> WPC = 4 / s warps (128 / s queries) per CTA
 template <int KMAX>
 int launch_search_ragged_k(const SearchParams& a, int G, int64_t cap_items, cudaStream_t st) {
-  if (G == 1) return launch_search_ragged_t<KMAX, 1>(a, cap_items, st);
+  if (G == 1) return launch_search_ragged_t<KMAX, 4>(a, cap_items, st);
   if (G == 2) return launch_search_ragged_t<KMAX, 2>(a, cap_items, st);
-  return launch_search_ragged_t<KMAX, 4>(a, cap_items, st);
+  return launch_search_ragged_t<KMAX, 1>(a, cap_items, st);
 }
 
 template <int KMAX>
 int launch_search_k(const SearchParams& a, int G, cudaStream_t st) {
-  if (G == 1) return launch_search_t<KMAX, 1>(a, st);
+  if (G == 1) return launch_search_t<KMAX, 4>(a, st);
   if (G == 2) return launch_search_t<KMAX, 2>(a, st);
-  return launch_search_t<KMAX, 4>(a, st);
+  return launch_search_t<KMAX, 1>(a, st);
 }
 
 // Splits per query group: the process-wide setting when one is made

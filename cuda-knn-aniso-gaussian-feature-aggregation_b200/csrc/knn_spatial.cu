@@ -222,9 +222,11 @@ __device__ double sym3_min_eig(double a00, double a11, double a22, double a01, d
 }
 
 // One CTA of 128 threads per search tile (tile blockIdx.x of group
-// blockIdx.y), one sorted point per thread: packs the tile in the
-// pair-interleaved layout (field kRecPad carries the original point index,
-// -1 for padding, whose sigma is NaN so its key is never a candidate) and
+// blockIdx.y), one sorted point per thread: packs the tile field-major --
+// field f of point pair m (points 2m, 2m+1) at float2 f * 64 + m, so a lane
+// reads its pair's 16 fields conflict-free and one packed f32x2 evaluation
+// gives both keys -- (field kRecPad carries the original point index, -1
+// for padding, whose sigma is NaN so its key is never a candidate) and
 // writes tinfo[tile*8] = {min xyz, max xyz, mu, 0}.
 __global__ void __launch_bounds__(kTilePoints) tile_info_kernel(const float* __restrict__ rec,
                                                                 const int* __restrict__ perm,
@@ -241,19 +243,19 @@ __global__ void __launch_bounds__(kTilePoints) tile_info_kernel(const float* __r
   float mu = INFINITY;
   bool bad = false;
   const int pos = t * kTilePoints + k;
-  float* slot = tile + (k >> 1) * kPairFloats + (k & 1);  // field f at slot[2 f]
+  float* slot = tile + k;  // field f of point k at slot[f * kTilePoints]
   if (pos >= g.P) {
 #pragma unroll
     for (int m = 0; m < kRecLen; ++m)
-      slot[2 * m] = m == kRecPad ? __int_as_float(-1)
-                                 : ((m == kS0 || m == kS1 || m == kS2) ? __int_as_float(0x7fc00000) : 0.0f);
+      slot[m * kTilePoints] = m == kRecPad ? __int_as_float(-1)
+                                           : ((m == kS0 || m == kS1 || m == kS2) ? __int_as_float(0x7fc00000) : 0.0f);
   } else {
     const int idx = perm[g.p0 + pos];
     const float* r = rec + (g.p0 + idx) * kRecLen;
     float v[kRecLen];
     load_rec(r, v);
 #pragma unroll
-    for (int m = 0; m < kRecLen; ++m) slot[2 * m] = m == kRecPad ? __int_as_float(idx) : v[m];
+    for (int m = 0; m < kRecLen; ++m) slot[m * kTilePoints] = m == kRecPad ? __int_as_float(idx) : v[m];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       const float c = -v[kNPX + a];
