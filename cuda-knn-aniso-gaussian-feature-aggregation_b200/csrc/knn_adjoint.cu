@@ -354,6 +354,7 @@ int launch_exclusive_scan(int* count, int n, int* out, cudaStream_t st) {
 }
 
 int launch_build_adjacency(const int64_t* idxs, int B, int Q, int P, int K, void* adjacency, cudaStream_t st) {
+  NvtxRange range("knnag:adjacency");
   const AdjLayout L = adj_layout(B, Q, P, K);
   char* base = static_cast<char*>(adjacency);
   int* rowptr = reinterpret_cast<int*>(base + L.rowptr);
@@ -654,13 +655,13 @@ __global__ void __launch_bounds__(256, 3) query_order1_kernel(QueryParams<T> a) 
 // Second order without dgfo and with K <= 16 (the Eikonal step): half a
 // warp per query, one neighbour per lane, so a warp serves two queries.
 template <typename T>
-__device__ __forceinline__ void query_order2_half(const QueryParams<T>& a) {
+__device__ __forceinline__ void query_order2_half(const QueryParams<T>& a, int64_t blk, int64_t nblk) {
   const int lane = threadIdx.x & 31;
   const int sub = lane >> 4, k = lane & 15;
   const int64_t BQ = (int64_t)a.B * a.Q;
   const int K = a.K, P = a.P;
-  const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = (gridDim.x * (int64_t)blockDim.x) >> 5;
+  const int64_t gw = (blk * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = (nblk * (int64_t)blockDim.x) >> 5;
   for (int64_t base = gw * 2; base < BQ; base += nw * 2) {
     const int64_t bq = base + sub;
     T acc[3] = {T(0), T(0), T(0)};
@@ -706,15 +707,15 @@ __device__ __forceinline__ void query_order2_half(const QueryParams<T>& a) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) query_order2_kernel(QueryParams<T> a) {
+__device__ __forceinline__ void query_order2_body(const QueryParams<T>& a, int blk, int nblk) {
   if (!a.dgfo && a.K <= 16) {
-    query_order2_half(a);
+    query_order2_half(a, blk, nblk);
     return;
   }
   const int lane = threadIdx.x & 31;
   const int BQ = a.B * a.Q, K = a.K, F = a.F, P = a.P;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int gw = (blk * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (nblk * blockDim.x) >> 5;
   for (int bq = gw; bq < BQ; bq += nw) {
     const int b = bq / a.Q;
     const T qx = a.q[(int64_t)bq * 3 + 0], qy = a.q[(int64_t)bq * 3 + 1], qz = a.q[(int64_t)bq * 3 + 2];
@@ -791,6 +792,11 @@ __global__ void __launch_bounds__(256) query_order2_kernel(QueryParams<T> a) {
   }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) query_order2_kernel(QueryParams<T> a) {
+  query_order2_body(a, blockIdx.x, gridDim.x);
+}
+
 // One warp per point row.  Lane j takes entry j of each 32-entry chunk of
 // the row for the per-entry geometry (15 point-side scalars, reduced over
 // the warp at the end); for df the warp then walks the chunk four entries at
@@ -798,10 +804,10 @@ __global__ void __launch_bounds__(256) query_order2_kernel(QueryParams<T> a) {
 // rows, four rows in flight).  The entry order of a row is fixed (sorted),
 // so every sum has a fixed order.
 template <typename T, int ORDER, int NCOL>
-__global__ void __launch_bounds__(256, 4) point_side_kernel(PointParams<T> a) {
+__device__ __forceinline__ void point_side_body(const PointParams<T>& a, int blk, int nblk) {
   const int lane = threadIdx.x & 31;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const int gw = (blk * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (nblk * blockDim.x) >> 5;
   const int rows = a.B * a.P;
   const int F = a.F, K = a.K;
   const int n_entries = a.B * a.Q * K;
@@ -939,6 +945,23 @@ __global__ void __launch_bounds__(256, 4) point_side_kernel(PointParams<T> a) {
   }
 }
 
+template <typename T, int ORDER, int NCOL>
+__global__ void __launch_bounds__(256, 4) point_side_kernel(PointParams<T> a) {
+  point_side_body<T, ORDER, NCOL>(a, blockIdx.x, gridDim.x);
+}
+
+// The second-order query side and point side in one launch: they read the
+// same inputs (ggq, coef, records) and write disjoint outputs, so the first
+// q_blocks CTAs run the query side and the rest the point side, side by side
+// instead of one after the other.
+template <typename T, int NCOL>
+__global__ void __launch_bounds__(256, 3) order2_fused_kernel(QueryParams<T> qa, PointParams<T> pa, int q_blocks) {
+  if ((int)blockIdx.x < q_blocks)
+    query_order2_body(qa, blockIdx.x, q_blocks);
+  else
+    point_side_body<T, 2, NCOL>(pa, blockIdx.x - q_blocks, gridDim.x - q_blocks);
+}
+
 // ------------------------------------------------------------------ host
 
 BwdLayout bwd_layout(int B, int Q, int P, int F, int K, int dtype) {
@@ -963,6 +986,7 @@ namespace {
 
 template <typename T>
 int launch_query(const QueryParams<T>& p, int order, cudaStream_t st) {
+  NvtxRange range("knnag:query_side");
   const int64_t warps = (int64_t)p.B * p.Q;
   const unsigned grid = blocks_for(warps * 32, 256);
   if (order == 1)
@@ -1024,7 +1048,25 @@ int launch_point_o(const PointParams<T>& p, cudaStream_t st) {
 }
 
 template <typename T>
+int launch_order2_fused(const QueryParams<T>& qa, const PointParams<T>& pa, cudaStream_t st) {
+  const unsigned qb = blocks_for((int64_t)qa.B * qa.Q * 32, 256);
+  const unsigned pb = blocks_for((int64_t)pa.B * pa.P * 32, 256);
+  const unsigned grid = qb + pb;
+  if (pa.F <= 32)
+    order2_fused_kernel<T, 1><<<grid, 256, 0, st>>>(qa, pa, (int)qb);
+  else if (pa.F <= 64)
+    order2_fused_kernel<T, 2><<<grid, 256, 0, st>>>(qa, pa, (int)qb);
+  else if (pa.F <= 128)
+    order2_fused_kernel<T, 4><<<grid, 256, 0, st>>>(qa, pa, (int)qb);
+  else
+    order2_fused_kernel<T, 8><<<grid, 256, 0, st>>>(qa, pa, (int)qb);
+  note_launches(1);
+  return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
+}
+
+template <typename T>
 int backward_t(const BwdArgs& x, cudaStream_t st) {
+  NvtxRange range(x.order == 1 ? "knnag:backward" : "knnag:backward_2nd");
   const BwdLayout L = bwd_layout(x.B, x.Q, x.P, x.F, x.K, x.dtype);
   char* ws = static_cast<char*>(x.workspace);
   int rc = KNNAG_OK;
@@ -1047,6 +1089,7 @@ int backward_t(const BwdArgs& x, cudaStream_t st) {
   const bool gfo_scalar = (x.needs & KNNAG_GFO_SCALAR) != 0;
   T* rowsum = reinterpret_cast<T*>(ws + L.rowsum);
   bool rowsum_ready = false;
+  bool query2_pending = false;
   // per-point column sums of f, for the query side with a broadcast grad_f_out
   auto ensure_rowsum = [&]() -> int {
     if (rowsum_ready) return KNNAG_OK;
@@ -1101,12 +1144,12 @@ int backward_t(const BwdArgs& x, cudaStream_t st) {
       qp.coef_in = coef;
       qp.dq = (x.needs & KNNAG_NEED_DQ) ? (T*)x.dq : nullptr;
       qp.dgfo = (x.needs & KNNAG_NEED_DGFO) ? (T*)x.dgfo : nullptr;
-      rc = launch_query<T>(qp, 2, st);
-      if (rc) return rc;
+      query2_pending = true;  // launched with the point side when that runs too
     }
   }
 
   if (x.needs & point_bits) {
+    NvtxRange r("knnag:point_side");
     const void* adj = x.adjacency;
     if (!adj) {
       rc = launch_build_adjacency(x.idxs, x.B, x.Q, x.P, x.K, ws + L.adj, st);
@@ -1134,8 +1177,15 @@ int backward_t(const BwdArgs& x, cudaStream_t st) {
     pp.dsigma = (T*)x.dsigma;
     pp.dR = (T*)x.dR;
     pp.gfo_scalar = gfo_scalar;
+    if (query2_pending && sizeof(T) == 4) {  // FP64 keeps separate launches (the fused one spills)
+      NvtxRange r2("knnag:query_side");
+      return launch_order2_fused<T>(qp, pp, st);
+    }
+    if (query2_pending && (rc = launch_query<T>(qp, 2, st))) return rc;
     rc = (x.order == 1) ? launch_point_o<T, 1>(pp, st) : launch_point_o<T, 2>(pp, st);
+    return rc;
   }
+  if (query2_pending) rc = launch_query<T>(qp, 2, st);
   return rc;
 }
 

@@ -3,12 +3,23 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stddef.h>
 #include <stdint.h>
 
 #include "knn_ragged.h"
 
 namespace knnag {
+
+// NVTX range over one host-side stage of a call (the kernels it enqueues
+// show up under it in a timeline profiler; without one attached the push
+// and pop are no-ops).  Names start with "knnag:".
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 template <typename T>
 struct ExactParams {

@@ -1128,6 +1128,7 @@ static int forward_exact_all(const T* q, const T* rec, const T* f, int B, int Q,
 int forward_impl(const void* q, const void* p, const void* f, const void* sigma, const void* R, int B, int Q,
                  int P, int F, int K, int dtype, void* f_out, void* w_out, void* dists, int64_t* idxs,
                  void* points, void* workspace, cudaStream_t st) {
+  NvtxRange range("knnag:forward");
   const bool own_rec = points == nullptr;
   const FwdLayout L = fwd_layout(B, Q, P, K, dtype, own_rec);
   char* ws = static_cast<char*>(workspace);
@@ -1135,7 +1136,11 @@ int forward_impl(const void* q, const void* p, const void* f, const void* sigma,
   int* flag_count = status + 1;
   int* flag_list = reinterpret_cast<int*>(ws + L.flag_list);
   void* rec = own_rec ? (void*)(ws + L.rec) : points;
-  int rc = launch_pack_points(p, sigma, R, B, P, dtype, rec, st, status, 2);  // also zeroes status, flag_count
+  int rc;
+  {
+    NvtxRange r("knnag:pack_points");
+    rc = launch_pack_points(p, sigma, R, B, P, dtype, rec, st, status, 2);  // also zeroes status, flag_count
+  }
   if (rc) return rc;
   if (dtype == KNNAG_F64)
     return forward_exact_all<double>((const double*)q, (const double*)rec, (const double*)f, B, Q, P, F, K,
@@ -1146,7 +1151,10 @@ int forward_impl(const void* q, const void* p, const void* f, const void* sigma,
   int dev = 0;
   cudaGetDevice(&dev);
   float* pairs = reinterpret_cast<float*>(ws + L.pairs);
-  rc = launch_spatial_index((const float*)q, (const float*)rec, B, Q, P, L.P_pad, ws, L, st);
+  {
+    NvtxRange r("knnag:spatial_index");
+    rc = launch_spatial_index((const float*)q, (const float*)rec, B, Q, P, L.P_pad, ws, L, st);
+  }
   if (rc) return rc;
   SearchParams sp{};
   sp.q = (const float*)q;
@@ -1172,14 +1180,18 @@ int forward_impl(const void* q, const void* p, const void* f, const void* sigma,
   sp.flag_list = flag_list;
   apply_search_debug(sp);
   const int G = choose_splits(B, Q, dev);
-  if (K <= 8)
-    rc = launch_search_k<8>(sp, G, st);
-  else if (K <= 16)
-    rc = launch_search_k<16>(sp, G, st);
-  else
-    rc = launch_search_k<32>(sp, G, st);
+  {
+    NvtxRange r("knnag:search");
+    if (K <= 8)
+      rc = launch_search_k<8>(sp, G, st);
+    else if (K <= 16)
+      rc = launch_search_k<16>(sp, G, st);
+    else
+      rc = launch_search_k<32>(sp, G, st);
+  }
   if (rc) return rc;
   // Exact MinK replay of the flagged queries (count read on the device).
+  NvtxRange r("knnag:replay_flagged");
   ExactParams<float> e{(const float*)q, (const float*)rec, (const float*)f, nullptr, nullptr, 0, B, Q, P, F, K, 1,
                        flag_list, flag_count, (float*)f_out, (float*)w_out, (float*)dists, idxs};
   return launch_exact<float>(e, st);
@@ -1209,6 +1221,7 @@ RaggedLayout ragged_layout(int cap_segs, int64_t cap_q) {
 int ragged_forward_impl(const char* cs, const void* segs, const float* q, const float* f, int F, int cap_segs,
                         int64_t cap_q, int64_t cap_e, int max_k, int ntile_cap, int splits, float* f_out, float* w_out,
                         float* dists, int64_t* idxs, void* workspace, cudaStream_t st) {
+  NvtxRange range("knnag:ragged_forward");
   const RaggedLayout L = ragged_layout(cap_segs, cap_q);
   char* ws = static_cast<char*>(workspace);
   int* status = reinterpret_cast<int*>(ws + L.status);
