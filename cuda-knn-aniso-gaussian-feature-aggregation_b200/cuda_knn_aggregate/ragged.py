@@ -251,8 +251,6 @@ def ragged_forward(cloudset: CloudSet, q, clouds, Qs, Ks, splits=None, grad_q=No
 
 # ---------------------------------------------------------------- autotuner
 
-_TUNE_CACHE: dict = {}
-
 
 def shape_bucket(cloudset: CloudSet, Qs, Ks):
     """Shape bucket of a ragged step: log2 of the largest cloud, of the step's
@@ -264,13 +262,20 @@ def shape_bucket(cloudset: CloudSet, Qs, Ks):
 
 
 def autotune_splits(cloudset: CloudSet, clouds, qs, Ks, reps=3, cache=True):
-    """Warps per 32-query group (1, 2 or 4) for steps shaped like this one:
-    each candidate runs the step as a captured graph ``reps`` times (after a
-    warm-up) and the fastest median wins.  Cached per ``shape_bucket``."""
+    """Queries per search CTA (128 / splits, splits in 1, 2, 4) for steps
+    shaped like this one: each candidate runs the step as a captured graph
+    ``reps`` times (after a warm-up) and the fastest median wins.  Cached per
+    ``shape_bucket`` in memory and in the tuner's JSON file
+    (``tuning.cache_path()``), so a later process reuses the choice."""
+    from . import tuning
+
     Qs = [int(x.shape[0]) for x in qs]
-    key = shape_bucket(cloudset, Qs, Ks)
-    if cache and key in _TUNE_CACHE:
-        return _TUNE_CACHE[key]
+    bucket = shape_bucket(cloudset, Qs, Ks)
+    dev = cloudset.buf.device
+    if cache:
+        hit = tuning.lookup("ragged", bucket, dev)
+        if hit is not None:
+            return int(hit["splits"])
     times = {}
     for g in _SPLITS:
         ex = RaggedExecutor(cloudset, len(clouds), sum(Qs), max(Ks), splits=g, copy_out=False)
@@ -286,15 +291,18 @@ def autotune_splits(cloudset: CloudSet, clouds, qs, Ks, reps=3, cache=True):
             e1.synchronize()
             ts.append(e0.elapsed_time(e1))
         times[g] = sorted(ts)[len(ts) // 2]
+        tuning.TIMED["runs"] += 1
         del ex
     best = min(times, key=times.get)
-    _TUNE_CACHE[key] = best
+    tuning.record("ragged", bucket, {"splits": best, "ms": {str(g): t for g, t in times.items()}}, dev)
     return best
 
 
 def tune_cache():
-    """The autotuner's choices so far: {shape bucket: splits}."""
-    return dict(_TUNE_CACHE)
+    """The autotuner's choices known to this process (both tuners)."""
+    from . import tuning
+
+    return tuning.tune_cache()
 
 
 class RaggedExecutor:

@@ -10,6 +10,12 @@ for p in (ROOT, PKG_DIR, os.path.join(ROOT, "oracle")):
         sys.path.insert(0, p)
 
 GOLDEN_DIR = os.path.join(ROOT, "tests", "golden")
+
+# the tests' autotuner choices go to a private file, not the user's cache
+if "KNNAG_TUNE_CACHE" not in os.environ:
+    import tempfile
+
+    os.environ["KNNAG_TUNE_CACHE"] = os.path.join(tempfile.mkdtemp(prefix="knnag_tune_"), "tune.json")
 GOLDEN_CASES = ["small", "readme", "ties", "k_eq_p", "k1_f5", "f1", "allkeys"]
 
 

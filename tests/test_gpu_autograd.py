@@ -137,9 +137,10 @@ def test_function_subclass_written_against_the_reference():
 
     shape, t = make(B=2, Q=300, P=400, F=8, K=8, seed=21)
     results = []
-    for op in (C.KNNAnisotropicAggregate.apply, Mine.apply, C.KNNPrecomputedAnisotropicAggregate.apply):
+    for name, op in (("base", C.KNNAnisotropicAggregate.apply), ("subclass", Mine.apply),
+                     ("precomputed", C.KNNPrecomputedAnisotropicAggregate.apply)):
         ins = [x.to(DEV).requires_grad_(True) for x in t]
-        if op is C.KNNPrecomputedAnisotropicAggregate.apply:
+        if name == "precomputed":
             idxs = C.knn_aggregate_aniso(*[x.detach() for x in ins], shape.K)[3]
             f_out = op(*ins, idxs, shape.K)[0]
         else:
