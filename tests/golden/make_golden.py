@@ -103,7 +103,39 @@ def variant_cases():
     out.append(("iso_kp", dict(q=q, p=p, f=f, sigma=sigma[..., :1].contiguous(), K=64)))
     lt = W.lattice_ties(B=1, n_side=4, Q=64, F=4, seed=8)
     out.append(("iso_ties", dict(q=lt[0], p=lt[1], f=lt[2], sigma=lt[3][..., :1].contiguous(), K=8)))
+    q, p, f, sigma, R, table = lookup_ties()
+    out.append(("lookup_ties", dict(q=q, p=p, f=f, sigma=sigma, R=R, knn_table=table, K=6)))
     return out
+
+
+def lookup_ties(n_side=5, seed=607, F=4):
+    """Lookup input whose nearest point depends on how x*x + y*y + z*z is
+    rounded: every query q (a float in [1, 2)^3) has six points q - d for
+    the six permutations d of one offset (a, b, c), each coordinate a
+    multiple of 2^-23, so q - p is exact and the six squared distances are
+    equal in exact arithmetic; their FP32 values differ only by the order
+    of the rounded operations.  The clusters are 0.18 apart, so each
+    query's nearest point is one of its own six."""
+    import itertools
+
+    g = torch.Generator().manual_seed(seed)
+    ax = 1.05 + 0.18 * torch.arange(n_side, dtype=torch.float64)
+    qc = torch.stack(torch.meshgrid(ax, ax, ax, indexing="ij"), -1).reshape(-1, 3)
+    qc = (qc + 0.02 * torch.rand(qc.shape, generator=g, dtype=torch.float64)).float().double()
+    Q = qc.shape[0]
+    k = torch.randint(100000, 160000, (Q, 3), generator=g).double() * 2.0 ** -23
+    offs = torch.stack([k[:, list(pm)] for pm in itertools.permutations(range(3))], 1)
+    pts = (qc[:, None, :] - offs).reshape(-1, 3)
+    pts = pts[torch.randperm(pts.shape[0], generator=g)]
+    P = pts.shape[0]
+    q, p = qc.float()[None].contiguous(), pts.float()[None].contiguous()
+    assert torch.equal(p.double()[0], pts), "points must be exact in FP32"
+    f = torch.rand(1, P, F, generator=g)
+    sigma = (0.05 + 0.15 * torch.rand(1, P, 3, generator=g)).contiguous()
+    R = W.random_rotations(P, g).reshape(1, P, 3, 3).contiguous()
+    d = ((pts[:, None, :] - pts[None, :, :]) ** 2).sum(-1)
+    table = torch.topk(d, 6, dim=-1, largest=False).indices
+    return q, p, f, sigma, R, table
 
 
 def run_variant(ref, name, c):
@@ -113,7 +145,7 @@ def run_variant(ref, name, c):
         o = ref.knn_precomputed_aggregate_aniso_forward(*[dev(c[k]) for k in ("q", "p", "f", "sigma", "R", "knn_idxs")],
                                                         c["K"])
         names = ("f_out", "w_out", "dists")
-    elif name == "lookup":
+    elif name.startswith("lookup"):
         o = ref.knn_lookup_aggregate_aniso_forward(*[dev(c[k]) for k in ("q", "p", "f", "sigma", "R", "knn_table")],
                                                    c["K"])
         names = ("f_out", "w_out", "dists", "idxs")
@@ -130,17 +162,20 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.dirname(os.path.abspath(__file__)))
     ap.add_argument("--only-variants", action="store_true")
+    ap.add_argument("--only", default=None, help="generate this one variant case (e.g. lookup_ties)")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
     ref = load_ref()
     for i, (name, t, K) in enumerate(cases()):
-        if a.only_variants:
+        if a.only_variants or a.only:
             break
         rec = run_case(ref, t, K, seed=500 + i)
         path = os.path.join(a.out, f"ref_{name}.npz")
         np.savez_compressed(path, **rec)
         print(f"{name}: {os.path.getsize(path)} bytes")
     for name, c in variant_cases():
+        if a.only and name != a.only:
+            continue
         rec = run_variant(ref, name, c)
         path = os.path.join(a.out, f"ref_var_{name}.npz")
         np.savez_compressed(path, **rec)
