@@ -46,8 +46,9 @@ def test_oracle_precomputed_vs_reference():
     assert rel_err(fo, z["f_out"]) < FWD_TOL
 
 
-def test_oracle_lookup_vs_reference():
-    z = load("lookup")
+@pytest.mark.parametrize("name", ["lookup", "lookup_ties"])
+def test_oracle_lookup_vs_reference(name):
+    z = load(name)
     fo, w, d, idx = O.lookup_f32(z["q"], z["p"], z["f"], z["sigma"], z["R"], z["knn_table"])
     assert np.array_equal(idx, z["idxs"])
     assert bits_equal(d, z["dists"])
@@ -78,6 +79,20 @@ def test_isotropic_contraction_is_pinned():
             ok &= bits_equal(d, z["dists"])
         hits.append(ok)
     assert hits[O.ISO_SQ_MODE] and sum(hits) == 1
+
+
+def test_lookup_contraction_is_pinned():
+    """lookup_ties is built so that the three roundings of x*x + y*y + z*z
+    pick different nearest points (six points per query at exactly equal
+    squared distances in exact arithmetic): only LOOKUP_SQ_MODE reproduces
+    the reference extension's nearest points, and each other mode differs
+    on some query."""
+    z = load("lookup_ties")
+    hits = []
+    for mode in range(3):
+        _, _, d, idx = O.lookup_f32(z["q"], z["p"], z["f"], z["sigma"], z["R"], z["knn_table"], mode=mode)
+        hits.append(np.array_equal(idx, z["idxs"]) and bits_equal(d, z["dists"]))
+    assert hits[O.LOOKUP_SQ_MODE] and sum(hits) == 1
 
 
 def test_isotropic_ties_fixture_has_ties():
@@ -120,11 +135,12 @@ def test_precomputed_vs_reference_fixture():
 
 
 @pytest.mark.gpu
-def test_lookup_vs_reference_fixture():
+@pytest.mark.parametrize("name", ["lookup", "lookup_ties"])
+def test_lookup_vs_reference_fixture(name):
     import cuda_knn_aggregate as C
     from cuda_knn_aggregate import capi
 
-    z = load("lookup")
+    z = load(name)
     q, p, f, s, R, table = _cuda(z, "q", "p", "f", "sigma", "R", "knn_table")
     K = int(z["K"])
     outs = C.knn_aggregate_aniso_lookup(q, p, f, s, R, table, K)
