@@ -81,37 +81,47 @@ struct SearchParams {
   int wait_spins;
 };
 
-// Search CTA: WPC warps (1, 2 or 4), each owning 32 queries (one per lane)
-// and sharing the CTA's tile ring; a work item is the CTA's 32 * WPC
-// queries.  The C ABI's `splits` setting s (1, 2, 4) selects WPC = 4 / s,
-// i.e. 128 / s queries per work item.
+// Search CTA: WPC warps (1, 2 or 4), each owning QPW queries (32, 16 or 8;
+// lane j < QPW keeps query j's list) and sharing the CTA's tile ring; a work
+// item is the CTA's WPC * QPW queries.  The C ABI's launch-shape code s
+// (knnag_set_search_splits, the segment tables' `splits`) selects
+//   s = 1: 4 warps x 32    s = 2: 2 x 32    s = 4: 1 x 32
+//   s = 8: 2 warps x 16    s = 16: 4 x 8
+// i.e. 128, 64, 32, 32 and 32 queries per CTA.
 constexpr int kSearchMaxThreads = 128;
-// Candidate queue entries per query: one half tile (64 points) always fits.
+// Candidate queue entries per query: 64 points (the points a query meets
+// between two folds of its queue) always fit.
 constexpr int kQCap = 64;
 // Tile buffers of the search ring: visit v lands in buffer v % kTileBufs,
 // so kTileBufs - 1 copies are in flight while a tile is being read.
 constexpr int kTileBufs = 2;
-constexpr size_t kSearchTileBytes = 8192;                  // 128 points x 16 floats
-constexpr size_t kWarpQueueBytes = (size_t)32 * kQCap * 8;  // keys + point indices
+constexpr size_t kSearchTileBytes = 8192;  // 128 points x 16 floats
 static_assert(kTileBufs * 12 + 8 <= 64, "search ring bookkeeping exceeds its 64 bytes");
+__host__ __device__ inline constexpr int search_wpc(int shape) { return shape == 1 ? 4 : shape == 2 ? 2 : shape == 4 ? 1 : shape == 8 ? 2 : 4; }
+__host__ __device__ inline constexpr int search_qpw(int shape) { return shape <= 4 ? 32 : shape == 8 ? 16 : 8; }
+__host__ __device__ inline constexpr int search_qpc(int shape) { return search_wpc(shape) * search_qpw(shape); }
+inline bool search_shape_ok(int shape) { return shape == 1 || shape == 2 || shape == 4 || shape == 8 || shape == 16; }
 
-// Shared-memory layout of the search kernel with `wpc` warps:
+// Shared-memory layout of the search kernel with `wpc` warps of `qpw` queries:
 //   ring      kTileBufs tiles
-//   queues    wpc x [32 queries][kQCap] keys, then indices (after the tile
+//   queues    wpc x [qpw queries][kQCap] keys, then indices (after the tile
 //             loop: the CTA's sorted lists, weights and flags)
-//   qtab      [32 wpc] float4 (x, y, z, threshold) of the CTA's queries
-//   misc      [32 wpc] original query index, [wpc][6] warp query boxes,
+//   qtab      [wpc qpw] float4 (x, y, z, threshold) of the CTA's queries
+//   misc      [wpc qpw] original query index, [wpc][6] warp query boxes,
 //             64 bytes of mbarriers / counters / flags
 //   region C  tile bounds and visit order [NTP x 8 B] + visit counter
 __host__ __device__ inline constexpr size_t search_queue_off() { return (size_t)kTileBufs * kSearchTileBytes; }
-__host__ __device__ inline constexpr size_t search_qtab_off(int wpc) {
-  return search_queue_off() + (size_t)wpc * kWarpQueueBytes;
+__host__ __device__ inline constexpr size_t search_warp_queue_bytes(int qpw) { return (size_t)qpw * kQCap * 8; }
+__host__ __device__ inline constexpr size_t search_qtab_off(int wpc, int qpw) {
+  return search_queue_off() + (size_t)wpc * search_warp_queue_bytes(qpw);
 }
-__host__ __device__ inline constexpr size_t search_misc_off(int wpc) { return search_qtab_off(wpc) + (size_t)wpc * 32 * 16; }
-__host__ __device__ inline constexpr size_t search_bars_off(int wpc) {
-  return search_misc_off(wpc) + (size_t)wpc * 32 * 4 + (size_t)wpc * 6 * 4;
+__host__ __device__ inline constexpr size_t search_misc_off(int wpc, int qpw) {
+  return search_qtab_off(wpc, qpw) + (size_t)wpc * qpw * 16;
 }
-__host__ __device__ inline constexpr size_t search_smem_bytes(int wpc) { return search_bars_off(wpc) + 64; }
+__host__ __device__ inline constexpr size_t search_bars_off(int wpc, int qpw) {
+  return search_misc_off(wpc, qpw) + (size_t)wpc * qpw * 4 + (size_t)wpc * 6 * 4;
+}
+__host__ __device__ inline constexpr size_t search_smem_bytes(int wpc, int qpw) { return search_bars_off(wpc, qpw) + 64; }
 // Tiles per cloud rounded up to a power of two (the visit-order sort).
 __host__ __device__ inline int search_tiles_pow2(int ntile) {
   int n = 1;
@@ -119,9 +129,9 @@ __host__ __device__ inline int search_tiles_pow2(int ntile) {
   return n;
 }
 __host__ __device__ inline size_t search_region_c_bytes(int ntile) { return (size_t)search_tiles_pow2(ntile) * 8 + 16; }
-// The sorted lists of the CTA's queries (keys, indices, weights) staged for
-// the epilogue must fit the queue region.
-static_assert((size_t)32 * 33 * 12 + 32 * 4 <= kWarpQueueBytes, "epilogue staging exceeds the queue region");
+// The sorted lists of a query (keys, indices, weights) and its flag, staged
+// for the epilogue, must fit the query's share of the queue region.
+static_assert((size_t)33 * 12 + 4 <= (size_t)kQCap * 8, "epilogue staging exceeds the queue region");
 
 // ------------------------------------------------------------- workspace
 // Forward workspace: [status, flag_count] | flag_list [B*Q] | records (when

@@ -120,7 +120,7 @@ __global__ void validate_segments_kernel(const char* cs, const void* segs, int c
   if (threadIdx.x == 0 && bad) atomicOr(status, kStatusBadTable);
 }
 
-int qpc_of(int splits) { return (splits == 1 || splits == 2 || splits == 4) ? 32 * (4 / splits) : 0; }
+int qpc_of(int splits) { return search_shape_ok(splits) ? search_qpc(splits) : 0; }
 
 }  // namespace
 

@@ -294,22 +294,24 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
 
 // ------------------------------------------------------- fused FP32 search
 //
-// CTA = WPC warps (1, 2 or 4).  Each warp owns 32 queries -- lane j keeps
-// query j's sorted register list -- and all warps share the CTA's ring of
-// point tiles (128 points, 8 KB, field-major: field f of pair m at float2
-// f * 64 + m), streamed into shared memory by one-dimensional bulk copies
-// (TMA, no multicast), double-buffered on mbarriers.
+// CTA = WPC warps (1, 2 or 4).  Each warp owns QPW queries (32, 16 or 8) --
+// lane j < QPW keeps query j's sorted register list -- and all warps share
+// the CTA's ring of point tiles (128 points, 8 KB, field-major: field f of
+// pair m at float2 f * 64 + m), streamed into shared memory by
+// one-dimensional bulk copies (TMA, no multicast), double-buffered on
+// mbarriers.  Fewer queries per warp give more warps for small query sets.
 //
-// Keys are computed with lanes over POINTS: for each half tile a lane holds
-// one point pair (16 float2 registers) and the warp loops over its queries
-// that the tile may matter to, each broadcast from a shared table
+// Keys are computed with lanes over POINTS: the warp's lanes form 32 / QPW
+// slots of QPW lanes; in one pass a lane holds one point pair (16 float2
+// registers, pair pass * QPW + lane % QPW of the tile) and every slot takes
+// a different query the tile may matter to, broadcast from a shared table
 // (x, y, z, threshold); one packed f32x2 evaluation gives the lane both of
 // its points' keys, so a warp instruction covers 64 (query, point) pairs.
 // Keys at or below the query's threshold are appended (ballot + popc
 // positions) to the query's candidate queue in shared memory, and after
-// every half tile each lane folds its own query's queue into its list.  A
-// query skips a tile whose lower bound against the query point exceeds its
-// threshold.
+// every 64 points of a query each owner lane folds its queue into its
+// list.  A query skips a tile whose lower bound against the query point
+// exceeds its threshold.
 //
 // Selection.  Each list holds the K+1 smallest keys accepted so far in
 // KMAX+1 slots whose lowest KMAX-K slots are -inf sentinels, so the
@@ -367,7 +369,7 @@ __device__ __forceinline__ void drain_queue(float (&keys)[L], int (&vals)[L], fl
   tau = fminf(tau, keys[L - 1]);
 }
 
-// One search work item: up to 32 * WPC queries of one batch element or
+// One search work item: up to WPC * QPW queries of one batch element or
 // segment, all against one cloud.  Pointers are offset to the group already.
 struct SearchItem {
   const float* q;      // query rows (group-local index)
@@ -402,38 +404,44 @@ __device__ __forceinline__ float tile_lower_bound(const float* ti, const float* 
 }
 
 // The tile-ring mbarriers of a search CTA.
-template <int WPC>
+template <int WPC, int QPW>
 __device__ __forceinline__ uint64_t* search_barriers(unsigned char* smem) {
-  return reinterpret_cast<uint64_t*>(smem + search_bars_off(WPC));
+  return reinterpret_cast<uint64_t*>(smem + search_bars_off(WPC, QPW));
 }
 
 // Search + aggregation of one work item.  The mbarriers are initialised by
 // the kernel; uses[buf] counts the phases buffer buf has completed so far
 // (a persistent CTA runs many items on the same barriers).  Returns false
 // when a tile copy timed out (status flagged; the CTA must stop).
-template <int KMAX, int WPC>
+template <int KMAX, int WPC, int QPW>
 __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchItem& it, unsigned char* smem,
                                             int ntp_cap, uint32_t (&uses)[kTileBufs]) {
   constexpr int L = KMAX + 1;
-  constexpr int NT = 32 * WPC;          // threads = queries of the item
+  constexpr int NT = QPW * WPC;         // queries of the item
+  constexpr int NTH = 32 * WPC;         // threads
+  constexpr int H = 32 / QPW;           // lane slots per warp (queries evaluated at once)
   constexpr int PPT = kTilePoints / 2;  // pairs per tile
+  constexpr int NPASS = PPT / QPW;      // passes per tile (QPW pairs each)
   constexpr unsigned FULL = 0xffffffffu;
-  static_assert((size_t)NT * L * 12 + NT * 4 <= (size_t)WPC * kWarpQueueBytes, "epilogue staging");
+  constexpr unsigned SLOT_MASK = QPW == 32 ? 0xffffffffu : ((1u << QPW) - 1u);
+  static_assert(QPW == 32 || QPW == 16 || QPW == 8, "queries per warp");
+  static_assert((size_t)NT * L * 12 + NT * 4 <= (size_t)WPC * search_warp_queue_bytes(QPW), "epilogue staging");
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const bool owner = lane < QPW;       // lane keeps query `lane` of the warp
   unsigned char* ring = smem;
-  float* qk = reinterpret_cast<float*>(smem + search_queue_off() + (size_t)warp * kWarpQueueBytes);
-  int* qv = reinterpret_cast<int*>(qk + 32 * kQCap);
-  float4* qtab = reinterpret_cast<float4*>(smem + search_qtab_off(WPC));  // [NT]
-  int* qorig = reinterpret_cast<int*>(smem + search_misc_off(WPC));       // [NT] original query index (-1: none)
-  float* qbox = reinterpret_cast<float*>(qorig + NT);                     // [WPC][6]
-  uint64_t* full = search_barriers<WPC>(smem);
+  float* qk = reinterpret_cast<float*>(smem + search_queue_off() + (size_t)warp * search_warp_queue_bytes(QPW));
+  int* qv = reinterpret_cast<int*>(qk + QPW * kQCap);
+  float4* qtab = reinterpret_cast<float4*>(smem + search_qtab_off(WPC, QPW));  // [NT]
+  int* qorig = reinterpret_cast<int*>(smem + search_misc_off(WPC, QPW));       // [NT] original query index (-1: none)
+  float* qbox = reinterpret_cast<float*>(qorig + NT);                          // [WPC][6]
+  uint64_t* full = search_barriers<WPC, QPW>(smem);
   int* cnt = reinterpret_cast<int*>(full + kTileBufs);               // warps done per buffer
   volatile int* s_final = reinterpret_cast<volatile int*>(cnt + kTileBufs);  // visit count once stopped
   volatile int* s_abort = s_final + 1;                               // a wait gave up
   // region C: per-tile lower bounds (sorted), visit order, visit counter
   const int NTP = search_tiles_pow2(it.ntile);
-  float* lbk = reinterpret_cast<float*>(smem + search_smem_bytes(WPC));
+  float* lbk = reinterpret_cast<float*>(smem + search_smem_bytes(WPC, QPW));
   int* lbt = reinterpret_cast<int*>(lbk + ntp_cap);
   volatile int* s_nvisit = reinterpret_cast<volatile int*>(lbt + ntp_cap);
   // epilogue views of the queue region (after the tile loop)
@@ -442,9 +450,9 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   float* out_w = reinterpret_cast<float*>(out_i + NT * L);
   int* out_f = reinterpret_cast<int*>(out_w + NT * L);
 
-  const int lq = tid;                   // query of this lane within the item
-  const int sp = it.qblock * NT + lq;   // position in the spatial order
-  bool valid = sp < it.Q;
+  const int lq = warp * QPW + lane;         // query of this (owner) lane within the item
+  const int sp = it.qblock * NT + lq;       // position in the spatial order
+  bool valid = owner && sp < it.Q;
   int qi = it.perm_q[valid ? sp : it.Q - 1];
   if ((unsigned)qi >= (unsigned)it.Q) {  // the query order is a permutation: never taken
     if (valid) atomicOr(a.status, kStatusBadIndex);
@@ -454,20 +462,27 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   const int K = it.K, P = it.P;
   const float qx = it.q[(int64_t)qi * 3 + 0], qy = it.q[(int64_t)qi * 3 + 1], qz = it.q[(int64_t)qi * 3 + 2];
   const float* recb = it.rec;
-  qorig[lq] = valid ? qi : -1;
-  qtab[lq] = make_float4(qx, qy, qz, valid ? INFINITY : -INFINITY);
+  if (owner) {
+    qorig[lq] = valid ? qi : -1;
+    qtab[lq] = make_float4(qx, qy, qz, valid ? INFINITY : -INFINITY);
+  }
 
   // MinK's fill phase stores points 0..K-1 whatever their key: a NaN there
   // changes the result in ways only the replay reproduces.
   bool nan_fill = false;
-  for (int i = 0; i < K; ++i) {
-    const float s = key_rec<float>(qx, qy, qz, recb + (int64_t)i * kRecLen);
-    if (s != s) nan_fill = true;
-  }
+  if (owner)
+    for (int i = 0; i < K; ++i) {
+      const float s = key_rec<float>(qx, qy, qz, recb + (int64_t)i * kRecLen);
+      if (s != s) nan_fill = true;
+    }
 
   // ---- box of this CTA's queries and the tile visit order
   {
     float bx[6] = {qx, qy, qz, qx, qy, qz};
+    if (!owner) {
+      bx[0] = bx[1] = bx[2] = INFINITY;
+      bx[3] = bx[4] = bx[5] = -INFINITY;
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
@@ -522,7 +537,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     }
     __syncthreads();
   } else {
-    for (int t = tid; t < NTP; t += NT) {
+    for (int t = tid; t < NTP; t += NTH) {
       float lb = INFINITY;
       if (t < it.ntile) {
         lb = tile_lower_bound(tinfo_b + t * 8, bmin, bmax);
@@ -534,7 +549,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     __syncthreads();
     for (int kk = 2; kk <= NTP; kk <<= 1) {  // bitonic sort of (bound, tile) ascending
       for (int j = kk >> 1; j > 0; j >>= 1) {
-        for (int i = tid; i < NTP; i += NT) {
+        for (int i = tid; i < NTP; i += NTH) {
           const int ixj = i ^ j;
           if (ixj > i) {
             const bool up = (i & kk) == 0;
@@ -637,61 +652,67 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     const float lbq = tile_lower_bound(tinfo_b + (int64_t)lbt[t] * 8, qpt, qpt);
     const unsigned need = __ballot_sync(FULL, valid && !(lbq > tau));
     if (need) {
+      const int slot = lane / QPW;
+      const unsigned my_mask = SLOT_MASK << (slot * QPW);
+      const unsigned lt_mask = (1u << lane) - 1u;
 #pragma unroll 1
-      for (int h = 0; h < 2; ++h) {
+      for (int pass = 0; pass < NPASS; ++pass) {
         float2 pr[kRecLen];
+        const int pidx = pass * QPW + (lane & (QPW - 1));
 #pragma unroll
-        for (int f = 0; f < kRecLen; ++f) pr[f] = tile[f * PPT + h * 32 + lane];
+        for (int f = 0; f < kRecLen; ++f) pr[f] = tile[f * PPT + pidx];
         const int i0 = __float_as_int(pr[kRecPad].x), i1 = __float_as_int(pr[kRecPad].y);
-        const unsigned lt_mask = (1u << lane) - 1u;
         unsigned rem = need;
         while (rem) {
-          const int j0 = __ffs(rem) - 1;
-          rem &= rem - 1;
-          const bool two = rem != 0;
-          const int j1 = two ? __ffs(rem) - 1 : j0;
-          if (two) rem &= rem - 1;
-          const float4 q0 = qtab[warp * 32 + j0], q1 = qtab[warp * 32 + j1];
-          const float2 s0 = key_pair(make_float2(q0.x, q0.x), make_float2(q0.y, q0.y), make_float2(q0.z, q0.z), pr);
-          const float2 s1 = key_pair(make_float2(q1.x, q1.x), make_float2(q1.y, q1.y), make_float2(q1.z, q1.z), pr);
+          // slot h takes the h-th lowest query still to do (-1: none)
+          int jh[H];
 #pragma unroll
-          for (int u = 0; u < 2; ++u) {
-            if (u == 1 && !two) break;
-            const int j = u ? j1 : j0;
-            const float th = u ? q1.w : q0.w;
-            const float2 s2 = u ? s1 : s0;
-            const bool c0 = s2.x <= th, c1 = s2.y <= th;
-            const unsigned b0 = __ballot_sync(FULL, c0), b1 = __ballot_sync(FULL, c1);
-            if (b0 | b1) {
-              const int n = __popc(b0) + __popc(b1);
-              int c = __shfl_sync(FULL, my_cnt, j);
-              if (c + n > kQCap) {  // the queue of query j would overflow: fold every queue first
-                __syncwarp();
-                drain_queue<L>(keys, vals, tie_key, tau, my_cnt, qk, qv, lane);
-                my_cnt = 0;
-                qtab[warp * 32 + lane].w = tau;
-                __syncwarp();
-                c = 0;
-              }
-              if (c0) {
-                const int s = queue_slot(j, c + __popc(b0 & lt_mask));
-                qk[s] = s2.x;
-                qv[s] = i0;
-              }
-              if (c1) {
-                const int s = queue_slot(j, c + __popc(b0) + __popc(b1 & lt_mask));
-                qk[s] = s2.y;
-                qv[s] = i1;
-              }
-              if (lane == j) my_cnt = c + n;
+          for (int h = 0; h < H; ++h) {
+            jh[h] = rem ? __ffs(rem) - 1 : -1;
+            rem &= rem - 1;
+          }
+          int j = jh[0];
+#pragma unroll
+          for (int h = 1; h < H; ++h) j = (slot == h) ? jh[h] : j;
+          const float4 qj = qtab[warp * QPW + (j >= 0 ? j : 0)];
+          const float2 s2 = key_pair(make_float2(qj.x, qj.x), make_float2(qj.y, qj.y), make_float2(qj.z, qj.z), pr);
+          const bool c0 = j >= 0 && s2.x <= qj.w, c1 = j >= 0 && s2.y <= qj.w;
+          const unsigned b0 = __ballot_sync(FULL, c0), b1 = __ballot_sync(FULL, c1);
+          if (b0 | b1) {
+            const int n = __popc(b0 & my_mask) + __popc(b1 & my_mask);
+            int c = __shfl_sync(FULL, my_cnt, j >= 0 ? j : 0);
+            if (__any_sync(FULL, j >= 0 && c + n > kQCap)) {  // a queue would overflow: fold every queue first
+              __syncwarp();
+              drain_queue<L>(keys, vals, tie_key, tau, my_cnt, qk, qv, lane);
+              my_cnt = 0;
+              if (owner) qtab[lq].w = tau;
+              __syncwarp();
+              c = 0;
+            }
+            if (c0) {
+              const int e = queue_slot(j, c + __popc(b0 & my_mask & lt_mask));
+              qk[e] = s2.x;
+              qv[e] = i0;
+            }
+            if (c1) {
+              const int e = queue_slot(j, c + __popc(b0 & my_mask) + __popc(b1 & my_mask & lt_mask));
+              qk[e] = s2.y;
+              qv[e] = i1;
+            }
+#pragma unroll
+            for (int h = 0; h < H; ++h) {
+              const unsigned m = SLOT_MASK << (h * QPW);
+              if (lane == jh[h]) my_cnt += __popc(b0 & m) + __popc(b1 & m);
             }
           }
         }
-        __syncwarp();
-        drain_queue<L>(keys, vals, tie_key, tau, my_cnt, qk, qv, lane);
-        my_cnt = 0;
-        qtab[warp * 32 + lane].w = tau;
-        __syncwarp();
+        if ((pass + 1) % H == 0) {  // every query met 64 more points since the last fold
+          __syncwarp();
+          drain_queue<L>(keys, vals, tie_key, tau, my_cnt, qk, qv, lane);
+          my_cnt = 0;
+          if (owner) qtab[lq].w = tau;
+          __syncwarp();
+        }
       }
     }
     // count this warp out of the tile (release: its reads of the buffer and
@@ -709,7 +730,6 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
       // visit t + kTileBufs unless a stop was made; a tile is needed while
       // its bound is below some query's threshold
       float tmax = -INFINITY;
-#pragma unroll
       for (int i = lane; i < NT; i += 32) tmax = fmaxf(tmax, qtab[i].w);
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) tmax = fmaxf(tmax, __shfl_xor_sync(FULL, tmax, o));
@@ -746,15 +766,16 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
 
   // ---- flags and staging; the queue region is free (every drain ended
   // before the last barrier)
+  if (owner) {
 #pragma unroll
-  for (int s = 0; s < L; ++s) {
-    const int j = s - (KMAX - K);
-    if (j >= 0) {
-      out_k[lq * L + j] = keys[s];
-      out_i[lq * L + j] = vals[s];
+    for (int s = 0; s < L; ++s) {
+      const int j = s - (KMAX - K);
+      if (j >= 0) {
+        out_k[lq * L + j] = keys[s];
+        out_i[lq * L + j] = vals[s];
+      }
     }
-  }
-  {
+
     const int nneed = (P > K) ? K + 1 : K;
     bool fl = nan_fill, bad = false;
     for (int j = 0; j < nneed; ++j) {
@@ -779,7 +800,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   // ---- epilogue: dists / idxs / w_out, then f_out = sum_k w_k f[idx_k]
   // accumulated in k order with fma, 128-bit gathers of f rows.  Rows go to
   // the queries' original positions.
-  for (int x = tid; x < NT * K; x += NT) {
+  for (int x = tid; x < NT * K; x += NTH) {
     const int l = x / K, k = x - l * K;
     if (out_f[l]) continue;
     const int64_t e = (int64_t)qorig[l] * K + k;
@@ -791,7 +812,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   const float* fb = it.f;
   if (a.vec4) {
     const int C4 = F >> 2;
-    for (int x = tid; x < NT * C4; x += NT) {
+    for (int x = tid; x < NT * C4; x += NTH) {
       const int l = x / C4, c = x - l * C4;
       if (out_f[l]) continue;
       float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -820,7 +841,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
       reinterpret_cast<float4*>(it.f_out + (int64_t)qorig[l] * F)[c] = acc;
     }
   } else {
-    for (int x = tid; x < NT * F; x += NT) {
+    for (int x = tid; x < NT * F; x += NTH) {
       const int l = x / F, c = x - l * F;
       if (out_f[l]) continue;
       float acc = 0.f;
@@ -832,10 +853,10 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   return true;
 }
 
-template <int KMAX, int WPC>
+template <int KMAX, int WPC, int QPW>
 __global__ void __launch_bounds__(32 * WPC) search_f32_kernel(SearchParams a) {
   extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t* full = search_barriers<WPC>(smem);
+  uint64_t* full = search_barriers<WPC, QPW>(smem);
   if (threadIdx.x == 0) {
     for (int b = 0; b < kTileBufs; ++b) mbar_init(&full[b], 1);
     fence_mbar_init();
@@ -860,21 +881,21 @@ __global__ void __launch_bounds__(32 * WPC) search_f32_kernel(SearchParams a) {
   it.ntile = a.ntile;
   it.qblock = blockIdx.x;
   uint32_t uses[kTileBufs] = {};
-  search_item<KMAX, WPC>(a, it, smem, search_tiles_pow2(a.ntile), uses);
+  search_item<KMAX, WPC, QPW>(a, it, smem, search_tiles_pow2(a.ntile), uses);
 }
 
 // Ragged search: a persistent CTA takes work items in order from a counter
 // until the segment table's items run out.  Item i belongs to the last
 // segment whose item_off <= i; its queries are that segment's sorted
-// positions [(i - item_off) * 32 * WPC, ...).  Each item runs with the
+// positions [(i - item_off) * WPC * QPW, ...).  Each item runs with the
 // register list of its own segment's K (8, 16 or 32 slots + 1), up to the
 // launch's KMAX.
-template <int KMAX, int WPC>
+template <int KMAX, int WPC, int QPW>
 __global__ void __launch_bounds__(32 * WPC) search_ragged_kernel(SearchParams a) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ int s_item;
   if (*a.status) return;  // the table failed validation
-  uint64_t* full = search_barriers<WPC>(smem);
+  uint64_t* full = search_barriers<WPC, QPW>(smem);
   if (threadIdx.x == 0) {
     for (int b = 0; b < kTileBufs; ++b) mbar_init(&full[b], 1);
     fence_mbar_init();
@@ -889,7 +910,7 @@ __global__ void __launch_bounds__(32 * WPC) search_ragged_kernel(SearchParams a)
   const float* ctinfo = reinterpret_cast<const float*>(a.cs + ch->tinfo_off);
   const int nseg = sh->nseg, n_items = sh->n_items;
   const int ntp_cap = search_tiles_pow2(a.ntile);
-  constexpr int QPC = 32 * WPC;
+  constexpr int QPC = WPC * QPW;
   uint32_t uses[kTileBufs] = {};
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(a.item_counter, 1);
@@ -924,11 +945,11 @@ __global__ void __launch_bounds__(32 * WPC) search_ragged_kernel(SearchParams a)
       it.qblock = item - g.item_off;
       bool ok;
       if (KMAX > 8 && g.K <= 8)
-        ok = search_item<8, WPC>(a, it, smem, ntp_cap, uses);
+        ok = search_item<8, WPC, QPW>(a, it, smem, ntp_cap, uses);
       else if (KMAX > 16 && g.K <= 16)
-        ok = search_item<(KMAX > 16 ? 16 : KMAX), WPC>(a, it, smem, ntp_cap, uses);
+        ok = search_item<(KMAX > 16 ? 16 : KMAX), WPC, QPW>(a, it, smem, ntp_cap, uses);
       else
-        ok = search_item<KMAX, WPC>(a, it, smem, ntp_cap, uses);
+        ok = search_item<KMAX, WPC, QPW>(a, it, smem, ntp_cap, uses);
       if (!ok) break;
     }
     __syncthreads();  // the next item reuses shared memory (and s_item)
@@ -950,43 +971,43 @@ int num_sms(int dev) {
   return cache[dev];
 }
 
-template <int KMAX, int WPC>
+template <int KMAX, int WPC, int QPW>
 int launch_search_t(const SearchParams& a, cudaStream_t st) {
-  const size_t smem = search_smem_bytes(WPC) + search_region_c_bytes(a.ntile);
+  const size_t smem = search_smem_bytes(WPC, QPW) + search_region_c_bytes(a.ntile);
   if (smem > 227 * 1024) return KNNAG_ERR_TOO_LARGE;
   static int attr_set[64] = {0};  // largest size already allowed, per device
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 0 && dev < 64 && attr_set[dev] < (int)smem) {
-    if (cudaFuncSetAttribute(search_f32_kernel<KMAX, WPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
+    if (cudaFuncSetAttribute(search_f32_kernel<KMAX, WPC, QPW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
       return KNNAG_ERR_CUDA;
     attr_set[dev] = (int)smem;
   }
-  constexpr int QPC = 32 * WPC;
+  constexpr int QPC = WPC * QPW;
   dim3 grid((a.Q + QPC - 1) / QPC, a.B);
   profile_begin(st);
-  search_f32_kernel<KMAX, WPC><<<grid, 32 * WPC, smem, st>>>(a);
+  search_f32_kernel<KMAX, WPC, QPW><<<grid, 32 * WPC, smem, st>>>(a);
   profile_end(st);
   note_launches(1);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 
-template <int KMAX, int WPC>
+template <int KMAX, int WPC, int QPW>
 int launch_search_ragged_t(const SearchParams& a, int64_t cap_items, cudaStream_t st) {
-  const size_t smem = search_smem_bytes(WPC) + search_region_c_bytes(a.ntile);
+  const size_t smem = search_smem_bytes(WPC, QPW) + search_region_c_bytes(a.ntile);
   if (smem > 227 * 1024) return KNNAG_ERR_TOO_LARGE;
   int dev = 0;
   cudaGetDevice(&dev);
   static int attr_set[64] = {0};
   if (dev >= 0 && dev < 64 && attr_set[dev] < (int)smem) {
-    if (cudaFuncSetAttribute(search_ragged_kernel<KMAX, WPC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(search_ragged_kernel<KMAX, WPC, QPW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem) != cudaSuccess)
       return KNNAG_ERR_CUDA;
     attr_set[dev] = (int)smem;
   }
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_ragged_kernel<KMAX, WPC>, 32 * WPC, smem) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_ragged_kernel<KMAX, WPC, QPW>, 32 * WPC, smem) !=
           cudaSuccess ||
       per_sm < 1)
     per_sm = 1;
@@ -994,39 +1015,48 @@ int launch_search_ragged_t(const SearchParams& a, int64_t cap_items, cudaStream_
   if (grid > cap_items) grid = cap_items;
   if (grid < 1) grid = 1;
   profile_begin(st);
-  search_ragged_kernel<KMAX, WPC><<<(unsigned)grid, 32 * WPC, smem, st>>>(a);
+  search_ragged_kernel<KMAX, WPC, QPW><<<(unsigned)grid, 32 * WPC, smem, st>>>(a);
   profile_end(st);
   note_launches(1);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 
-// splits s (1, 2, 4) -> WPC = 4 / s warps (128 / s queries) per CTA
+// launch-shape code s -> (warps per CTA, queries per warp)
 template <int KMAX>
-int launch_search_ragged_k(const SearchParams& a, int G, int64_t cap_items, cudaStream_t st) {
-  if (G == 1) return launch_search_ragged_t<KMAX, 4>(a, cap_items, st);
-  if (G == 2) return launch_search_ragged_t<KMAX, 2>(a, cap_items, st);
-  return launch_search_ragged_t<KMAX, 1>(a, cap_items, st);
+int launch_search_ragged_k(const SearchParams& a, int s, int64_t cap_items, cudaStream_t st) {
+  switch (s) {
+    case 1: return launch_search_ragged_t<KMAX, 4, 32>(a, cap_items, st);
+    case 2: return launch_search_ragged_t<KMAX, 2, 32>(a, cap_items, st);
+    case 8: return launch_search_ragged_t<KMAX, 2, 16>(a, cap_items, st);
+    case 16: return launch_search_ragged_t<KMAX, 4, 8>(a, cap_items, st);
+    default: return launch_search_ragged_t<KMAX, 1, 32>(a, cap_items, st);
+  }
 }
 
 template <int KMAX>
-int launch_search_k(const SearchParams& a, int G, cudaStream_t st) {
-  if (G == 1) return launch_search_t<KMAX, 4>(a, st);
-  if (G == 2) return launch_search_t<KMAX, 2>(a, st);
-  return launch_search_t<KMAX, 1>(a, st);
+int launch_search_k(const SearchParams& a, int s, cudaStream_t st) {
+  switch (s) {
+    case 1: return launch_search_t<KMAX, 4, 32>(a, st);
+    case 2: return launch_search_t<KMAX, 2, 32>(a, st);
+    case 8: return launch_search_t<KMAX, 2, 16>(a, st);
+    case 16: return launch_search_t<KMAX, 4, 8>(a, st);
+    default: return launch_search_t<KMAX, 1, 32>(a, st);
+  }
 }
 
-// Splits per query group: the process-wide setting when one is made
-// (knnag_set_search_splits), else the fewest that still give ~4 CTAs per SM.
+// Launch shape of the uniform search: the process-wide setting when one is
+// made (knnag_set_search_splits), else by the warps the query set gives at
+// 32 queries per warp: many (large query sets) -> 128-query CTAs of 4 warps;
+// few -> fewer queries per warp, so that there are more warps to hide the
+// latency of each one's dependent work.
 int choose_splits(int B, int Q, int dev) {
   const int forced = search_splits_setting();
-  if (forced == 1 || forced == 2 || forced == 4) return forced;
-  const int64_t target = (int64_t)num_sms(dev) * 4;
-  for (int g = 1; g <= 4; g *= 2) {
-    const int qpc = 32 * (4 / g);
-    const int64_t ctas = (int64_t)B * ((Q + qpc - 1) / qpc);
-    if (ctas >= target) return g;
-  }
-  return 4;
+  if (search_shape_ok(forced)) return forced;
+  const int64_t warps32 = ((int64_t)B * Q + 31) / 32;
+  const int64_t sms = num_sms(dev);
+  if (warps32 >= 16 * sms) return 1;
+  if (warps32 >= 4 * sms) return 8;
+  return 16;
 }
 
 inline unsigned grid_for(int64_t n, int threads, int dev) {
@@ -1230,7 +1260,7 @@ int ragged_forward_impl(const char* cs, const void* segs, const float* q, const 
   int* flag_list = reinterpret_cast<int*>(ws + L.flag_list);
   int* perm_q = reinterpret_cast<int*>(ws + L.perm_q);
   const int G = splits;
-  const int qpc = 32 * (4 / G);
+  const int qpc = search_qpc(G);
   if (cudaMemsetAsync(status, 0, 4 * sizeof(int), st) != cudaSuccess) return KNNAG_ERR_CUDA;
   int rc = launch_validate_segments(cs, segs, cap_segs, cap_q, cap_e, max_k, ntile_cap, qpc, status, st);
   if (rc) return rc;

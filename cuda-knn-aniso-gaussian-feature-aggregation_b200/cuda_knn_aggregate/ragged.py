@@ -25,7 +25,10 @@ import torch
 
 from . import capi
 
-_SPLITS = (1, 2, 4)
+# search launch shapes (the C ABI's `splits` code): 1, 2, 4 -> 4, 2, 1 warps of
+# 32 queries per CTA; 8 -> 2 warps of 16; 16 -> 4 warps of 8
+_SPLITS = (1, 2, 4, 8, 16)
+_QPC = {1: 128, 2: 64, 4: 32, 8: 32, 16: 32}
 
 
 def _i32(xs):
@@ -132,14 +135,17 @@ class CloudSet:
 
 
 def default_splits(total_queries, device=None):
-    """Warps per 32-query group: the fewest that still give about 4 search
-    CTAs per SM (the uniform op's rule)."""
+    """Search launch shape by the warps the queries give at 32 per warp (the
+    uniform op's rule): many -> 128-query CTAs; few -> fewer queries per
+    warp, for more warps."""
     sms = torch.cuda.get_device_properties(device or torch.cuda.current_device()).multi_processor_count \
         if torch.cuda.is_available() else 148
-    for g in _SPLITS:
-        if total_queries / (32 * (4 // g)) >= 4 * sms:
-            return g
-    return 4
+    warps32 = (int(total_queries) + 31) // 32
+    if warps32 >= 16 * sms:
+        return 1
+    if warps32 >= 4 * sms:
+        return 8
+    return 16
 
 
 class SegmentTable:
@@ -262,8 +268,8 @@ def shape_bucket(cloudset: CloudSet, Qs, Ks):
 
 
 def autotune_splits(cloudset: CloudSet, clouds, qs, Ks, reps=3, cache=True):
-    """Queries per search CTA (128 / splits, splits in 1, 2, 4) for steps
-    shaped like this one: each candidate runs the step as a captured graph
+    """Search launch shape (queries per CTA and per warp, the ``splits`` codes
+    1, 2, 4, 8, 16) for steps shaped like this one: each candidate runs the step as a captured graph
     ``reps`` times (after a warm-up) and the fastest median wins.  Cached per
     ``shape_bucket`` in memory and in the tuner's JSON file
     (``tuning.cache_path()``), so a later process reuses the choice."""

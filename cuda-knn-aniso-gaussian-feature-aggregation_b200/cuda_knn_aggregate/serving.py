@@ -137,7 +137,7 @@ def step_bytes_per_query(F, max_k):
 class Server:
     def __init__(self, cloudset: CloudSet, hbm_budget_bytes=40e9, max_k=16, step_queries=1 << 20, inflight=3,
                  cap_segments=256, splits=None, graph=True, host_budget_bytes=2e9, tune_requests=None):
-        """``splits``: warps per 32-query group of the search (1, 2, 4), or
+        """``splits``: the search launch shape (1, 2, 4, 8, 16; see ``tuning``), or
         "auto" to let the autotuner time the candidates on one step packed
         from ``tune_requests``."""
         self.cs = cloudset

@@ -2,8 +2,10 @@
 
 The tuned knobs change only the time, never a result:
 
-* ``splits`` (1, 2, 4): the search CTA holds 4 / splits warps, i.e. 128 /
-  splits queries per CTA (the C ABI's ``knnag_set_search_splits``);
+* ``splits``, the search launch shape (the C ABI's
+  ``knnag_set_search_splits``): 1, 2, 4 -> 4, 2, 1 warps of 32 queries per
+  CTA; 8 -> 2 warps of 16 queries; 16 -> 4 warps of 8 -- queries per CTA
+  and per warp;
 * the K register layout: the list length is the K bucket (8, 16, 32) --
   part of the shape bucket, not a free knob.
 
@@ -29,7 +31,7 @@ import torch
 
 from . import capi
 
-SPLITS = (1, 2, 4)
+SPLITS = (1, 2, 4, 8, 16)
 _CACHE: dict = {}      # in-memory: full key -> choice dict
 _LOADED: set = set()   # files already read into _CACHE
 TIMED = {"runs": 0}    # number of candidate timings made in this process

@@ -271,7 +271,7 @@ int knnag_cloudset_build(const float* p, const float* sigma, const float* R, int
  * indices within the cloud.  knnag_segments_encode writes the table into a
  * HOST buffer of knnag_segments_bytes(nseg); the caller copies it to a
  * device buffer (256-byte aligned) before the call that uses it.  `splits`
- * (1, 2 or 4 warps per 32 queries) must match the forward's.  want_grad
+ * (the search launch shape code, as for knnag_set_search_splits) must match the forward's.  want_grad
  * (NULL: every segment) marks the segments knnag_ragged_grad_q serves; they
  * must come first. */
 size_t knnag_segments_bytes(int nseg);
@@ -325,12 +325,14 @@ void knnag_set_profile_events(void* ev_begin, void* ev_end);
 /* Process-wide count of kernels this library has launched so far. */
 long long knnag_launch_count(void);
 
-/* Tuning: warps per 32-query group (1, 2 or 4) of the FP32 search of every
- * later knnag_forward / knnag_forward_noalloc in the process (the autotuner
- * sets it from timings cached per shape bucket); 0 restores the automatic
- * choice (the fewest splits that still give about 4 CTAs per SM).  Results
- * do not depend on it.  Returns KNNAG_ERR_ARG for other values.  No
- * reference counterpart. */
+/* Tuning: launch shape of the FP32 search of every later knnag_forward /
+ * knnag_forward_noalloc in the process (the autotuner sets it from timings
+ * cached per shape bucket): 1, 2, 4 -> CTAs of 4, 2, 1 warps of 32 queries;
+ * 8 -> 2 warps of 16 queries; 16 -> 4 warps of 8 queries (fewer queries per
+ * warp give more warps for small query sets); 0 restores the automatic
+ * choice (by the warps the query set gives).  Results do not depend on it.
+ * Returns KNNAG_ERR_ARG for other values.  The same codes are the `splits`
+ * of segment tables.  No reference counterpart. */
 int knnag_set_search_splits(int splits);
 int knnag_get_search_splits(void);
 
