@@ -194,125 +194,6 @@ __global__ void cell_scatter_kernel(CellJob j0, CellJob j1, const float* __restr
   }
 }
 
-// The counting sort of one uniform batch element in one CTA, for groups
-// small enough that its cell counts fit shared memory: the points' bounding
-// box (block reduction), the Hilbert-cell histograms of the points and of
-// the queries (shared-memory atomics, points' cells first), their exclusive
-// scan in place, and the scatter into perm_p / perm_q -- what
-// point_bounds_kernel, cell_count_kernel, the scan and cell_scatter_kernel
-// do in four launches (plus a memset) for large groups.  The order of
-// elements inside a cell follows the atomics; it never changes a result.
-constexpr int kGroupIndexThreads = 1024;
-constexpr int kGroupIndexMaxBits = 4;            // 8^4 = 4096 cells per kind (32 KB of counts)
-constexpr int64_t kGroupIndexMaxItems = 1 << 16;  // points + queries of one group
-
-__global__ void __launch_bounds__(kGroupIndexThreads) group_index_kernel(const float* __restrict__ rec,
-                                                                         const float* __restrict__ q, int P, int Q,
-                                                                         int bits, float* __restrict__ bnd,
-                                                                         int* __restrict__ perm_p,
-                                                                         int* __restrict__ perm_q) {
-  extern __shared__ int cnt[];  // [2 * cells]: counts, then running offsets
-  __shared__ float red[6][kGroupIndexThreads / 32];
-  __shared__ float gb[8];
-  __shared__ int warp_sums[33];
-  const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int cells = 1 << (3 * bits), n = 2 * cells;
-  const float* rb = rec + (int64_t)b * P * kRecLen;
-  const float* qb = q + (int64_t)b * Q * 3;
-  // bounds of the points (records hold -p)
-  float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-  for (int i = tid; i < P; i += kGroupIndexThreads) {
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const float v = -rb[(int64_t)i * kRecLen + kNPX + a];
-      mn[a] = fminf(mn[a], v);
-      mx[a] = fmaxf(mx[a], v);
-    }
-  }
-#pragma unroll
-  for (int a = 0; a < 3; ++a)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      mn[a] = fminf(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], o));
-      mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
-    }
-  if (lane == 0)
-    for (int a = 0; a < 3; ++a) {
-      red[a][warp] = mn[a];
-      red[3 + a][warp] = mx[a];
-    }
-  for (int c = tid; c < n; c += kGroupIndexThreads) cnt[c] = 0;
-  __syncthreads();
-  if (tid < 6) {
-    float v = tid < 3 ? INFINITY : -INFINITY;
-    for (int w = 0; w < kGroupIndexThreads / 32; ++w) v = tid < 3 ? fminf(v, red[tid][w]) : fmaxf(v, red[tid][w]);
-    gb[tid] = v;
-    bnd[b * 8 + tid] = v;
-  }
-  __syncthreads();
-  // histograms: point cells in [0, cells), query cells in [cells, 2 cells)
-  for (int i = tid; i < P; i += kGroupIndexThreads) {
-    const float* r = rb + (int64_t)i * kRecLen;
-    atomicAdd(&cnt[cell_of(-r[kNPX], -r[kNPY], -r[kNPZ], gb, bits)], 1);
-  }
-  for (int j = tid; j < Q; j += kGroupIndexThreads) {
-    const float* v = qb + (int64_t)j * 3;
-    atomicAdd(&cnt[cells + cell_of(v[0], v[1], v[2], gb, bits)], 1);
-  }
-  __syncthreads();
-  // exclusive scan in place (each thread owns `per` consecutive counts);
-  // query offsets come out shifted by P
-  const int per = (n + kGroupIndexThreads - 1) / kGroupIndexThreads;  // <= 8
-  int v8[8];
-  int local = 0;
-#pragma unroll
-  for (int u = 0; u < 8; ++u) {
-    const int i = tid * per + u;
-    v8[u] = (u < per && i < n) ? cnt[i] : 0;
-    local += v8[u];
-  }
-  int incl = local;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int t = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += t;
-  }
-  if (lane == 31) warp_sums[warp] = incl;
-  __syncthreads();
-  if (warp == 0) {
-    const int ws = warp_sums[lane];
-    int wi = ws;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, wi, o);
-      if (lane >= o) wi += t;
-    }
-    warp_sums[lane] = wi - ws;
-  }
-  __syncthreads();
-  int run = warp_sums[warp] + incl - local;
-#pragma unroll
-  for (int u = 0; u < 8; ++u) {
-    const int i = tid * per + u;
-    if (u < per && i < n) {
-      cnt[i] = run;
-      run += v8[u];
-    }
-  }
-  __syncthreads();
-  // scatter (positions are group-local: points [0, P), queries [0, Q))
-  for (int i = tid; i < P; i += kGroupIndexThreads) {
-    const float* r = rb + (int64_t)i * kRecLen;
-    const int pos = atomicAdd(&cnt[cell_of(-r[kNPX], -r[kNPY], -r[kNPZ], gb, bits)], 1);
-    perm_p[(int64_t)b * P + pos] = i;
-  }
-  for (int j = tid; j < Q; j += kGroupIndexThreads) {
-    const float* v = qb + (int64_t)j * 3;
-    const int pos = atomicAdd(&cnt[cells + cell_of(v[0], v[1], v[2], gb, bits)], 1) - P;
-    perm_q[(int64_t)b * Q + pos] = j;
-  }
-}
-
 // Point groups of the tile kernels: uniform (group b: records [b*P, ...),
 // tiles [b*ntile, ...)) or the clouds of a cloud set.
 struct TileGroup {
@@ -473,14 +354,6 @@ int launch_spatial_index(const float* q, const float* rec, int B, int Q, int P, 
   float* pairs = reinterpret_cast<float*>(ws + L.pairs);
   float* tinfo = reinterpret_cast<float*>(ws + L.tinfo);
   const int ntile = P_pad / kTilePoints;
-  if (bits <= kGroupIndexMaxBits && (int64_t)P + Q <= kGroupIndexMaxItems) {
-    // small groups: bounds, histograms, scan and scatter in one CTA each
-    group_index_kernel<<<B, kGroupIndexThreads, 2 * (size_t)cells * sizeof(int), st>>>(rec, q, P, Q, bits, bnd, perm,
-                                                                                         perm + (size_t)B * P);
-    tile_info_kernel<<<dim3(ntile, B), kTilePoints, 0, st>>>(rec, perm, nullptr, P, ntile, pairs, tinfo);
-    note_launches(2);
-    return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
-  }
   GroupMap pm{P, bits, nullptr, nullptr, nullptr, nullptr, nullptr};
   GroupMap qm{Q, bits, nullptr, nullptr, nullptr, nullptr, nullptr};
   point_bounds_kernel<<<B, 512, 0, st>>>(rec, pm, bnd);
