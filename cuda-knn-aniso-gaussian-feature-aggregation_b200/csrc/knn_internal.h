@@ -104,18 +104,16 @@ inline bool search_shape_ok(int shape) { return shape == 1 || shape == 2 || shap
 
 // Shared-memory layout of the search kernel with `wpc` warps of `qpw` queries:
 //   ring      kTileBufs tiles
-//   queues    wpc x [32 lanes][kQCap] keys, then indices (after the tile
-//             loop: the lanes' sub-lists, then the queries' sorted lists,
-//             weights and flags)
+//   queues    wpc x [qpw queries][kQCap] keys, then indices (after the tile
+//             loop: the CTA's sorted lists, weights and flags)
 //   qtab      [wpc qpw] float4 (x, y, z, threshold) of the CTA's queries
 //   misc      [wpc qpw] original query index, [wpc][6] warp query boxes,
 //             64 bytes of mbarriers / counters / flags
 //   region C  tile bounds and visit order [NTP x 8 B] + visit counter
 __host__ __device__ inline constexpr size_t search_queue_off() { return (size_t)kTileBufs * kSearchTileBytes; }
-// every lane of a warp has its own candidate queue of kQCap entries
-constexpr size_t kWarpQueueBytes = (size_t)32 * kQCap * 8;
+__host__ __device__ inline constexpr size_t search_warp_queue_bytes(int qpw) { return (size_t)qpw * kQCap * 8; }
 __host__ __device__ inline constexpr size_t search_qtab_off(int wpc, int qpw) {
-  return search_queue_off() + (size_t)wpc * kWarpQueueBytes;
+  return search_queue_off() + (size_t)wpc * search_warp_queue_bytes(qpw);
 }
 __host__ __device__ inline constexpr size_t search_misc_off(int wpc, int qpw) {
   return search_qtab_off(wpc, qpw) + (size_t)wpc * qpw * 16;
@@ -131,7 +129,9 @@ __host__ __device__ inline int search_tiles_pow2(int ntile) {
   return n;
 }
 __host__ __device__ inline size_t search_region_c_bytes(int ntile) { return (size_t)search_tiles_pow2(ntile) * 8 + 16; }
-
+// The sorted lists of a query (keys, indices, weights) and its flag, staged
+// for the epilogue, must fit the query's share of the queue region.
+static_assert((size_t)33 * 12 + 4 <= (size_t)kQCap * 8, "epilogue staging exceeds the queue region");
 
 // ------------------------------------------------------------- workspace
 // Forward workspace: [status, flag_count] | flag_list [B*Q] | records (when

@@ -328,58 +328,57 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
 // equal keys or an empty slot, when tie_key <= its (K+1)-th key, or when a
 // fill-phase key is NaN.
 
+// Insert (k, i) into the sorted list when k is below its top.  The list is
+// ascending, so lt[s] = k < keys[s] is false up to the insertion point and
+// true after it; every slot takes its left neighbour (lt[s-1]), the new
+// entry (lt[s] only) or stays -- all comparisons are independent, so the
+// insertion is a few instructions deep instead of a chain through the list.
+// The entry that falls off the top is remembered when it was a real entry
+// equal to the new top (a tie the exactness flags must see).
 template <int L>
 __device__ __forceinline__ void list_insert(float (&keys)[L], int (&vals)[L], float k, int i, float& tie_key) {
+  bool lt[L];
 #pragma unroll
-  for (int s = 0; s < L; ++s) {
-    const bool lt = k < keys[s];
-    const float nk = lt ? k : keys[s];
-    const float ek = lt ? keys[s] : k;
-    const int ni = lt ? i : vals[s];
-    const int ei = lt ? vals[s] : i;
-    keys[s] = nk;
-    vals[s] = ni;
-    k = ek;
-    i = ei;
+  for (int s = 0; s < L; ++s) lt[s] = k < keys[s];
+  const float out_k = keys[L - 1];
+  const int out_i = vals[L - 1];
+#pragma unroll
+  for (int s = L - 1; s > 0; --s) {
+    keys[s] = lt[s - 1] ? keys[s - 1] : (lt[s] ? k : keys[s]);
+    vals[s] = lt[s - 1] ? vals[s - 1] : (lt[s] ? i : vals[s]);
   }
-  // (k, i) left the list: if it was a real entry equal to the new top, remember it.
-  if (i >= 0 && k == keys[L - 1]) tie_key = fminf(tie_key, k);
+  keys[0] = lt[0] ? k : keys[0];
+  vals[0] = lt[0] ? i : vals[0];
+  if (lt[L - 1] && out_i >= 0 && out_k == keys[L - 1]) tie_key = fminf(tie_key, out_k);
 }
 
-// Queue slot s of lane l's candidate queue: rows are rotated by the lane so
-// that a drain (every lane its own queue, the same slot) is free of bank
-// conflicts.
-__device__ __forceinline__ int queue_slot(int l, int s) { return l * kQCap + ((s + l) & (kQCap - 1)); }
+// Queue slot of entry e of query (lane) j: rows are rotated by j so that
+// appends (one query, consecutive entries) and drains (every lane its own
+// query, the same entry) are both free of bank conflicts.
+__device__ __forceinline__ int queue_slot(int j, int e) { return j * kQCap + ((e + j) & (kQCap - 1)); }
 
-// Merge the sorted sub-lists of one query (G lanes' lists staged at rows
-// base .. base + G - 1 of mk/mv, slots [start, L) of each; entries with a
-// negative index count as +inf) and write the `count` smallest to ok/oi.
-template <int G, int L>
-__device__ __forceinline__ void merge_sublists(const float* mk, const int* mv, int base, int start, int count,
-                                               float* ok, int* oi) {
-  int h[G];
-#pragma unroll
-  for (int g = 0; g < G; ++g) h[g] = start;
-  for (int j = 0; j < count; ++j) {
-    float bk = INFINITY;
-    int bi = -1, bg = -1;
-#pragma unroll
-    for (int g = 0; g < G; ++g) {
-      if (h[g] < L) {
-        const int v = mv[(base + g) * L + h[g]];
-        const float kk = v >= 0 ? mk[(base + g) * L + h[g]] : INFINITY;
-        if (bg < 0 || kk < bk) {
-          bk = kk;
-          bi = v;
-          bg = g;
-        }
-      }
+// Lane `lane` folds its query's n queued candidates into its list and
+// refreshes its threshold; the caller resets the counts.
+template <int L>
+__device__ __forceinline__ void drain_queue(float (&keys)[L], int (&vals)[L], float& tie_key, float& tau, int n,
+                                            const float* qk, const int* qv, int lane) {
+  // the next entry is loaded while this one is folded in
+  float k = n > 0 ? qk[queue_slot(lane, 0)] : 0.f;
+  int i = n > 0 ? qv[queue_slot(lane, 0)] : -1;
+  for (int e = 0; e < n; ++e) {
+    const int s = queue_slot(lane, e + 1);
+    const float kn = e + 1 < n ? qk[s] : 0.f;
+    const int in = e + 1 < n ? qv[s] : -1;
+    const float top = keys[L - 1];
+    if (k < top) {
+      list_insert<L>(keys, vals, k, i, tie_key);
+    } else if (k == top) {
+      tie_key = fminf(tie_key, k);
     }
-#pragma unroll
-    for (int g = 0; g < G; ++g) h[g] += (g == bg) ? 1 : 0;
-    ok[j] = bk;
-    oi[j] = bi >= 0 ? bi : -1;
+    k = kn;
+    i = in;
   }
+  tau = fminf(tau, keys[L - 1]);
 }
 
 // One search work item: up to WPC * QPW queries of one batch element or
@@ -432,25 +431,19 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   constexpr int L = KMAX + 1;
   constexpr int NT = QPW * WPC;         // queries of the item
   constexpr int NTH = 32 * WPC;         // threads
-  constexpr int H = 32 / QPW;           // lane slots per warp = lanes (sub-lists) per query
-  constexpr int LPQ = H;
+  constexpr int H = 32 / QPW;           // lane slots per warp (queries evaluated at once)
   constexpr int PPT = kTilePoints / 2;  // pairs per tile
   constexpr int NPASS = PPT / QPW;      // passes per tile (QPW pairs each)
   constexpr unsigned FULL = 0xffffffffu;
   constexpr unsigned SLOT_MASK = QPW == 32 ? 0xffffffffu : ((1u << QPW) - 1u);
   static_assert(QPW == 32 || QPW == 16 || QPW == 8, "queries per warp");
-  // epilogue staging in the queue region: sub-lists [NTH][L] keys + indices
-  // + tie keys [NTH] (when LPQ > 1), then per query keys / indices /
-  // weights [NT][L] and flags [NT]
-  constexpr size_t kMergeBytes = LPQ > 1 ? ((size_t)NTH * (L * 8 + 4) + 15) / 16 * 16 : 0;
-  static_assert(kMergeBytes + (size_t)NT * (L * 12 + 4) <= (size_t)WPC * kWarpQueueBytes, "epilogue staging");
+  static_assert((size_t)NT * L * 12 + NT * 4 <= (size_t)WPC * search_warp_queue_bytes(QPW), "epilogue staging");
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int jq = lane / LPQ, sub = lane % LPQ;  // this lane keeps sub-list `sub` of the warp's query jq
-  const bool head = sub == 0;                   // the query's first lane (its count, threshold, outputs)
+  const bool owner = lane < QPW;       // lane keeps query `lane` of the warp
   unsigned char* ring = smem;
-  float* qk = reinterpret_cast<float*>(smem + search_queue_off() + (size_t)warp * kWarpQueueBytes);
-  int* qv = reinterpret_cast<int*>(qk + 32 * kQCap);
+  float* qk = reinterpret_cast<float*>(smem + search_queue_off() + (size_t)warp * search_warp_queue_bytes(QPW));
+  int* qv = reinterpret_cast<int*>(qk + QPW * kQCap);
   float4* qtab = reinterpret_cast<float4*>(smem + search_qtab_off(WPC, QPW));  // [NT]
   int* qorig = reinterpret_cast<int*>(smem + search_misc_off(WPC, QPW));       // [NT] original query index (-1: none)
   float* qbox = reinterpret_cast<float*>(qorig + NT);                          // [WPC][6]
@@ -464,27 +457,24 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   int* lbt = reinterpret_cast<int*>(lbk + ntp_cap);
   volatile int* s_nvisit = reinterpret_cast<volatile int*>(lbt + ntp_cap);
   // epilogue views of the queue region (after the tile loop)
-  float* mk = reinterpret_cast<float*>(smem + search_queue_off());
-  int* mv = reinterpret_cast<int*>(mk + NTH * L);
-  float* mf = reinterpret_cast<float*>(mv + NTH * L);
-  float* out_k = reinterpret_cast<float*>(smem + search_queue_off() + kMergeBytes);
+  float* out_k = reinterpret_cast<float*>(smem + search_queue_off());
   int* out_i = reinterpret_cast<int*>(out_k + NT * L);
   float* out_w = reinterpret_cast<float*>(out_i + NT * L);
   int* out_f = reinterpret_cast<int*>(out_w + NT * L);
 
-  const int lq = warp * QPW + jq;           // this lane's query within the item
-  const int sp = it.qblock * NT + lq;       // its position in the spatial order
-  bool valid = sp < it.Q;
+  const int lq = warp * QPW + lane;         // query of this (owner) lane within the item
+  const int sp = it.qblock * NT + lq;       // position in the spatial order
+  bool valid = owner && sp < it.Q;
   int qi = it.perm_q[valid ? sp : it.Q - 1];
   if ((unsigned)qi >= (unsigned)it.Q) {  // the query order is a permutation: never taken
-    if (valid && head) atomicOr(a.status, kStatusBadIndex);
+    if (valid) atomicOr(a.status, kStatusBadIndex);
     qi = 0;
     valid = false;
   }
   const int K = it.K, P = it.P;
   const float qx = it.q[(int64_t)qi * 3 + 0], qy = it.q[(int64_t)qi * 3 + 1], qz = it.q[(int64_t)qi * 3 + 2];
   const float* recb = it.rec;
-  if (head) {
+  if (owner) {
     qorig[lq] = valid ? qi : -1;
     qtab[lq] = make_float4(qx, qy, qz, valid ? INFINITY : -INFINITY);
   }
@@ -492,7 +482,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   // MinK's fill phase stores points 0..K-1 whatever their key: a NaN there
   // changes the result in ways only the replay reproduces.
   bool nan_fill = false;
-  if (head)
+  if (owner)
     for (int i = 0; i < K; ++i) {
       const float s = key_rec<float>(qx, qy, qz, recb + (int64_t)i * kRecLen);
       if (s != s) nan_fill = true;
@@ -501,6 +491,10 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   // ---- box of this CTA's queries and the tile visit order
   {
     float bx[6] = {qx, qy, qz, qx, qy, qz};
+    if (!owner) {
+      bx[0] = bx[1] = bx[2] = INFINITY;
+      bx[3] = bx[4] = bx[5] = -INFINITY;
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
@@ -594,45 +588,8 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     vals[s] = -1;
   }
   float tau = valid ? INFINITY : -INFINITY, tie_key = INFINITY;
-  int my_cnt = 0;  // queued candidates of query jq (kept by its head lane)
-  // slot of a sub-list's c-th smallest real key, c = ceil((K+1)/LPQ): the
-  // LPQ sub-lists hold LPQ * c >= K+1 keys at or below the largest of those
-  const int cslot = (KMAX - K) + (K + LPQ) / LPQ - 1;
-
-  // Fold this lane's queued candidates into its sub-list, then refresh the
-  // query's threshold from its sub-lists' tops and c-th keys (warp-uniform
-  // call: the shuffles need every lane).
-  auto drain = [&]() {
-    __syncwarp();
-    const int cj = __shfl_sync(FULL, my_cnt, jq * LPQ);
-    const int nr = cj > sub ? (cj - sub + LPQ - 1) / LPQ : 0;
-    for (int s = 0; s < nr; ++s) {
-      const int e = queue_slot(lane, s);
-      const float k = qk[e];
-      const float top = keys[L - 1];
-      if (k < top) {
-        list_insert<L>(keys, vals, k, qv[e], tie_key);
-      } else if (k == top) {
-        tie_key = fminf(tie_key, k);
-      }
-    }
-    my_cnt = 0;
-    float t = keys[L - 1];
-    if (LPQ > 1) {
-      float c = keys[0];  // keys[cslot] without a dynamic register index
-#pragma unroll
-      for (int s = 1; s < L; ++s) c = (s == cslot) ? keys[s] : c;
-#pragma unroll
-      for (int o = LPQ >> 1; o > 0; o >>= 1) {
-        t = fminf(t, __shfl_xor_sync(FULL, t, o));
-        c = fmaxf(c, __shfl_xor_sync(FULL, c, o));
-      }
-      t = fminf(t, c);
-    }
-    tau = fminf(tau, t);
-    if (head) qtab[lq].w = tau;
-    __syncwarp();
-  };
+  int my_cnt = 0;  // queued candidates of this lane's query
+  const float qpt[3] = {qx, qy, qz};
 
   const int ntile = it.ntile;
   const float* pairs_b = it.pairs;
@@ -689,9 +646,6 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   // t + kTileBufs into the same buffer.  A warp does that duty before it
   // starts its next tile, so the decision for t + kTileBufs - 1 is complete
   // before any warp can be last for tile t: decisions stay in order.
-  const int slot = lane / QPW;
-  const unsigned my_mask = SLOT_MASK << (slot * QPW);
-  const unsigned lt_mask = (1u << lane) - 1u;
   int t = 0;
   for (;; ++t) {
     const int buf = t % kTileBufs;
@@ -705,18 +659,14 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     }
     if (*s_abort || t >= *s_final) break;
     const float2* tile = reinterpret_cast<const float2*>(ring + buf * kSearchTileBytes);
-    // queries of this warp the tile may matter to (lane l < QPW judges
-    // query l): the bound against the query point itself not above its
-    // threshold
-    unsigned need;
-    {
-      const int l = lane < QPW ? lane : 0;
-      const float4 qq = qtab[warp * QPW + l];
-      const float qp3[3] = {qq.x, qq.y, qq.z};
-      const float lbq = tile_lower_bound(tinfo_b + (int64_t)lbt[t] * 8, qp3, qp3);
-      need = __ballot_sync(FULL, lane < QPW && qorig[warp * QPW + l] >= 0 && !(lbq > qq.w));
-    }
+    // queries of this warp the tile may matter to: bound against the query
+    // point itself not above its threshold
+    const float lbq = tile_lower_bound(tinfo_b + (int64_t)lbt[t] * 8, qpt, qpt);
+    const unsigned need = __ballot_sync(FULL, valid && !(lbq > tau));
     if (need) {
+      const int slot = lane / QPW;
+      const unsigned my_mask = SLOT_MASK << (slot * QPW);
+      const unsigned lt_mask = (1u << lane) - 1u;
 #pragma unroll 1
       for (int pass = 0; pass < NPASS; ++pass) {
         float2 pr[kRecLen];
@@ -742,32 +692,39 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
           const unsigned b0 = __ballot_sync(FULL, c0), b1 = __ballot_sync(FULL, c1);
           if (b0 | b1) {
             const int n = __popc(b0 & my_mask) + __popc(b1 & my_mask);
-            int c = __shfl_sync(FULL, my_cnt, (j >= 0 ? j : 0) * LPQ);
-            if (__any_sync(FULL, j >= 0 && c + n > LPQ * kQCap)) {  // a queue would overflow: fold them all first
-              drain();
+            int c = __shfl_sync(FULL, my_cnt, j >= 0 ? j : 0);
+            if (__any_sync(FULL, j >= 0 && c + n > kQCap)) {  // a queue would overflow: fold every queue first
+              __syncwarp();
+              drain_queue<L>(keys, vals, tie_key, tau, my_cnt, qk, qv, lane);
+              my_cnt = 0;
+              if (owner) qtab[lq].w = tau;
+              __syncwarp();
               c = 0;
             }
-            // candidate e of query j goes to slot e / LPQ of the query's lane j * LPQ + e % LPQ
             if (c0) {
-              const int e = c + __popc(b0 & my_mask & lt_mask);
-              const int dst = queue_slot(j * LPQ + (e % LPQ), e / LPQ);
-              qk[dst] = s2.x;
-              qv[dst] = i0;
+              const int e = queue_slot(j, c + __popc(b0 & my_mask & lt_mask));
+              qk[e] = s2.x;
+              qv[e] = i0;
             }
             if (c1) {
-              const int e = c + __popc(b0 & my_mask) + __popc(b1 & my_mask & lt_mask);
-              const int dst = queue_slot(j * LPQ + (e % LPQ), e / LPQ);
-              qk[dst] = s2.y;
-              qv[dst] = i1;
+              const int e = queue_slot(j, c + __popc(b0 & my_mask) + __popc(b1 & my_mask & lt_mask));
+              qk[e] = s2.y;
+              qv[e] = i1;
             }
 #pragma unroll
             for (int h = 0; h < H; ++h) {
               const unsigned m = SLOT_MASK << (h * QPW);
-              if (jh[h] >= 0 && lane == jh[h] * LPQ) my_cnt += __popc(b0 & m) + __popc(b1 & m);
+              if (lane == jh[h]) my_cnt += __popc(b0 & m) + __popc(b1 & m);
             }
           }
         }
-        if ((pass + 1) % H == 0) drain();  // every query met 64 more points since the last fold
+        if ((pass + 1) % H == 0) {  // every query met 64 more points since the last fold
+          __syncwarp();
+          drain_queue<L>(keys, vals, tie_key, tau, my_cnt, qk, qv, lane);
+          my_cnt = 0;
+          if (owner) qtab[lq].w = tau;
+          __syncwarp();
+        }
       }
     }
     // count this warp out of the tile (release: its reads of the buffer and
@@ -819,23 +776,9 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     for (int b = 0; b < kTileBufs; ++b) uses[b] += n > b ? (n - b + kTileBufs - 1) / kTileBufs : 0;
   }
 
-  // ---- sub-list merge, flags and staging; the queue region is free (every
-  // drain ended before the last barrier)
-  float fl_tie = tie_key;
-  if (LPQ > 1) {
-#pragma unroll
-    for (int s = 0; s < L; ++s) {
-      mk[tid * L + s] = keys[s];
-      mv[tid * L + s] = vals[s];
-    }
-    mf[tid] = tie_key;
-    __syncwarp();
-    if (head) {
-#pragma unroll
-      for (int g = 1; g < LPQ; ++g) fl_tie = fminf(fl_tie, mf[tid + g]);
-      merge_sublists<LPQ, L>(mk, mv, tid, KMAX - K, K + 1, out_k + lq * L, out_i + lq * L);
-    }
-  } else {
+  // ---- flags and staging; the queue region is free (every drain ended
+  // before the last barrier)
+  if (owner) {
 #pragma unroll
     for (int s = 0; s < L; ++s) {
       const int j = s - (KMAX - K);
@@ -844,8 +787,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
         out_i[lq * L + j] = vals[s];
       }
     }
-  }
-  if (head) {
+
     const int nneed = (P > K) ? K + 1 : K;
     bool fl = nan_fill, bad = false;
     for (int j = 0; j < nneed; ++j) {
@@ -857,7 +799,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     for (int j = 0; j + 1 < nneed; ++j)
       if (out_k[lq * L + j] == out_k[lq * L + j + 1]) fl = true;
     const float m = (P > K) ? out_k[lq * L + K] : INFINITY;
-    if (fl_tie <= m) fl = true;
+    if (tie_key <= m) fl = true;
     for (int j = 0; j < K; ++j) out_w[lq * L + j] = weight_of(out_k[lq * L + j]);
     out_f[lq] = (fl || bad || !valid) ? 1 : 0;
     if (valid && fl && !bad) {
