@@ -676,45 +676,63 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
         const int i0 = __float_as_int(pr[kRecPad].x), i1 = __float_as_int(pr[kRecPad].y);
         unsigned rem = need;
         while (rem) {
-          // slot h takes the h-th lowest query still to do (-1: none)
-          int jh[H];
+          // two rounds per iteration (independent key evaluations in
+          // flight): in round u slot h takes the (u * H + h)-th lowest
+          // query still to do (-1: none)
+          int jh[2 * H];
 #pragma unroll
-          for (int h = 0; h < H; ++h) {
+          for (int h = 0; h < 2 * H; ++h) {
             jh[h] = rem ? __ffs(rem) - 1 : -1;
             rem &= rem - 1;
           }
-          int j = jh[0];
+          int jr[2];
+          float4 qr[2];
+          float2 sr[2];
 #pragma unroll
-          for (int h = 1; h < H; ++h) j = (slot == h) ? jh[h] : j;
-          const float4 qj = qtab[warp * QPW + (j >= 0 ? j : 0)];
-          const float2 s2 = key_pair(make_float2(qj.x, qj.x), make_float2(qj.y, qj.y), make_float2(qj.z, qj.z), pr);
-          const bool c0 = j >= 0 && s2.x <= qj.w, c1 = j >= 0 && s2.y <= qj.w;
-          const unsigned b0 = __ballot_sync(FULL, c0), b1 = __ballot_sync(FULL, c1);
-          if (b0 | b1) {
-            const int n = __popc(b0 & my_mask) + __popc(b1 & my_mask);
-            int c = __shfl_sync(FULL, my_cnt, j >= 0 ? j : 0);
-            if (__any_sync(FULL, j >= 0 && c + n > kQCap)) {  // a queue would overflow: fold every queue first
-              __syncwarp();
-              drain_queue<L>(keys, vals, tie_key, tau, my_cnt, qk, qv, lane);
-              my_cnt = 0;
-              if (owner) qtab[lq].w = tau;
-              __syncwarp();
-              c = 0;
-            }
-            if (c0) {
-              const int e = queue_slot(j, c + __popc(b0 & my_mask & lt_mask));
-              qk[e] = s2.x;
-              qv[e] = i0;
-            }
-            if (c1) {
-              const int e = queue_slot(j, c + __popc(b0 & my_mask) + __popc(b1 & my_mask & lt_mask));
-              qk[e] = s2.y;
-              qv[e] = i1;
-            }
+          for (int u = 0; u < 2; ++u) {
+            int j = jh[u * H];
 #pragma unroll
-            for (int h = 0; h < H; ++h) {
-              const unsigned m = SLOT_MASK << (h * QPW);
-              if (lane == jh[h]) my_cnt += __popc(b0 & m) + __popc(b1 & m);
+            for (int h = 1; h < H; ++h) j = (slot == h) ? jh[u * H + h] : j;
+            jr[u] = j;
+            qr[u] = qtab[warp * QPW + (j >= 0 ? j : 0)];
+          }
+#pragma unroll
+          for (int u = 0; u < 2; ++u)
+            sr[u] = key_pair(make_float2(qr[u].x, qr[u].x), make_float2(qr[u].y, qr[u].y),
+                             make_float2(qr[u].z, qr[u].z), pr);
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            if (u == 1 && jh[H] < 0) break;  // warp-uniform: no query left for round 1
+            const int j = jr[u];
+            const float2 s2 = sr[u];
+            const bool c0 = j >= 0 && s2.x <= qr[u].w, c1 = j >= 0 && s2.y <= qr[u].w;
+            const unsigned b0 = __ballot_sync(FULL, c0), b1 = __ballot_sync(FULL, c1);
+            if (b0 | b1) {
+              const int n = __popc(b0 & my_mask) + __popc(b1 & my_mask);
+              int c = __shfl_sync(FULL, my_cnt, j >= 0 ? j : 0);
+              if (__any_sync(FULL, j >= 0 && c + n > kQCap)) {  // a queue would overflow: fold every queue first
+                __syncwarp();
+                drain_queue<L>(keys, vals, tie_key, tau, my_cnt, qk, qv, lane);
+                my_cnt = 0;
+                if (owner) qtab[lq].w = tau;
+                __syncwarp();
+                c = 0;
+              }
+              if (c0) {
+                const int e = queue_slot(j, c + __popc(b0 & my_mask & lt_mask));
+                qk[e] = s2.x;
+                qv[e] = i0;
+              }
+              if (c1) {
+                const int e = queue_slot(j, c + __popc(b0 & my_mask) + __popc(b1 & my_mask & lt_mask));
+                qk[e] = s2.y;
+                qv[e] = i1;
+              }
+#pragma unroll
+              for (int h = 0; h < H; ++h) {
+                const unsigned m = SLOT_MASK << (h * QPW);
+                if (lane == jh[u * H + h]) my_cnt += __popc(b0 & m) + __popc(b1 & m);
+              }
             }
           }
         }
