@@ -86,8 +86,8 @@ struct SearchParams {
 // item is the CTA's WPC * QPW queries.  The C ABI's launch-shape code s
 // (knnag_set_search_splits, the segment tables' `splits`) selects
 //   s = 1: 4 warps x 32    s = 2: 2 x 32    s = 4: 1 x 32
-//   s = 8: 2 warps x 16    s = 16: 4 x 8
-// i.e. 128, 64, 32, 32 and 32 queries per CTA.
+//   s = 8: 2 warps x 16    s = 16: 4 x 8    s = 32: 1 x 16    s = 64: 1 x 8
+// i.e. 128, 64, 32, 32, 32, 16 and 8 queries per CTA.
 constexpr int kSearchMaxThreads = 128;
 // Candidate queue entries per query: 64 points (the points a query meets
 // between two folds of its queue) always fit.
@@ -97,10 +97,16 @@ constexpr int kQCap = 64;
 constexpr int kTileBufs = 2;
 constexpr size_t kSearchTileBytes = 8192;  // 128 points x 16 floats
 static_assert(kTileBufs * 12 + 8 <= 64, "search ring bookkeeping exceeds its 64 bytes");
-__host__ __device__ inline constexpr int search_wpc(int shape) { return shape == 1 ? 4 : shape == 2 ? 2 : shape == 4 ? 1 : shape == 8 ? 2 : 4; }
-__host__ __device__ inline constexpr int search_qpw(int shape) { return shape <= 4 ? 32 : shape == 8 ? 16 : 8; }
+__host__ __device__ inline constexpr int search_wpc(int shape) {
+  return shape == 1 ? 4 : shape == 2 ? 2 : shape == 4 ? 1 : shape == 8 ? 2 : shape == 16 ? 4 : 1;
+}
+__host__ __device__ inline constexpr int search_qpw(int shape) {
+  return shape <= 4 ? 32 : (shape == 8 || shape == 32) ? 16 : 8;
+}
 __host__ __device__ inline constexpr int search_qpc(int shape) { return search_wpc(shape) * search_qpw(shape); }
-inline bool search_shape_ok(int shape) { return shape == 1 || shape == 2 || shape == 4 || shape == 8 || shape == 16; }
+inline bool search_shape_ok(int shape) {
+  return shape == 1 || shape == 2 || shape == 4 || shape == 8 || shape == 16 || shape == 32 || shape == 64;
+}
 
 // Shared-memory layout of the search kernel with `wpc` warps of `qpw` queries:
 //   ring      kTileBufs tiles

@@ -81,7 +81,7 @@ __global__ void validate_segments_kernel(const char* cs, const void* segs, int c
   if (threadIdx.x == 0) {
     bad = (sh->magic != kSegMagic || ch->magic != kCloudSetMagic || sh->nseg < 1 || sh->nseg > cap_segs ||
            sh->total_q < 0 || sh->total_q > cap_q || sh->total_e < 0 || sh->total_e > cap_e || sh->kmax > max_k ||
-           sh->qpc != qpc || (qpc != 32 && qpc != 64 && qpc != 128) || sh->total_qcells < 0 ||
+           sh->qpc != qpc || (qpc != 8 && qpc != 16 && qpc != 32 && qpc != 64 && qpc != 128) || sh->total_qcells < 0 ||
            sh->total_qcells > cap_cells || sh->n_items < 0 || sh->bigk_q < 0 || sh->bigk_q > sh->total_q ||
            sh->grad_rows < 0 || sh->grad_rows > sh->total_q)
               ? 1

@@ -1059,6 +1059,8 @@ int launch_search_ragged_k(const SearchParams& a, int s, int64_t cap_items, cuda
     case 2: return launch_search_ragged_t<KMAX, 2, 32>(a, cap_items, st);
     case 8: return launch_search_ragged_t<KMAX, 2, 16>(a, cap_items, st);
     case 16: return launch_search_ragged_t<KMAX, 4, 8>(a, cap_items, st);
+    case 32: return launch_search_ragged_t<KMAX, 1, 16>(a, cap_items, st);
+    case 64: return launch_search_ragged_t<KMAX, 1, 8>(a, cap_items, st);
     default: return launch_search_ragged_t<KMAX, 1, 32>(a, cap_items, st);
   }
 }
@@ -1070,6 +1072,8 @@ int launch_search_k(const SearchParams& a, int s, cudaStream_t st) {
     case 2: return launch_search_t<KMAX, 2, 32>(a, st);
     case 8: return launch_search_t<KMAX, 2, 16>(a, st);
     case 16: return launch_search_t<KMAX, 4, 8>(a, st);
+    case 32: return launch_search_t<KMAX, 1, 16>(a, st);
+    case 64: return launch_search_t<KMAX, 1, 8>(a, st);
     default: return launch_search_t<KMAX, 1, 32>(a, st);
   }
 }

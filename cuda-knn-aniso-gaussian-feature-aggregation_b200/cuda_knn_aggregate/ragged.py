@@ -26,9 +26,9 @@ import torch
 from . import capi
 
 # search launch shapes (the C ABI's `splits` code): 1, 2, 4 -> 4, 2, 1 warps of
-# 32 queries per CTA; 8 -> 2 warps of 16; 16 -> 4 warps of 8
-_SPLITS = (1, 2, 4, 8, 16)
-_QPC = {1: 128, 2: 64, 4: 32, 8: 32, 16: 32}
+# 32 queries per CTA; 8 -> 2 warps of 16; 16 -> 4 warps of 8; 32 -> 1 warp of
+# 16; 64 -> 1 warp of 8
+_SPLITS = (1, 2, 4, 8, 16, 32, 64)
 
 
 def _i32(xs):
@@ -269,7 +269,7 @@ def shape_bucket(cloudset: CloudSet, Qs, Ks):
 
 def autotune_splits(cloudset: CloudSet, clouds, qs, Ks, reps=3, cache=True):
     """Search launch shape (queries per CTA and per warp, the ``splits`` codes
-    1, 2, 4, 8, 16) for steps shaped like this one: each candidate runs the step as a captured graph
+    1, 2, 4, 8, 16, 32, 64) for steps shaped like this one: each candidate runs the step as a captured graph
     ``reps`` times (after a warm-up) and the fastest median wins.  Cached per
     ``shape_bucket`` in memory and in the tuner's JSON file
     (``tuning.cache_path()``), so a later process reuses the choice."""

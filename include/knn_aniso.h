@@ -328,8 +328,9 @@ long long knnag_launch_count(void);
 /* Tuning: launch shape of the FP32 search of every later knnag_forward /
  * knnag_forward_noalloc in the process (the autotuner sets it from timings
  * cached per shape bucket): 1, 2, 4 -> CTAs of 4, 2, 1 warps of 32 queries;
- * 8 -> 2 warps of 16 queries; 16 -> 4 warps of 8 queries (fewer queries per
- * warp give more warps for small query sets); 0 restores the automatic
+ * 8 -> 2 warps of 16 queries; 16 -> 4 warps of 8 queries; 32 -> 1 warp of
+ * 16; 64 -> 1 warp of 8 (fewer queries per warp give more warps for small
+ * query sets); 0 restores the automatic
  * choice (by the warps the query set gives).  Results do not depend on it.
  * Returns KNNAG_ERR_ARG for other values.  The same codes are the `splits`
  * of segment tables.  No reference counterpart. */
