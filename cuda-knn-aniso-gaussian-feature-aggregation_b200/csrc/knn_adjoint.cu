@@ -353,7 +353,8 @@ int launch_exclusive_scan(int* count, int n, int* out, cudaStream_t st) {
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 
-int launch_build_adjacency(const int64_t* idxs, int B, int Q, int P, int K, void* adjacency, cudaStream_t st) {
+int launch_build_adjacency(const int64_t* idxs, int B, int Q, int P, int K, void* adjacency, cudaStream_t st,
+                           bool counted) {
   NvtxRange range("knnag:adjacency");
   const AdjLayout L = adj_layout(B, Q, P, K);
   char* base = static_cast<char*>(adjacency);
@@ -362,15 +363,18 @@ int launch_build_adjacency(const int64_t* idxs, int B, int Q, int P, int K, void
   int* unsorted = reinterpret_cast<int*>(base + L.unsorted);
   int* entries = reinterpret_cast<int*>(base + L.entries);
   const int n = B * Q * K, rows = B * P, qk = Q * K;  // sizes checked < 2^31 by the caller
-  if (cudaMemsetAsync(cursor, 0, (size_t)rows * 4, st) != cudaSuccess) return KNNAG_ERR_CUDA;
-  adj_count_kernel<<<blocks_for(n, 256), 256, 0, st>>>(idxs, n, qk, P, cursor);
+  if (!counted) {  // else the forward counted the entries per row already
+    if (cudaMemsetAsync(cursor, 0, (size_t)rows * 4, st) != cudaSuccess) return KNNAG_ERR_CUDA;
+    adj_count_kernel<<<blocks_for(n, 256), 256, 0, st>>>(idxs, n, qk, P, cursor);
+    note_launches(1);
+  }
   const int rc = launch_exclusive_scan(cursor, rows, rowptr, st);
   if (rc) return rc;
   adj_fill_kernel<<<blocks_for(n, 256), 256, 0, st>>>(idxs, n, qk, P, rowptr, cursor, unsorted);
   const int sort_threads = kAdjSortWarps * 32;
   adj_sort_kernel<<<blocks_for((int64_t)rows * 32, sort_threads), sort_threads, 0, st>>>(rowptr, unsorted, rows,
                                                                                        entries);
-  note_launches(3);
+  note_launches(2);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 

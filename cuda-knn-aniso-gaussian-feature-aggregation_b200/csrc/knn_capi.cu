@@ -139,6 +139,30 @@ int knnag_forward(const void* q, const void* p, const void* f, const void* sigma
                       static_cast<cudaStream_t>(stream));
 }
 
+int knnag_forward_counted(const void* q, const void* p, const void* f, const void* sigma, const void* R, int B,
+                          int Q, int P, int F, int K, int dtype, void* f_out, void* w_out, void* dists, int64_t* idxs,
+                          void* points, void* adjacency, void* workspace, size_t workspace_bytes, void* stream) {
+  if (dtype != KNNAG_F32 && dtype != KNNAG_F64) return KNNAG_ERR_DTYPE;
+  int rc = check_sizes(B, Q, P, F, K);
+  if (rc) return rc;
+  if ((int64_t)B * Q == 0) return KNNAG_OK;
+  if (!q || !p || !sigma || !R || !w_out || !dists || !idxs || !workspace || !adjacency) return KNNAG_ERR_ARG;
+  if (F > 0 && (!f || !f_out)) return KNNAG_ERR_ARG;
+  if (workspace_bytes < fwd_layout(B, Q, P, K, dtype, points == nullptr).total || !aligned16(workspace) ||
+      (points && !aligned16(points)) || !aligned16(adjacency))
+    return KNNAG_ERR_WORKSPACE;
+  return forward_impl(q, p, f, sigma, R, B, Q, P, F, K, dtype, f_out, w_out, dists, idxs, points, workspace,
+                      static_cast<cudaStream_t>(stream), adjacency);
+}
+
+int knnag_build_adjacency_counted(const int64_t* idxs, int B, int Q, int P, int K, void* adjacency, void* stream) {
+  int rc = check_sizes(B, Q, P, 0, K);
+  if (rc) return rc;
+  if (!adjacency || (!idxs && (int64_t)B * Q > 0)) return KNNAG_ERR_ARG;
+  if ((int64_t)B * P == 0) return KNNAG_OK;
+  return launch_build_adjacency(idxs, B, Q, P, K, adjacency, static_cast<cudaStream_t>(stream), true);
+}
+
 int knnag_pack_points(const void* p, const void* sigma, const void* R, int B, int P, int dtype, void* points,
                       void* stream) {
   if (dtype != KNNAG_F32 && dtype != KNNAG_F64) return KNNAG_ERR_DTYPE;

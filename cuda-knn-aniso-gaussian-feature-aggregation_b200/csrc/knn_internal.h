@@ -48,6 +48,9 @@ struct ExactParams {
   const char* cs;
   const void* segs;
   int* status;
+  // optional (uniform calls): per point row b*P + i, the number of written
+  // entries that select it (the adjacency's first pass), zeroed beforehand
+  int* adj_count;
 };
 
 struct SearchParams {
@@ -79,6 +82,8 @@ struct SearchParams {
   // and the default budget otherwise.
   int stall_visit;
   int wait_spins;
+  // optional (uniform calls): entries per point row, counted as written
+  int* adj_count;
 };
 
 // Search CTA: WPC warps (1, 2 or 4), each owning QPW queries (32, 16 or 8;
@@ -227,10 +232,13 @@ int backward_impl(const BwdArgs& x, cudaStream_t st);
 // Packs the point records; block 0 also zeroes zero_words[0..n_zero) (a
 // call's status words) so no separate memset is needed.
 int launch_pack_points(const void* p, const void* sigma, const void* R, int B, int P, int dtype, void* rec,
-                       cudaStream_t st, int* zero_words = nullptr, int n_zero = 0);
+                       cudaStream_t st, int* zero_words = nullptr, int n_zero = 0, int* zero_rows = nullptr);
+// adjacency: optional buffer (adj_layout) whose per-point entry counts the
+// forward writes, for launch_build_adjacency(..., counted = true)
 int forward_impl(const void* q, const void* p, const void* f, const void* sigma, const void* R, int B, int Q,
                  int P, int F, int K, int dtype, void* f_out, void* w_out, void* dists, int64_t* idxs,
-                 void* points, void* workspace, cudaStream_t st);
-int launch_build_adjacency(const int64_t* idxs, int B, int Q, int P, int K, void* adjacency, cudaStream_t st);
+                 void* points, void* workspace, cudaStream_t st, void* adjacency = nullptr);
+int launch_build_adjacency(const int64_t* idxs, int B, int Q, int P, int K, void* adjacency, cudaStream_t st,
+                           bool counted = false);
 
 }  // namespace knnag

@@ -25,13 +25,16 @@ __device__ __forceinline__ void store_rec(double* dst, const double (&v)[kRecLen
 }
 
 // rec[(b*P+i)*16 + field]: -p, R (row-major), sigma, pad.
+// zero_rows (optional): one int per point zeroed too (the adjacency's
+// per-point entry counts the forward accumulates).
 template <typename T>
 __global__ void pack_points_kernel(const T* __restrict__ p, const T* __restrict__ sigma,
                                    const T* __restrict__ R, int64_t n_points, T* __restrict__ rec,
-                                   int* __restrict__ zero_words, int n_zero) {
+                                   int* __restrict__ zero_words, int n_zero, int* __restrict__ zero_rows) {
   if (blockIdx.x == 0 && (int)threadIdx.x < n_zero) zero_words[threadIdx.x] = 0;  // the call's status words
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_points;
        i += (int64_t)gridDim.x * blockDim.x) {
+    if (zero_rows) zero_rows[i] = 0;
     T v[kRecLen];
     v[kNPX] = -p[i * 3 + 0];
     v[kNPY] = -p[i * 3 + 1];
@@ -278,6 +281,7 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
         a.dists[e] = slot_k[k];
         a.idxs[e] = (int64_t)slot_v[k];
         a.w_out[e] = weight_of(slot_k[k]);
+        if (a.adj_count && (unsigned)slot_v[k] < (unsigned)P) atomicAdd(&a.adj_count[b * P + slot_v[k]], 1);
       }
       __syncthreads();
       for (int k = tid; k < K; k += kReplayThreads) slot_k[k] = weight_of(slot_k[k]);
@@ -395,6 +399,7 @@ struct SearchItem {
   float* dists;
   int64_t* idxs;
   int64_t row0;        // global query row of group-local query 0
+  int* adj_count;      // the group's per-point entry counts (optional)
   int Q, P, K, ntile, qblock;
 };
 
@@ -834,9 +839,11 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     const int l = x / K, k = x - l * K;
     if (out_f[l]) continue;
     const int64_t e = (int64_t)qorig[l] * K + k;
+    const int idx = out_i[l * L + k];
     it.dists[e] = out_k[l * L + k];
-    it.idxs[e] = (int64_t)out_i[l * L + k];
+    it.idxs[e] = (int64_t)idx;
     it.w_out[e] = out_w[l * L + k];
+    if (it.adj_count) atomicAdd(&it.adj_count[idx], 1);  // idx is in [0, P): unflagged
   }
   const int F = a.F;
   const float* fb = it.f;
@@ -905,6 +912,7 @@ __global__ void __launch_bounds__(32 * WPC) search_f32_kernel(SearchParams a) {
   it.dists = a.dists + b * a.Q * a.K;
   it.idxs = a.idxs + b * a.Q * a.K;
   it.row0 = b * a.Q;
+  it.adj_count = a.adj_count ? a.adj_count + b * a.P : nullptr;
   it.Q = a.Q;
   it.P = a.P;
   it.K = a.K;
@@ -968,6 +976,7 @@ __global__ void __launch_bounds__(32 * WPC) search_ragged_kernel(SearchParams a)
       it.dists = a.dists + g.e_off;
       it.idxs = a.idxs + g.e_off;
       it.row0 = g.q_off;
+      it.adj_count = nullptr;
       it.Q = g.Q;
       it.P = c.P;
       it.K = g.K;
@@ -1167,32 +1176,35 @@ FwdLayout fwd_layout(int B, int Q, int P, int K, int dtype, bool own_rec) {
 }
 
 int launch_pack_points(const void* p, const void* sigma, const void* R, int B, int P, int dtype, void* rec,
-                       cudaStream_t st, int* zero_words, int n_zero) {
+                       cudaStream_t st, int* zero_words, int n_zero, int* zero_rows) {
   int dev = 0;
   cudaGetDevice(&dev);
   const int64_t n = (int64_t)B * P;
   if (dtype == KNNAG_F64)
     pack_points_kernel<double><<<grid_for(n, 256, dev), 256, 0, st>>>(
-        (const double*)p, (const double*)sigma, (const double*)R, n, (double*)rec, zero_words, n_zero);
+        (const double*)p, (const double*)sigma, (const double*)R, n, (double*)rec, zero_words, n_zero, zero_rows);
   else
     pack_points_kernel<float><<<grid_for(n, 256, dev), 256, 0, st>>>((const float*)p, (const float*)sigma,
                                                                      (const float*)R, n, (float*)rec, zero_words,
-                                                                     n_zero);
+                                                                     n_zero, zero_rows);
   note_launches(1);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 
 template <typename T>
 static int forward_exact_all(const T* q, const T* rec, const T* f, int B, int Q, int P, int F, int K, T* f_out,
-                             T* w_out, T* dists, int64_t* idxs, cudaStream_t st) {
+                             T* w_out, T* dists, int64_t* idxs, int* adj_count, cudaStream_t st) {
   ExactParams<T> e{q, rec, f, nullptr, nullptr, 0, B, Q, P, F, K, 0, nullptr, nullptr, f_out, w_out, dists, idxs};
+  e.adj_count = adj_count;
   return launch_exact<T>(e, st);
 }
 
 int forward_impl(const void* q, const void* p, const void* f, const void* sigma, const void* R, int B, int Q,
                  int P, int F, int K, int dtype, void* f_out, void* w_out, void* dists, int64_t* idxs,
-                 void* points, void* workspace, cudaStream_t st) {
+                 void* points, void* workspace, cudaStream_t st, void* adjacency) {
   NvtxRange range("knnag:forward");
+  int* adj_count = adjacency ? reinterpret_cast<int*>(static_cast<char*>(adjacency) + adj_layout(B, Q, P, K).cursor)
+                             : nullptr;
   const bool own_rec = points == nullptr;
   const FwdLayout L = fwd_layout(B, Q, P, K, dtype, own_rec);
   char* ws = static_cast<char*>(workspace);
@@ -1203,15 +1215,16 @@ int forward_impl(const void* q, const void* p, const void* f, const void* sigma,
   int rc;
   {
     NvtxRange r("knnag:pack_points");
-    rc = launch_pack_points(p, sigma, R, B, P, dtype, rec, st, status, 2);  // also zeroes status, flag_count
+    // also zeroes the status words and the adjacency's entry counts
+    rc = launch_pack_points(p, sigma, R, B, P, dtype, rec, st, status, 2, adj_count);
   }
   if (rc) return rc;
   if (dtype == KNNAG_F64)
     return forward_exact_all<double>((const double*)q, (const double*)rec, (const double*)f, B, Q, P, F, K,
-                                     (double*)f_out, (double*)w_out, (double*)dists, idxs, st);
+                                     (double*)f_out, (double*)w_out, (double*)dists, idxs, adj_count, st);
   if (K > 32)
     return forward_exact_all<float>((const float*)q, (const float*)rec, (const float*)f, B, Q, P, F, K,
-                                    (float*)f_out, (float*)w_out, (float*)dists, idxs, st);
+                                    (float*)f_out, (float*)w_out, (float*)dists, idxs, adj_count, st);
   int dev = 0;
   cudaGetDevice(&dev);
   float* pairs = reinterpret_cast<float*>(ws + L.pairs);
@@ -1242,6 +1255,7 @@ int forward_impl(const void* q, const void* p, const void* f, const void* sigma,
   sp.status = status;
   sp.flag_count = flag_count;
   sp.flag_list = flag_list;
+  sp.adj_count = adj_count;
   apply_search_debug(sp);
   const int G = choose_splits(B, Q, dev);
   {
@@ -1258,6 +1272,7 @@ int forward_impl(const void* q, const void* p, const void* f, const void* sigma,
   NvtxRange r("knnag:replay_flagged");
   ExactParams<float> e{(const float*)q, (const float*)rec, (const float*)f, nullptr, nullptr, 0, B, Q, P, F, K, 1,
                        flag_list, flag_count, (float*)f_out, (float*)w_out, (float*)dists, idxs};
+  e.adj_count = adj_count;
   return launch_exact<float>(e, st);
 }
 

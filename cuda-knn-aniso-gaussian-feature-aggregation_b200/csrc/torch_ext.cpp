@@ -97,9 +97,11 @@ void* stream_of(const torch::Tensor& t) { return (void*)at::cuda::getCurrentCUDA
 
 void* ptr_or_null(const c10::optional<torch::Tensor>& t) { return (t && t->defined()) ? t->data_ptr() : nullptr; }
 
+// want_adj: also count the point -> entry adjacency's rows in the forward
+// (knnag_forward_counted); the buffer is returned last.
 std::vector<torch::Tensor> forward_impl(const torch::Tensor& q, const torch::Tensor& p, const torch::Tensor& f,
                                         const torch::Tensor& sigma, const torch::Tensor& R, int64_t K,
-                                        bool want_points) {
+                                        bool want_points, bool want_adj = false) {
   const Dims d = check_inputs(q, p, f, sigma, R);
   check_k(K, d.P);
   const c10::cuda::CUDAGuard guard(q.device());
@@ -111,14 +113,25 @@ std::vector<torch::Tensor> forward_impl(const torch::Tensor& q, const torch::Ten
   if (want_points) points = torch::empty({d.B, d.P, 16}, p.options());
   const size_t ws_bytes = knnag_forward_workspace_bytes(d.B, d.Q, d.P, d.F, (int)K, d.dtype);
   auto ws = scratch(ws_bytes, q);
-  const int rc = knnag_forward(q.data_ptr(), p.data_ptr(), f.data_ptr(), sigma.data_ptr(), R.data_ptr(), d.B, d.Q,
+  torch::Tensor adj;
+  int rc;
+  if (want_adj) {
+    adj = scratch(knnag_adjacency_bytes(d.B, d.Q, d.P, (int)K), q);
+    rc = knnag_forward_counted(q.data_ptr(), p.data_ptr(), f.data_ptr(), sigma.data_ptr(), R.data_ptr(), d.B, d.Q,
                                d.P, d.F, (int)K, d.dtype, f_out.data_ptr(), w_out.data_ptr(), dists.data_ptr(),
-                               idxs.data_ptr<int64_t>(), want_points ? points.data_ptr() : nullptr, ws.data_ptr(),
-                               ws_bytes, stream_of(q));
+                               idxs.data_ptr<int64_t>(), want_points ? points.data_ptr() : nullptr, adj.data_ptr(),
+                               ws.data_ptr(), ws_bytes, stream_of(q));
+  } else {
+    rc = knnag_forward(q.data_ptr(), p.data_ptr(), f.data_ptr(), sigma.data_ptr(), R.data_ptr(), d.B, d.Q, d.P, d.F,
+                       (int)K, d.dtype, f_out.data_ptr(), w_out.data_ptr(), dists.data_ptr(), idxs.data_ptr<int64_t>(),
+                       want_points ? points.data_ptr() : nullptr, ws.data_ptr(), ws_bytes, stream_of(q));
+  }
   check_status(rc, "knn_aggregate_aniso_forward");
   check_device_status(ws, stream_of(q), "knn_aggregate_aniso_forward");
-  if (want_points) return {f_out, w_out, dists, idxs, points};
-  return {f_out, w_out, dists, idxs};
+  std::vector<torch::Tensor> out{f_out, w_out, dists, idxs};
+  if (want_points) out.push_back(points);
+  if (want_adj) out.push_back(adj);
+  return out;
 }
 
 void check_idxs(const torch::Tensor& idxs, const Dims& d) {
@@ -312,35 +325,55 @@ std::vector<torch::Tensor> forward_ex(torch::Tensor q, torch::Tensor p, torch::T
   return forward_impl(q, p, f, sigma, R, K, true);
 }
 
+// The adjacency of idxs; `counted` (optional): the buffer a counting
+// forward wrote the per-row entry counts into -- it is completed in place.
+torch::Tensor build_adjacency_impl(const torch::Tensor& idxs, int64_t P, const torch::Tensor& counted, void* stream) {
+  const int B = (int)idxs.size(0), Q = (int)idxs.size(1), K = (int)idxs.size(2);
+  check_k(K, (int)P);
+  if (counted.defined() && counted.numel() > 0) {
+    TORCH_CHECK(counted.is_cuda() && counted.scalar_type() == torch::kUInt8 &&
+                    (size_t)counted.numel() >= knnag_adjacency_bytes(B, Q, (int)P, K),
+                "counted adjacency must be the uint8 CUDA buffer of a counting forward");
+    check_status(knnag_build_adjacency_counted(idxs.data_ptr<int64_t>(), B, Q, (int)P, K, counted.data_ptr(), stream),
+                 "build_adjacency");
+    return counted;
+  }
+  auto adj = scratch(knnag_adjacency_bytes(B, Q, (int)P, K), idxs);
+  check_status(knnag_build_adjacency(idxs.data_ptr<int64_t>(), B, Q, (int)P, K, adj.data_ptr(), stream),
+               "build_adjacency");
+  return adj;
+}
+
 torch::Tensor build_adjacency(torch::Tensor idxs, int64_t P) {
   KNN_CHECK_INPUT(idxs);
   TORCH_CHECK(idxs.scalar_type() == torch::kInt64 && idxs.dim() == 3, "idxs must be int64 [B, Q, K]");
-  const int B = (int)idxs.size(0), Q = (int)idxs.size(1), K = (int)idxs.size(2);
-  check_k(K, (int)P);
   const c10::cuda::CUDAGuard guard(idxs.device());
-  auto adj = scratch(knnag_adjacency_bytes(B, Q, (int)P, K), idxs);
-  check_status(knnag_build_adjacency(idxs.data_ptr<int64_t>(), B, Q, (int)P, K, adj.data_ptr(), stream_of(idxs)),
-               "build_adjacency");
-  return adj;
+  return build_adjacency_impl(idxs, P, torch::Tensor(), stream_of(idxs));
 }
 
 // The same on a pool stream forked from the current one, so that it runs
 // beside the next kernels of the current stream.  The buffer is allocated on
 // the current stream; the caller must call join.block(current stream)
 // before the buffer is used or released there.
-torch::Tensor build_adjacency_forked(const torch::Tensor& idxs, int64_t P, at::cuda::CUDAEvent& join) {
+torch::Tensor build_adjacency_forked(const torch::Tensor& idxs, int64_t P, at::cuda::CUDAEvent& join,
+                                     const torch::Tensor& counted) {
   const int B = (int)idxs.size(0), Q = (int)idxs.size(1), K = (int)idxs.size(2);
   check_k(K, (int)P);
   const c10::cuda::CUDAGuard guard(idxs.device());
-  auto adj = scratch(knnag_adjacency_bytes(B, Q, (int)P, K), idxs);
+  // a fresh buffer is allocated here, on the current stream, before the fork
+  const bool use_counted = counted.defined() && counted.numel() > 0;
+  torch::Tensor fresh;
+  if (!use_counted) fresh = scratch(knnag_adjacency_bytes(B, Q, (int)P, K), idxs);
   const auto dev = idxs.device().index();
   auto main = at::cuda::getCurrentCUDAStream(dev);
   auto side = at::cuda::getStreamFromPool(false, dev);
   at::cuda::CUDAEvent fork;
   fork.record(main);
   fork.block(side);
-  check_status(knnag_build_adjacency(idxs.data_ptr<int64_t>(), B, Q, (int)P, K, adj.data_ptr(), side.stream()),
-               "build_adjacency");
+  torch::Tensor adj = use_counted ? build_adjacency_impl(idxs, P, counted, side.stream()) : fresh;
+  if (!use_counted)
+    check_status(knnag_build_adjacency(idxs.data_ptr<int64_t>(), B, Q, (int)P, K, adj.data_ptr(), side.stream()),
+                 "build_adjacency");
   join.record(side);
   return adj;
 }
@@ -410,16 +443,20 @@ bool is_broadcast_scalar(const torch::Tensor& g) {
 }
 
 struct AggBackwardFn : public torch::autograd::Function<AggBackwardFn> {
-  // differentiable inputs: gfo, q, p, f, sigma, R; then idxs, points (no grad)
+  // differentiable inputs: gfo, q, p, f, sigma, R; then idxs, points and the
+  // adjacency counted by the forward (empty if none) (no grad)
   static variable_list forward(AutogradContext* ctx, torch::Tensor gfo, torch::Tensor q, torch::Tensor p,
                                torch::Tensor f, torch::Tensor sigma, torch::Tensor R, torch::Tensor idxs,
-                               torch::Tensor points, int64_t needs) {
+                               torch::Tensor points, torch::Tensor adj_counted, int64_t needs) {
     torch::Tensor adj;
     at::cuda::CUDAEvent join;
     const bool forked = (needs & kPrebuildAdjacency) && !(needs & kPointBits);
     needs &= ~kPrebuildAdjacency;
-    if (needs & kPointBits) adj = build_adjacency(idxs, p.size(1));
-    if (forked) adj = build_adjacency_forked(idxs, p.size(1), join);
+    if (needs & kPointBits) {
+      const c10::cuda::CUDAGuard guard(idxs.device());
+      adj = build_adjacency_impl(idxs, p.size(1), adj_counted, stream_of(idxs));
+    }
+    if (forked) adj = build_adjacency_forked(idxs, p.size(1), join, adj_counted);
     auto o = backward_impl(1, c10::nullopt, gfo, q, p, f, sigma, R, c10::nullopt, idxs, points,
                            (adj.defined() && !forked) ? c10::optional<torch::Tensor>(adj) : c10::nullopt,
                            c10::nullopt, needs, true);
@@ -434,7 +471,7 @@ struct AggBackwardFn : public torch::autograd::Function<AggBackwardFn> {
   }
 
   static variable_list backward(AutogradContext* ctx, variable_list gg) {
-    variable_list out(9);
+    variable_list out(10);
     if (gg.empty() || !gg[0].defined()) return out;  // only dq is differentiated
     int64_t needs = 0;
     if (ctx->needs_input_grad(0)) needs |= KNNAG_NEED_DGFO;
@@ -457,9 +494,13 @@ struct AggBackwardFn : public torch::autograd::Function<AggBackwardFn> {
 struct AggFn : public torch::autograd::Function<AggFn> {
   static variable_list forward(AutogradContext* ctx, torch::Tensor q, torch::Tensor p, torch::Tensor f,
                                torch::Tensor sigma, torch::Tensor R, int64_t K) {
-    auto o = forward_impl(q, p, f, sigma, R, K, true);
+    // a point input that requires grad: its backward will want the
+    // adjacency, whose first pass (row counts) the forward makes for free
+    const bool want_adj = p.requires_grad() || f.requires_grad() || sigma.requires_grad() || R.requires_grad();
+    auto o = forward_impl(q, p, f, sigma, R, K, true, want_adj);
     ctx->save_for_backward({q, p, f, sigma, R, o[3]});
     ctx->saved_data["points"] = o[4];
+    if (want_adj) ctx->saved_data["adj_counted"] = o[5];
     ctx->set_materialize_grads(false);
     return {o[0], o[1], o[2], o[3]};
   }
@@ -477,8 +518,10 @@ struct AggFn : public torch::autograd::Function<AggFn> {
     // this graph may want point gradients (the Eikonal step does)
     const bool prebuild = torch::GradMode::is_enabled() &&
                           (s[1].requires_grad() || s[2].requires_grad() || s[3].requires_grad() || s[4].requires_grad());
+    torch::Tensor counted;
+    if (ctx->saved_data.count("adj_counted")) counted = ctx->saved_data["adj_counted"].toTensor();
     auto r = AggBackwardFn::apply(scalar ? g[0] : g[0].contiguous(), s[0], s[1], s[2], s[3], s[4], s[5],
-                                  ctx->saved_data["points"].toTensor(),
+                                  ctx->saved_data["points"].toTensor(), or_placeholder(counted, s[5]),
                                   needs | (scalar ? KNNAG_GFO_SCALAR : 0) | (prebuild ? kPrebuildAdjacency : 0));
     for (int i = 0; i < 5; ++i) out[i] = (needs & kNeedBits[i]) ? r[i] : torch::Tensor();
     return out;

@@ -53,6 +53,8 @@ _SIGS = {
     "knnag_pack_points": ([_V, _V, _V, _I, _I, _I, _V, _V], _I),
     "knnag_adjacency_bytes": ([_I, _I, _I, _I], _S),
     "knnag_build_adjacency": ([_V, _I, _I, _I, _I, _V, _V], _I),
+    "knnag_forward_counted": ([_V] * 5 + [_I] * 6 + [_V] * 4 + [_V, _V, _V, _S, _V], _I),
+    "knnag_build_adjacency_counted": ([_V, _I, _I, _I, _I, _V, _V], _I),
     "knnag_backward_workspace_bytes": ([_I, _I, _I, _I, _I, _I], _S),
     "knnag_backward": ([_V] * 9 + [_I] * 7 + [_V, _V] + [_V] * 6 + [_V, _S, _V], _I),
     "knnag_backward_2nd": ([_V] * 10 + [_I] * 7 + [_V, _V, _V] + [_V] * 6 + [_V, _S, _V], _I),
@@ -203,6 +205,25 @@ def build_adjacency(idxs, P):
     adj = torch.empty(max(nb, 1), dtype=torch.uint8, device=idxs.device)
     _check(lib().knnag_build_adjacency(_p(idxs), B, Q, P, K, _p(adj), _stream(idxs.device)))
     return adj
+
+
+def forward_counted(q, p, f, sigma, R, K):
+    """knnag_forward_counted, then knnag_build_adjacency_counted: returns
+    (f_out, w_out, dists, idxs, adjacency)."""
+    B, Q, P, F = q.shape[0], q.shape[1], p.shape[1], f.shape[2]
+    dt = _dtype(q)
+    o = dict(dtype=q.dtype, device=q.device)
+    f_out, w_out, dists = torch.empty(B, Q, F, **o), torch.empty(B, Q, K, **o), torch.empty(B, Q, K, **o)
+    idxs = torch.empty(B, Q, K, dtype=torch.int64, device=q.device)
+    nb = lib().knnag_forward_workspace_bytes(B, Q, P, F, K, dt)
+    ws = torch.empty(max(nb, 1), dtype=torch.uint8, device=q.device)
+    na = lib().knnag_adjacency_bytes(B, Q, P, K)
+    adj = torch.empty(max(na, 1), dtype=torch.uint8, device=q.device)
+    st = _stream(q.device)
+    _check(lib().knnag_forward_counted(_p(q), _p(p), _p(f), _p(sigma), _p(R), B, Q, P, F, K, dt, _p(f_out), _p(w_out),
+                                       _p(dists), _p(idxs), None, _p(adj), _p(ws), nb, st))
+    _check(lib().knnag_build_adjacency_counted(_p(idxs), B, Q, P, K, _p(adj), st))
+    return f_out, w_out, dists, idxs, adj
 
 
 def adjacency_arrays(adj, B, Q, P, K):

@@ -184,6 +184,24 @@ size_t knnag_adjacency_bytes(int B, int Q, int P, int K);
  */
 int knnag_build_adjacency(const int64_t* idxs, int B, int Q, int P, int K, void* adjacency, void* stream);
 
+/*
+ * knnag_forward that also makes the first pass of the point -> entry
+ * adjacency: for every point (b, i) it counts the entries e with
+ * idxs[e] == i into `adjacency` (knnag_adjacency_bytes(B, Q, P, K), 16-byte
+ * aligned), as the entries are written; knnag_build_adjacency_counted on the
+ * same buffer and idxs then skips that pass.  A caller that will need
+ * point-side gradients (it wants dp, df, dsigma or dR) saves the counting
+ * launch of the backward this way.  No reference counterpart.
+ */
+int knnag_forward_counted(const void* q, const void* p, const void* f, const void* sigma, const void* R,
+                          int B, int Q, int P, int F, int K, int dtype,
+                          void* f_out, void* w_out, void* dists, int64_t* idxs,
+                          void* points, void* adjacency, void* workspace, size_t workspace_bytes, void* stream);
+
+/* knnag_build_adjacency for a buffer whose per-point counts were written by
+ * knnag_forward_counted with these idxs (and not used since). */
+int knnag_build_adjacency_counted(const int64_t* idxs, int B, int Q, int P, int K, void* adjacency, void* stream);
+
 /* --------------------------------------------------------------- backward */
 
 /* Bytes of scratch knnag_backward / knnag_backward_2nd need. */

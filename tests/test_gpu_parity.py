@@ -202,3 +202,30 @@ def test_search_splits_setting_does_not_change_results():
             assert torch.equal(a, b)
     with pytest.raises(RuntimeError):
         capi.set_search_splits(3)
+
+
+@pytest.mark.parametrize("shape", [dict(B=2, Q=3000, P=2000, F=16, K=16), dict(B=1, Q=500, P=300, F=8, K=40),
+                                   dict(B=2, Q=200, P=300, F=6, K=9, dtype=torch.float64)])
+def test_counting_forward_gives_the_same_adjacency(shape):
+    """knnag_forward_counted + knnag_build_adjacency_counted: the same outputs
+    as knnag_forward and the same rowptr / sorted entries as a full
+    knnag_build_adjacency, on the search path, the exact path (K > 32) and
+    FP64."""
+    from cuda_knn_aggregate import workloads as W
+
+    shape = dict(shape)
+    K = shape.pop("K")
+    dtype = shape.pop("dtype", torch.float32)
+    _, t = W.make("small", K=K, seed=61, dtype=dtype, **shape)
+    x = [a.cuda() for a in t]
+    C = capi()
+    ref = C.forward(*x, K)
+    *outs, adj = C.forward_counted(*x, K)
+    for a, b in zip(ref, outs):
+        assert torch.equal(a, b)
+    B, Q, P = shape["B"], shape["Q"], shape["P"]
+    full = C.build_adjacency(ref[3], P)
+    torch.cuda.synchronize()
+    r0, e0 = C.adjacency_arrays(full, B, Q, P, K)
+    r1, e1 = C.adjacency_arrays(adj, B, Q, P, K)
+    assert torch.equal(r0, r1) and torch.equal(e0, e1)
