@@ -149,7 +149,7 @@ static_assert((size_t)33 * 12 + 4 <= (size_t)kQCap * 8, "epilogue staging exceed
 // the caller passed no points buffer) | pair tiles (FP32 fast path).
 struct FwdLayout {
   size_t status, flag_list, rec, pairs, total;
-  // spatial index (FP32 search path): bounds [B*8], cell counts / offsets
+  // spatial index (FP32 search path): bound parts [B*kBoundParts*8], cell counts / offsets
   // [B*cells(+1)], point and query permutations, tile boxes [B*ntile*8]
   size_t bounds, cell_count, cell_offset, perm_p, perm_q, tinfo;
   int P_pad, bits;
@@ -233,6 +233,13 @@ int backward_impl(const BwdArgs& x, cudaStream_t st);
 // call's status words) so no separate memset is needed.
 int launch_pack_points(const void* p, const void* sigma, const void* R, int B, int P, int dtype, void* rec,
                        cudaStream_t st, int* zero_words = nullptr, int n_zero = 0, int* zero_rows = nullptr);
+// Chunks per batch element of the FP32 packing kernel that also bounds the
+// points: chunk c of element b writes its box to parts[(b * kBoundParts +
+// c) * 8 ...] (min xyz, max xyz), which the cell kernels reduce.
+constexpr int kBoundParts = 32;
+int launch_pack_points_bounded(const float* p, const float* sigma, const float* R, int B, int P, float* rec,
+                               float* parts, cudaStream_t st, int* zero_words, int n_zero, int* zero_rows,
+                               int* zero_cells, int64_t n_cells);
 // adjacency: optional buffer (adj_layout) whose per-point entry counts the
 // forward writes, for launch_build_adjacency(..., counted = true)
 int forward_impl(const void* q, const void* p, const void* f, const void* sigma, const void* R, int B, int Q,

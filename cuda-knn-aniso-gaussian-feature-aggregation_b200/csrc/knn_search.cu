@@ -24,6 +24,72 @@ __device__ __forceinline__ void store_rec(double* dst, const double (&v)[kRecLen
   for (int m = 0; m < kRecLen; m += 2) *reinterpret_cast<double2*>(dst + m) = make_double2(v[m], v[m + 1]);
 }
 
+// One record from p, sigma, R (the shared body of the packing kernels).
+template <typename T>
+__device__ __forceinline__ void pack_one(const T* __restrict__ p, const T* __restrict__ sigma,
+                                         const T* __restrict__ R, int64_t i, T* __restrict__ rec) {
+  T v[kRecLen];
+  v[kNPX] = -p[i * 3 + 0];
+  v[kNPY] = -p[i * 3 + 1];
+  v[kNPZ] = -p[i * 3 + 2];
+#pragma unroll
+  for (int m = 0; m < 9; ++m) v[kR00 + m] = R[i * 9 + m];
+  v[kS0] = sigma[i * 3 + 0];
+  v[kS1] = sigma[i * 3 + 1];
+  v[kS2] = sigma[i * 3 + 2];
+  v[kRecPad] = T(0);
+  store_rec(rec + i * kRecLen, v);
+}
+
+// FP32 packing of the search path, grid (kBoundParts, B): CTA (c, b) packs
+// chunk c of batch element b's points, writes the chunk's bounding box to
+// parts (what the cell kernels reduce to the element's box), zeroes the
+// chunk's adjacency counts (zero_rows, optional) and its share of the cell
+// counts; CTA (0, 0) zeroes the call's status words.
+__global__ void __launch_bounds__(256) pack_points_bounded_kernel(
+    const float* __restrict__ p, const float* __restrict__ sigma, const float* __restrict__ R, int P,
+    float* __restrict__ rec, float* __restrict__ parts, int* __restrict__ zero_words, int n_zero,
+    int* __restrict__ zero_rows, int* __restrict__ zero_cells, int64_t n_cells) {
+  __shared__ float red[6][8];
+  const int c = blockIdx.x, b = blockIdx.y, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (c == 0 && b == 0 && tid < n_zero) zero_words[tid] = 0;
+  const int64_t flat = ((int64_t)b * gridDim.x + c) * blockDim.x + tid;
+  const int64_t nthreads = (int64_t)gridDim.x * gridDim.y * blockDim.x;
+  for (int64_t i = flat; i < n_cells; i += nthreads) zero_cells[i] = 0;
+  const int chunk = (P + kBoundParts - 1) / kBoundParts;
+  const int i0 = min(P, c * chunk), i1 = min(P, i0 + chunk);
+  float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int k = i0 + tid; k < i1; k += blockDim.x) {
+    const int64_t i = (int64_t)b * P + k;
+    pack_one<float>(p, sigma, R, i, rec);
+    if (zero_rows) zero_rows[i] = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float v = p[i * 3 + a];
+      mn[a] = fminf(mn[a], v);
+      mx[a] = fmaxf(mx[a], v);
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mn[a] = fminf(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], o));
+      mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
+    }
+  if (lane == 0)
+    for (int a = 0; a < 3; ++a) {
+      red[a][warp] = mn[a];
+      red[3 + a][warp] = mx[a];
+    }
+  __syncthreads();
+  if (tid < 6) {
+    float v = tid < 3 ? INFINITY : -INFINITY;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v = tid < 3 ? fminf(v, red[tid][w]) : fmaxf(v, red[tid][w]);
+    parts[((int64_t)b * kBoundParts + c) * 8 + tid] = v;
+  }
+}
+
 // rec[(b*P+i)*16 + field]: -p, R (row-major), sigma, pad.
 // zero_rows (optional): one int per point zeroed too (the adjacency's
 // per-point entry counts the forward accumulates).
@@ -35,17 +101,7 @@ __global__ void pack_points_kernel(const T* __restrict__ p, const T* __restrict_
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_points;
        i += (int64_t)gridDim.x * blockDim.x) {
     if (zero_rows) zero_rows[i] = 0;
-    T v[kRecLen];
-    v[kNPX] = -p[i * 3 + 0];
-    v[kNPY] = -p[i * 3 + 1];
-    v[kNPZ] = -p[i * 3 + 2];
-#pragma unroll
-    for (int m = 0; m < 9; ++m) v[kR00 + m] = R[i * 9 + m];
-    v[kS0] = sigma[i * 3 + 0];
-    v[kS1] = sigma[i * 3 + 1];
-    v[kS2] = sigma[i * 3 + 2];
-    v[kRecPad] = T(0);
-    store_rec(rec + i * kRecLen, v);
+    pack_one<T>(p, sigma, R, i, rec);
   }
 }
 
@@ -1158,8 +1214,8 @@ FwdLayout fwd_layout(int B, int Q, int P, int K, int dtype, bool own_rec) {
     const size_t cells = (size_t)1 << (3 * L.bits);
     L.pairs = off;
     off += align256((size_t)B * L.P_pad * kRecLen * 4);
-    L.bounds = off;
-    off += align256((size_t)B * 8 * 4);
+    L.bounds = off;  // per element kBoundParts partial boxes
+    off += align256((size_t)B * kBoundParts * 8 * 4);
     // point and query cells of each batch element, sorted together
     L.cell_count = off;
     off += align256(2 * (size_t)B * cells * 4);
@@ -1173,6 +1229,15 @@ FwdLayout fwd_layout(int B, int Q, int P, int K, int dtype, bool own_rec) {
   }
   L.total = off;
   return L;
+}
+
+int launch_pack_points_bounded(const float* p, const float* sigma, const float* R, int B, int P, float* rec,
+                               float* parts, cudaStream_t st, int* zero_words, int n_zero, int* zero_rows,
+                               int* zero_cells, int64_t n_cells) {
+  pack_points_bounded_kernel<<<dim3(kBoundParts, B), 256, 0, st>>>(p, sigma, R, P, rec, parts, zero_words, n_zero,
+                                                                   zero_rows, zero_cells, n_cells);
+  note_launches(1);
+  return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 
 int launch_pack_points(const void* p, const void* sigma, const void* R, int B, int P, int dtype, void* rec,
@@ -1213,10 +1278,18 @@ int forward_impl(const void* q, const void* p, const void* f, const void* sigma,
   int* flag_list = reinterpret_cast<int*>(ws + L.flag_list);
   void* rec = own_rec ? (void*)(ws + L.rec) : points;
   int rc;
+  const bool search_path = dtype == KNNAG_F32 && K <= 32;
   {
     NvtxRange r("knnag:pack_points");
-    // also zeroes the status words and the adjacency's entry counts
-    rc = launch_pack_points(p, sigma, R, B, P, dtype, rec, st, status, 2, adj_count);
+    // also zeroes the status words and the adjacency's entry counts; on
+    // the search path also the cell counts, and it bounds the points
+    if (search_path)
+      rc = launch_pack_points_bounded((const float*)p, (const float*)sigma, (const float*)R, B, P, (float*)rec,
+                                      reinterpret_cast<float*>(ws + L.bounds), st, status, 2, adj_count,
+                                      reinterpret_cast<int*>(ws + L.cell_count),
+                                      2 * (int64_t)B << (3 * L.bits));
+    else
+      rc = launch_pack_points(p, sigma, R, B, P, dtype, rec, st, status, 2, adj_count);
   }
   if (rc) return rc;
   if (dtype == KNNAG_F64)

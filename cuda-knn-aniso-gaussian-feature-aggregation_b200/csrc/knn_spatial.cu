@@ -162,15 +162,36 @@ struct CellJob {
   int stride, negate;
   GroupMap m;
   int cell_base;
+  int nparts;  // > 0: bnd holds nparts partial boxes per group, reduced here
 };
+
+// The box of group r: bnd's entry, or the reduction of its nparts partial
+// boxes (into shared memory, by the first threads of the CTA; all threads
+// of the CTA must call this).
+__device__ __forceinline__ const float* job_bounds(const CellJob& j, const float* bnd, const GroupRange& r,
+                                                   float* gbs) {
+  if (j.nparts <= 0) return group_bounds(j.m, bnd) + r.bnd * 8;
+  if (threadIdx.x < 6) {
+    const int a = threadIdx.x;
+    float v = a < 3 ? INFINITY : -INFINITY;
+    for (int i = 0; i < j.nparts; ++i) {
+      const float x = bnd[((int64_t)r.bnd * j.nparts + i) * 8 + a];
+      v = a < 3 ? fminf(v, x) : fmaxf(v, x);
+    }
+    gbs[a] = v;
+  }
+  __syncthreads();
+  return gbs;
+}
 
 // Cell histogram of the elements of group blockIdx.y of job blockIdx.z.
 __global__ void cell_count_kernel(CellJob j0, CellJob j1, const float* __restrict__ bnd, int* __restrict__ count) {
+  __shared__ float gbs[6];
   const CellJob& j = blockIdx.z ? j1 : j0;
   GroupRange r;
   if (!group_range(j.m, blockIdx.y, r)) return;
   const float s = j.negate ? -1.f : 1.f;
-  const float* gb = group_bounds(j.m, bnd) + r.bnd * 8;
+  const float* gb = job_bounds(j, bnd, r, gbs);
   int* cnt = count + j.cell_base + r.cell_off;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n; i += gridDim.x * blockDim.x) {
     const float* v = j.xyz + (r.start + i) * j.stride;
@@ -181,11 +202,12 @@ __global__ void cell_count_kernel(CellJob j0, CellJob j1, const float* __restric
 // perm[offset[cell] + rank] = index within the group.
 __global__ void cell_scatter_kernel(CellJob j0, CellJob j1, const float* __restrict__ bnd,
                                     const int* __restrict__ offset, int* __restrict__ cursor, int* __restrict__ perm) {
+  __shared__ float gbs[6];
   const CellJob& j = blockIdx.z ? j1 : j0;
   GroupRange r;
   if (!group_range(j.m, blockIdx.y, r)) return;
   const float s = j.negate ? -1.f : 1.f;
-  const float* gb = group_bounds(j.m, bnd) + r.bnd * 8;
+  const float* gb = job_bounds(j, bnd, r, gbs);
   const int base = j.cell_base + r.cell_off;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n; i += gridDim.x * blockDim.x) {
     const float* v = j.xyz + (r.start + i) * j.stride;
@@ -356,21 +378,20 @@ int launch_spatial_index(const float* q, const float* rec, int B, int Q, int P, 
   const int ntile = P_pad / kTilePoints;
   GroupMap pm{P, bits, nullptr, nullptr, nullptr, nullptr, nullptr};
   GroupMap qm{Q, bits, nullptr, nullptr, nullptr, nullptr, nullptr};
-  point_bounds_kernel<<<B, 512, 0, st>>>(rec, pm, bnd);
-  // points and queries in one counting sort: their cells are scanned
-  // together, so the queries' positions start after all points' and land in
-  // perm_q, which follows perm_p
+  // the packing kernel wrote kBoundParts partial boxes per element (reduced
+  // by the cell kernels) and zeroed the cell counts.  Points and queries in
+  // one counting sort: their cells are scanned together, so the queries'
+  // positions start after all points' and land in perm_q, which follows perm_p
   const int64_t nc = 2 * (int64_t)B * cells;
-  if (cudaMemsetAsync(cnt, 0, (size_t)nc * 4, st) != cudaSuccess) return KNNAG_ERR_CUDA;
-  const CellJob jp{rec + kNPX, kRecLen, 1, pm, 0};
-  const CellJob jq{q, 3, 0, qm, B * cells};
+  const CellJob jp{rec + kNPX, kRecLen, 1, pm, 0, kBoundParts};
+  const CellJob jq{q, 3, 0, qm, B * cells, kBoundParts};
   const dim3 grid(grid_x(P > Q ? P : Q, sms, B), B, 2);
   cell_count_kernel<<<grid, 256, 0, st>>>(jp, jq, bnd, cnt);
   int rc = launch_exclusive_scan(cnt, (int)nc, off, st);
   if (rc) return rc;
   cell_scatter_kernel<<<grid, 256, 0, st>>>(jp, jq, bnd, off, cnt, perm);
   tile_info_kernel<<<dim3(ntile, B), kTilePoints, 0, st>>>(rec, perm, nullptr, P, ntile, pairs, tinfo);
-  note_launches(4);  // + 1 scan, counted by launch_exclusive_scan
+  note_launches(3);  // + 1 scan, counted by launch_exclusive_scan
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
 
@@ -390,7 +411,7 @@ int launch_cloudset_index(char* cs, const CloudSetHeader& h, const CloudDesc* cd
   GroupMap pm{0, 0, cd_dev, nullptr, nullptr, nullptr, nullptr};
   point_bounds_kernel<<<C, 512, 0, st>>>(rec, pm, bnd);
   if (cudaMemsetAsync(cnt, 0, (size_t)h.total_cells * 4, st) != cudaSuccess) return KNNAG_ERR_CUDA;
-  const CellJob jp{rec + kNPX, kRecLen, 1, pm, 0};
+  const CellJob jp{rec + kNPX, kRecLen, 1, pm, 0, 0};
   const dim3 grid(grid_x(max_p, sms, C), C, 1);
   cell_count_kernel<<<grid, 256, 0, st>>>(jp, jp, bnd, cnt);
   int rc = launch_exclusive_scan(cnt, h.total_cells, off, st);
@@ -415,7 +436,7 @@ int launch_query_order(const float* q, const char* cs, const void* segs_dev, int
   GroupMap qm{0, 0, nullptr, seg_descs(segs_dev), static_cast<const SegHeader*>(segs_dev), cs, status};
   if (cudaMemsetAsync(cnt, 0, (size_t)cap_cells * 4, st) != cudaSuccess) return KNNAG_ERR_CUDA;
   const dim3 grid(grid_x(cap_q, sms, cap_segs), cap_segs, 1);
-  const CellJob jq{q, 3, 0, qm, 0};
+  const CellJob jq{q, 3, 0, qm, 0, 0};
   cell_count_kernel<<<grid, 256, 0, st>>>(jq, jq, nullptr, cnt);
   int rc = launch_exclusive_scan(cnt, cap_cells, off, st);
   if (rc) return rc;
