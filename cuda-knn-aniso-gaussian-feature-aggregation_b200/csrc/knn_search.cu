@@ -1284,10 +1284,12 @@ int forward_impl(const void* q, const void* p, const void* f, const void* sigma,
     // also zeroes the status words and the adjacency's entry counts; on
     // the search path also the cell counts, and it bounds the points
     if (search_path)
+      // cell counts and offsets (the offsets are the scatter's cursors when
+      // the scan is folded into it) are zeroed, padding between them included
       rc = launch_pack_points_bounded((const float*)p, (const float*)sigma, (const float*)R, B, P, (float*)rec,
                                       reinterpret_cast<float*>(ws + L.bounds), st, status, 2, adj_count,
                                       reinterpret_cast<int*>(ws + L.cell_count),
-                                      2 * (int64_t)B << (3 * L.bits));
+                                      (int64_t)(L.cell_offset - L.cell_count) / 4 + (2 * (int64_t)B << (3 * L.bits)) + 1);
     else
       rc = launch_pack_points(p, sigma, R, B, P, dtype, rec, st, status, 2, adj_count);
   }

@@ -216,6 +216,61 @@ __global__ void cell_scatter_kernel(CellJob j0, CellJob j1, const float* __restr
   }
 }
 
+// The scatter with the scan folded in, for at most kScatterScanMax cells:
+// every CTA scans the cell counts into shared memory itself (a few KB
+// read from L2), so no separate scan launch sits between the count and the
+// scatter; `cursor` (zeroed beforehand) ranks the elements of a cell.
+constexpr int kScatterScanMax = 8192;
+
+__global__ void __launch_bounds__(256) cell_scatter_scan_kernel(CellJob j0, CellJob j1, const float* __restrict__ bnd,
+                                                                const int* __restrict__ count, int nc,
+                                                                int* __restrict__ cursor, int* __restrict__ perm) {
+  __shared__ int soff[kScatterScanMax];
+  __shared__ int wsum[8];
+  __shared__ float gbs[6];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int per = (nc + 255) / 256;  // <= 32 consecutive counts per thread
+  int local = 0;
+  for (int u = 0; u < per; ++u) {
+    const int i = tid * per + u;
+    if (i < nc) {
+      const int v = count[i];
+      soff[i] = v;
+      local += v;
+    }
+  }
+  int incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  int run = incl - local;
+  for (int w = 0; w < warp; ++w) run += wsum[w];
+  for (int u = 0; u < per; ++u) {
+    const int i = tid * per + u;
+    if (i < nc) {
+      const int v = soff[i];
+      soff[i] = run;
+      run += v;
+    }
+  }
+  __syncthreads();
+  const CellJob& j = blockIdx.z ? j1 : j0;
+  GroupRange r;
+  if (!group_range(j.m, blockIdx.y, r)) return;
+  const float s = j.negate ? -1.f : 1.f;
+  const float* gb = job_bounds(j, bnd, r, gbs);
+  const int base = j.cell_base + r.cell_off;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n; i += gridDim.x * blockDim.x) {
+    const float* v = j.xyz + (r.start + i) * j.stride;
+    const int c = base + (int)cell_of(s * v[0], s * v[1], s * v[2], gb, r.bits);
+    perm[soff[c] + atomicAdd(&cursor[c], 1)] = i;
+  }
+}
+
 // Point groups of the tile kernels: uniform (group b: records [b*P, ...),
 // tiles [b*ntile, ...)) or the clouds of a cloud set.
 struct TileGroup {
@@ -387,9 +442,15 @@ int launch_spatial_index(const float* q, const float* rec, int B, int Q, int P, 
   const CellJob jq{q, 3, 0, qm, B * cells, kBoundParts};
   const dim3 grid(grid_x(P > Q ? P : Q, sms, B), B, 2);
   cell_count_kernel<<<grid, 256, 0, st>>>(jp, jq, bnd, cnt);
-  int rc = launch_exclusive_scan(cnt, (int)nc, off, st);
-  if (rc) return rc;
-  cell_scatter_kernel<<<grid, 256, 0, st>>>(jp, jq, bnd, off, cnt, perm);
+  if (nc <= kScatterScanMax) {
+    // the packing kernel zeroed the offsets region too: it is the cursor here
+    cell_scatter_scan_kernel<<<grid, 256, 0, st>>>(jp, jq, bnd, cnt, (int)nc, off, perm);
+    note_launches(1);
+  } else {
+    int rc = launch_exclusive_scan(cnt, (int)nc, off, st);
+    if (rc) return rc;
+    cell_scatter_kernel<<<grid, 256, 0, st>>>(jp, jq, bnd, off, cnt, perm);
+  }
   tile_info_kernel<<<dim3(ntile, B), kTilePoints, 0, st>>>(rec, perm, nullptr, P, ntile, pairs, tinfo);
   note_launches(3);  // + 1 scan, counted by launch_exclusive_scan
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
