@@ -84,6 +84,10 @@ struct SearchParams {
   int wait_spins;
   // optional (uniform calls): entries per point row, counted as written
   int* adj_count;
+  // optional (uniform calls): per batch element [Q], sorted query position
+  // -> a position in the sorted point order near the query (the middle of
+  // its cell's points), where the seed window of the threshold is taken
+  const int* qseed;
 };
 
 // Search CTA: WPC warps (1, 2 or 4), each owning QPW queries (32, 16 or 8;
@@ -152,6 +156,7 @@ struct FwdLayout {
   // spatial index (FP32 search path): bound parts [B*kBoundParts*8], cell counts / offsets
   // [B*cells(+1)], point and query permutations, tile boxes [B*ntile*8]
   size_t bounds, cell_count, cell_offset, perm_p, perm_q, tinfo;
+  size_t qseed;  // [B*Q] ints: seed positions of the sorted queries
   int P_pad, bits;
 };
 int spatial_bits(int P);

@@ -456,6 +456,7 @@ struct SearchItem {
   int64_t* idxs;
   int64_t row0;        // global query row of group-local query 0
   int* adj_count;      // the group's per-point entry counts (optional)
+  const int* qseed;    // seed positions of the group's sorted queries (optional)
   int Q, P, K, ntile, qblock;
 };
 
@@ -538,6 +539,63 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   if (owner) {
     qorig[lq] = valid ? qi : -1;
     qtab[lq] = make_float4(qx, qy, qz, valid ? INFINITY : -INFINITY);
+  }
+
+  // ---- seed thresholds.  Any K+1 distinct points bound the query's
+  // (K+1)-th smallest key from above by their own (K+1)-th smallest key, so
+  // keys above that can be dropped from the start instead of streaming
+  // through the list.  The points are a window of NS points of the sorted
+  // order around the middle of the query's cell (near the query, so the
+  // bound is tight); the half-warp (the warp for NS = 64) of a query
+  // evaluates two points per lane and sorts the NS keys (bitonic, NaN as
+  // +inf), and the lane holding element K writes the bound into the query
+  // table.
+  if (it.qseed) {
+    constexpr int NS = KMAX <= 16 ? 32 : 64;  // >= K + 1
+    constexpr int LG = NS / 2;                // lanes per query
+    constexpr int GPR = 32 / LG;              // queries per round
+    const int my_seed = valid ? it.qseed[sp] : 0;
+    __syncwarp();
+    if (P >= NS) {
+      const int gl = lane % LG;  // lane within the query's group
+      const float2* pairs2 = reinterpret_cast<const float2*>(it.pairs);
+#pragma unroll 1
+      for (int r = 0; r < QPW / GPR; ++r) {
+        const int jj = r * GPR + lane / LG;  // warp-local query of this group
+        const int center = __shfl_sync(FULL, my_seed, jj);
+        const bool qok = __shfl_sync(FULL, valid, jj);
+        int a0 = center - NS / 2;
+        a0 = (a0 < 0 ? 0 : (a0 > P - NS ? P - NS : a0)) & ~1;
+        const int pos = a0 + 2 * gl;  // even, pos + 1 < P
+        const float2* tp = pairs2 + (int64_t)(pos >> 7) * (PPT * kRecLen) + ((pos & (kTilePoints - 1)) >> 1);
+        float2 pr[kRecLen];
+#pragma unroll
+        for (int f = 0; f < kRecLen; ++f) pr[f] = __ldg(tp + f * PPT);
+        const float4 qq = qtab[warp * QPW + jj];
+        const float2 s2 = key_pair(make_float2(qq.x, qq.x), make_float2(qq.y, qq.y), make_float2(qq.z, qq.z), pr);
+        float v0 = s2.x == s2.x ? s2.x : INFINITY, v1 = s2.y == s2.y ? s2.y : INFINITY;
+        // element e = 2 * gl + h; ascending bitonic network over NS elements
+#pragma unroll
+        for (int kk = 2; kk <= NS; kk <<= 1) {
+          const bool up = ((2 * gl) & kk) == 0;
+#pragma unroll
+          for (int j = kk >> 1; j > 0; j >>= 1) {
+            if (j == 1) {
+              const float lo = fminf(v0, v1), hi = fmaxf(v0, v1);
+              v0 = up ? lo : hi;
+              v1 = up ? hi : lo;
+            } else {
+              const float o0 = __shfl_xor_sync(FULL, v0, j >> 1), o1 = __shfl_xor_sync(FULL, v1, j >> 1);
+              const bool take_min = (((2 * gl) & j) == 0) == up;
+              v0 = take_min ? fminf(v0, o0) : fmaxf(v0, o0);
+              v1 = take_min ? fminf(v1, o1) : fmaxf(v1, o1);
+            }
+          }
+        }
+        if (qok && gl == (K >> 1)) qtab[warp * QPW + jj].w = (K & 1) ? v1 : v0;
+      }
+    }
+    __syncwarp();
   }
 
   // MinK's fill phase stores points 0..K-1 whatever their key: a NaN there
@@ -648,7 +706,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     keys[s] = (s < KMAX - K) ? -INFINITY : INFINITY;
     vals[s] = -1;
   }
-  float tau = valid ? INFINITY : -INFINITY, tie_key = INFINITY;
+  float tau = owner ? qtab[lq].w : -INFINITY, tie_key = INFINITY;  // the seed, +inf or -inf (no query)
   int my_cnt = 0;  // queued candidates of this lane's query
   const float qpt[3] = {qx, qy, qz};
 
@@ -969,6 +1027,7 @@ __global__ void __launch_bounds__(32 * WPC) search_f32_kernel(SearchParams a) {
   it.idxs = a.idxs + b * a.Q * a.K;
   it.row0 = b * a.Q;
   it.adj_count = a.adj_count ? a.adj_count + b * a.P : nullptr;
+  it.qseed = a.qseed ? a.qseed + b * a.Q : nullptr;
   it.Q = a.Q;
   it.P = a.P;
   it.K = a.K;
@@ -1033,6 +1092,7 @@ __global__ void __launch_bounds__(32 * WPC) search_ragged_kernel(SearchParams a)
       it.idxs = a.idxs + g.e_off;
       it.row0 = g.q_off;
       it.adj_count = nullptr;
+      it.qseed = nullptr;
       it.Q = g.Q;
       it.P = c.P;
       it.K = g.K;
@@ -1207,7 +1267,7 @@ FwdLayout fwd_layout(int B, int Q, int P, int K, int dtype, bool own_rec) {
   L.rec = off;
   if (own_rec) off += align256((size_t)B * P * kRecLen * esz);
   L.P_pad = (int)round_up(P, kTilePoints);
-  L.pairs = L.bounds = L.cell_count = L.cell_offset = L.perm_p = L.perm_q = L.tinfo = off;
+  L.pairs = L.bounds = L.cell_count = L.cell_offset = L.perm_p = L.perm_q = L.tinfo = L.qseed = off;
   L.bits = 0;
   if (dtype == KNNAG_F32 && K <= 32) {
     L.bits = spatial_bits(P);
@@ -1226,6 +1286,8 @@ FwdLayout fwd_layout(int B, int Q, int P, int K, int dtype, bool own_rec) {
     off += align256((size_t)B * P * 4 + (size_t)B * Q * 4);
     L.tinfo = off;
     off += align256((size_t)B * (L.P_pad / kTilePoints) * 8 * 4);
+    L.qseed = off;
+    off += align256((size_t)B * Q * 4);
   }
   L.total = off;
   return L;
@@ -1331,6 +1393,7 @@ int forward_impl(const void* q, const void* p, const void* f, const void* sigma,
   sp.flag_count = flag_count;
   sp.flag_list = flag_list;
   sp.adj_count = adj_count;
+  sp.qseed = reinterpret_cast<const int*>(ws + L.qseed);
   apply_search_debug(sp);
   const int G = choose_splits(B, Q, dev);
   {

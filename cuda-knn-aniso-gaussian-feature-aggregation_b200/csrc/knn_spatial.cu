@@ -163,7 +163,21 @@ struct CellJob {
   GroupMap m;
   int cell_base;
   int nparts;  // > 0: bnd holds nparts partial boxes per group, reduced here
+  // queries of a uniform batch sorted together with its points (whose cells
+  // come first in the scan): seed[position - seed_sub] = the middle of the
+  // element's cell in its group's sorted points
+  int* seed;
+  int64_t seed_sub;
 };
+
+// Seed position of an element in cell c (global index in the scanned
+// arrays) of the query job j: the middle of the same cell's points, as a
+// position in the group's sorted points.  The points' cells of group r sit
+// at r.cell_off + (c - j.cell_base); off[] is the exclusive scan.
+__device__ __forceinline__ int seed_of(const CellJob& j, const GroupRange& r, const int* off, int c) {
+  const int pc = c - j.cell_base;
+  return ((off[pc] + off[pc + 1]) >> 1) - off[r.cell_off];
+}
 
 // The box of group r: bnd's entry, or the reduction of its nparts partial
 // boxes (into shared memory, by the first threads of the CTA; all threads
@@ -212,7 +226,9 @@ __global__ void cell_scatter_kernel(CellJob j0, CellJob j1, const float* __restr
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n; i += gridDim.x * blockDim.x) {
     const float* v = j.xyz + (r.start + i) * j.stride;
     const int c = base + (int)cell_of(s * v[0], s * v[1], s * v[2], gb, r.bits);
-    perm[offset[c] + atomicAdd(&cursor[c], 1)] = i;
+    const int pos = offset[c] + atomicAdd(&cursor[c], 1);
+    perm[pos] = i;
+    if (j.seed) j.seed[pos - j.seed_sub] = seed_of(j, r, offset, c);
   }
 }
 
@@ -267,7 +283,9 @@ __global__ void __launch_bounds__(256) cell_scatter_scan_kernel(CellJob j0, Cell
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < r.n; i += gridDim.x * blockDim.x) {
     const float* v = j.xyz + (r.start + i) * j.stride;
     const int c = base + (int)cell_of(s * v[0], s * v[1], s * v[2], gb, r.bits);
-    perm[soff[c] + atomicAdd(&cursor[c], 1)] = i;
+    const int pos = soff[c] + atomicAdd(&cursor[c], 1);
+    perm[pos] = i;
+    if (j.seed) j.seed[pos - j.seed_sub] = seed_of(j, r, soff, c);
   }
 }
 
@@ -439,7 +457,7 @@ int launch_spatial_index(const float* q, const float* rec, int B, int Q, int P, 
   // positions start after all points' and land in perm_q, which follows perm_p
   const int64_t nc = 2 * (int64_t)B * cells;
   const CellJob jp{rec + kNPX, kRecLen, 1, pm, 0, kBoundParts};
-  const CellJob jq{q, 3, 0, qm, B * cells, kBoundParts};
+  const CellJob jq{q, 3, 0, qm, B * cells, kBoundParts, reinterpret_cast<int*>(ws + L.qseed), (int64_t)B * P};
   const dim3 grid(grid_x(P > Q ? P : Q, sms, B), B, 2);
   cell_count_kernel<<<grid, 256, 0, st>>>(jp, jq, bnd, cnt);
   if (nc <= kScatterScanMax) {
