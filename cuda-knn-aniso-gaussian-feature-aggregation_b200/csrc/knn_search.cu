@@ -518,6 +518,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   float* lbk = reinterpret_cast<float*>(smem + search_smem_bytes(WPC, QPW));
   int* lbt = reinterpret_cast<int*>(lbk + ntp_cap);
   volatile int* s_nvisit = reinterpret_cast<volatile int*>(lbt + ntp_cap);
+  volatile int* s_ncand = s_nvisit + 1;  // tiles in the visit order (the rest are never needed)
   // epilogue views of the queue region (after the tile loop)
   float* out_k = reinterpret_cast<float*>(smem + search_queue_off());
   int* out_i = reinterpret_cast<int*>(out_k + NT * L);
@@ -639,62 +640,108 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     }
   }
   const float* tinfo_b = it.tinfo;
+  // Seeded queries bound the tiles worth visiting: a tile whose bound
+  // against the CTA's box exceeds every query's seed holds no point below
+  // any threshold the search will ever use.  Only the tiles at or below the
+  // largest seed are sorted (all of them without seeds).
+  float tmax0 = INFINITY;
+  if (it.qseed) {
+    tmax0 = -INFINITY;
+    for (int i = lane; i < NT; i += 32) tmax0 = fmaxf(tmax0, qtab[i].w);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tmax0 = fmaxf(tmax0, __shfl_xor_sync(FULL, tmax0, o));
+  }
+  // (bound, tile) ascending, ties by tile, in registers across warp 0's
+  // lanes (shuffle bitonic network); invalid entries carry +inf.
+  auto warp_sort_tiles = [&](float& lb, int& ti) {
+#pragma unroll
+    for (int kk = 2; kk <= 32; kk <<= 1) {
+#pragma unroll
+      for (int j = kk >> 1; j > 0; j >>= 1) {
+        const float ok = __shfl_xor_sync(FULL, lb, j);
+        const int oi = __shfl_xor_sync(FULL, ti, j);
+        const bool up = (lane & kk) == 0;
+        const bool lower = (lane & j) == 0;
+        const bool other_less = ok < lb || (ok == lb && oi < ti);
+        if (lower == up ? other_less : !other_less) {
+          lb = ok;
+          ti = oi;
+        }
+      }
+    }
+  };
   if (NTP <= 32) {
-    // Up to 32 tiles: warp 0 computes the bounds and sorts (bound, tile)
-    // ascending in registers with a shuffle bitonic network (ties by tile).
+    // Up to 32 tiles: warp 0 computes the bounds and sorts them in registers.
     if (warp == 0) {
       float lb = INFINITY;
       int ti = lane;
-      if (lane < it.ntile) lb = fminf(tile_lower_bound(tinfo_b + lane * 8, bmin, bmax), 3.4e38f);
-#pragma unroll
-      for (int kk = 2; kk <= 32; kk <<= 1) {
-#pragma unroll
-        for (int j = kk >> 1; j > 0; j >>= 1) {
-          const float ok = __shfl_xor_sync(FULL, lb, j);
-          const int oi = __shfl_xor_sync(FULL, ti, j);
-          const bool up = (lane & kk) == 0;
-          const bool lower = (lane & j) == 0;
-          const bool other_less = ok < lb || (ok == lb && oi < ti);
-          if (lower == up ? other_less : !other_less) {
-            lb = ok;
-            ti = oi;
-          }
-        }
+      bool keep = false;
+      if (lane < it.ntile) {
+        lb = tile_lower_bound(tinfo_b + lane * 8, bmin, bmax);
+        keep = !(lb > tmax0);
+        lb = keep ? fminf(lb, 3.4e38f) : INFINITY;  // kept tiles sort before the rest
       }
+      const int nkeep = __popc(__ballot_sync(FULL, keep));
+      warp_sort_tiles(lb, ti);
       if (lane < NTP) {
         lbk[lane] = lb;
         lbt[lane] = ti;
       }
+      if (lane == 0) *s_ncand = nkeep;
     }
     __syncthreads();
   } else {
-    for (int t = tid; t < NTP; t += NTH) {
-      float lb = INFINITY;
-      if (t < it.ntile) {
-        lb = tile_lower_bound(tinfo_b + t * 8, bmin, bmax);
-        lb = fminf(lb, 3.4e38f);  // real tiles sort before the +inf padding entries
+    // Compact the kept tiles (in any order), then sort them: in warp 0's
+    // registers when at most 32, else in shared memory over the next power
+    // of two (padding +inf).
+    if (tid == 0) *s_ncand = 0;
+    __syncthreads();
+    for (int t = tid; t < it.ntile; t += NTH) {
+      const float lb = tile_lower_bound(tinfo_b + t * 8, bmin, bmax);
+      if (!(lb > tmax0)) {
+        const int pos = atomicAdd(const_cast<int*>(s_ncand), 1);
+        lbk[pos] = fminf(lb, 3.4e38f);
+        lbt[pos] = t;
       }
-      lbk[t] = lb;
-      lbt[t] = t;
     }
     __syncthreads();
-    for (int kk = 2; kk <= NTP; kk <<= 1) {  // bitonic sort of (bound, tile) ascending
-      for (int j = kk >> 1; j > 0; j >>= 1) {
-        for (int i = tid; i < NTP; i += NTH) {
-          const int ixj = i ^ j;
-          if (ixj > i) {
-            const bool up = (i & kk) == 0;
-            const float ki = lbk[i], kj = lbk[ixj];
-            if ((ki > kj) == up) {
-              lbk[i] = kj;
-              lbk[ixj] = ki;
-              const int ti = lbt[i];
-              lbt[i] = lbt[ixj];
-              lbt[ixj] = ti;
+    const int nkeep = *s_ncand;
+    if (nkeep <= 32) {
+      if (warp == 0) {
+        float lb = lane < nkeep ? lbk[lane] : INFINITY;
+        int ti = lane < nkeep ? lbt[lane] : 0x7fffffff;
+        warp_sort_tiles(lb, ti);
+        if (lane < nkeep) {
+          lbk[lane] = lb;
+          lbt[lane] = ti;
+        }
+      }
+      __syncthreads();
+    } else {
+      const int ns = search_tiles_pow2(nkeep);  // <= NTP
+      for (int t = nkeep + tid; t < ns; t += NTH) {
+        lbk[t] = INFINITY;
+        lbt[t] = 0x7fffffff;
+      }
+      __syncthreads();
+      for (int kk = 2; kk <= ns; kk <<= 1) {  // bitonic sort of (bound, tile) ascending
+        for (int j = kk >> 1; j > 0; j >>= 1) {
+          for (int i = tid; i < ns; i += NTH) {
+            const int ixj = i ^ j;
+            if (ixj > i) {
+              const bool up = (i & kk) == 0;
+              const float ki = lbk[i], kj = lbk[ixj];
+              const int ti = lbt[i], tj = lbt[ixj];
+              if ((ki > kj || (ki == kj && ti > tj)) == up) {
+                lbk[i] = kj;
+                lbk[ixj] = ki;
+                lbt[i] = tj;
+                lbt[ixj] = ti;
+              }
             }
           }
+          __syncthreads();
         }
-        __syncthreads();
       }
     }
   }
@@ -724,7 +771,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   // ascending, so nothing after it is needed either).  Decisions are made
   // one visit at a time, in order (see below), so *s_nvisit == v here.
   auto decide = [&](int v, float tmax) {
-    if (v >= ntile || *s_nvisit != v) return false;
+    if (v >= *s_ncand || *s_nvisit != v) return false;
     if ((unsigned)lbt[v] >= (unsigned)ntile) {  // real tiles sort first: never taken
       atomicOr(a.status, kStatusBadIndex);
       return false;
