@@ -211,4 +211,63 @@ __device__ __forceinline__ void bulk_copy_g2s(void* smem_dst, const void* gmem_s
       : "memory");
 }
 
+// ------------------------------------------------ Hilbert grid cells
+
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+// Position of grid cell (x, y, z) (bits bits per axis) along the 3-D Hilbert
+// curve, by J. Skilling's transpose algorithm ("Programming the Hilbert
+// curve", AIP Conf. Proc. 707, 2004): undo the excess work, Gray-encode,
+// then interleave the transposed coordinates (X[0] most significant).
+// Consecutive cells along the curve are always face neighbours, so a run of
+// sorted points (a search tile) or queries (a CTA) stays compact; the
+// Z-order curve jumps across the box at every level.
+__device__ __forceinline__ uint32_t hilbert3(uint32_t x, uint32_t y, uint32_t z, int bits) {
+  uint32_t X[3] = {x, y, z};
+  const uint32_t M = 1u << (bits - 1);
+  for (uint32_t Q = M; Q > 1; Q >>= 1) {
+    const uint32_t P = Q - 1;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      if (X[i] & Q) {
+        X[0] ^= P;
+      } else {
+        const uint32_t t = (X[0] ^ X[i]) & P;
+        X[0] ^= t;
+        X[i] ^= t;
+      }
+    }
+  }
+  X[1] ^= X[0];
+  X[2] ^= X[1];
+  uint32_t t = 0;
+  for (uint32_t Q = M; Q > 1; Q >>= 1)
+    if (X[2] & Q) t ^= Q - 1;
+  X[0] ^= t;
+  X[1] ^= t;
+  X[2] ^= t;
+  return (spread3(X[0]) << 2) | (spread3(X[1]) << 1) | spread3(X[2]);
+}
+
+__device__ __forceinline__ uint32_t cell_of(float x, float y, float z, const float* bnd, int bits) {
+  const float res = (float)(1 << bits);
+  uint32_t c[3];
+  const float v[3] = {x, y, z};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float lo = bnd[a], ext = bnd[3 + a] - bnd[a];
+    float t = ext > 0.f ? (v[a] - lo) / ext * res : 0.f;
+    t = fminf(fmaxf(t, 0.f), res - 1.f);  // NaN -> 0
+    c[a] = (uint32_t)t;
+  }
+  return hilbert3(c[0], c[1], c[2], bits);
+}
+
 }  // namespace knnag

@@ -164,7 +164,7 @@ int launch_spatial_index(const float* q, const float* rec, int B, int Q, int P, 
                          cudaStream_t st);
 int launch_exclusive_scan(int* count, int n, int* out, cudaStream_t st);
 int launch_cloudset_index(char* cs, const CloudSetHeader& h, const CloudDesc* cd_dev, int max_p, int max_ntile,
-                          int* cnt, int* off, int* perm_p, cudaStream_t st);
+                          int* cnt, int* perm_p, cudaStream_t st);
 int launch_query_order(const float* q, const char* cs, const void* segs_dev, int cap_segs, int64_t cap_q,
                        int cap_cells, int* cnt, int* off, int* perm_q, const int* status, cudaStream_t st);
 

@@ -50,20 +50,21 @@ size_t cloudset_layout(int C, const int* P, CloudSetHeader* h, CloudDesc* descs)
   x.pairs_off = x.rec_off + (int64_t)align256((size_t)total_p * kRecLen * 4);
   x.tinfo_off = x.pairs_off + (int64_t)align256((size_t)total_tiles * kTilePoints * kRecLen * 4);
   x.bnd_off = x.tinfo_off + (int64_t)align256((size_t)total_tiles * 8 * 4);
-  x.total_bytes = x.bnd_off + (int64_t)align256((size_t)C * 8 * 4);
+  x.celloff_off = x.bnd_off + (int64_t)align256((size_t)C * 8 * 4);
+  x.total_bytes = x.celloff_off + (int64_t)align256(((size_t)total_cells + 1) * 4);
   if (h) *h = x;
   return (size_t)x.total_bytes;
 }
 
-// Cloud-set build scratch: cell counts, offsets, point permutation.
+// Cloud-set build scratch: cell counts, point permutation (the cell offsets
+// live in the cloud set).
 struct BuildScratch {
-  size_t cnt, off, perm, total;
+  size_t cnt, perm, total;
 };
 BuildScratch build_scratch(const CloudSetHeader& h) {
   BuildScratch b{};
   b.cnt = 0;
-  b.off = align256((size_t)h.total_cells * 4);
-  b.perm = b.off + align256(((size_t)h.total_cells + 1) * 4);
+  b.perm = align256((size_t)h.total_cells * 4);
   b.total = b.perm + align256((size_t)h.total_p * 4);
   return b;
 }
@@ -181,8 +182,7 @@ int knnag_cloudset_build(const float* p, const float* sigma, const float* R, int
   int rc = launch_pack_points(p, sigma, R, 1, (int)h.total_p, KNNAG_F32, cs + h.rec_off, st);
   if (rc) return rc;
   return launch_cloudset_index(cs, h, reinterpret_cast<const CloudDesc*>(cs + h.desc_off), max_p, h.max_ntile,
-                               reinterpret_cast<int*>(ws + b.cnt), reinterpret_cast<int*>(ws + b.off),
-                               reinterpret_cast<int*>(ws + b.perm), st);
+                               reinterpret_cast<int*>(ws + b.cnt), reinterpret_cast<int*>(ws + b.perm), st);
 }
 
 size_t knnag_segments_bytes(int nseg) {

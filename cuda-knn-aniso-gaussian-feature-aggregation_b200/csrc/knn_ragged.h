@@ -34,6 +34,10 @@ struct CloudSetHeader {
   int C, max_ntile, total_cells;
   int64_t total_p, total_tiles;
   int64_t desc_off, rec_off, pairs_off, tinfo_off, bnd_off, total_bytes;
+  // exclusive scan of the point counts of every cloud's grid cells
+  // [total_cells + 1] (global point positions): where a query's cell starts
+  // in its cloud's sorted points, for the search's seed windows
+  int64_t celloff_off;
 };
 
 struct SegDesc {

@@ -457,6 +457,11 @@ struct SearchItem {
   int64_t row0;        // global query row of group-local query 0
   int* adj_count;      // the group's per-point entry counts (optional)
   const int* qseed;    // seed positions of the group's sorted queries (optional)
+  // or seeds from the query's cell: the scanned point counts of the
+  // cloud's grid cells (global positions, cell 0 first), its box and grid
+  const int* cell_start;
+  const float* cbox;
+  int cbits;
   int Q, P, K, ntile, qblock;
 };
 
@@ -551,11 +556,20 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   // evaluates two points per lane and sorts the NS keys (bitonic, NaN as
   // +inf), and the lane holding element K writes the bound into the query
   // table.
-  if (it.qseed) {
+  const bool seeded = it.qseed || it.cell_start;
+  if (seeded) {
     constexpr int NS = KMAX <= 16 ? 32 : 64;  // >= K + 1
     constexpr int LG = NS / 2;                // lanes per query
     constexpr int GPR = 32 / LG;              // queries per round
-    const int my_seed = valid ? it.qseed[sp] : 0;
+    int my_seed = 0;  // the middle of the query's cell in the sorted points
+    if (valid) {
+      if (it.qseed) {
+        my_seed = it.qseed[sp];
+      } else {
+        const int c = (int)cell_of(qx, qy, qz, it.cbox, it.cbits);
+        my_seed = ((it.cell_start[c] + it.cell_start[c + 1]) >> 1) - it.cell_start[0];
+      }
+    }
     __syncwarp();
     if (P >= NS) {
       const int gl = lane % LG;  // lane within the query's group
@@ -645,7 +659,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   // any threshold the search will ever use.  Only the tiles at or below the
   // largest seed are sorted (all of them without seeds).
   float tmax0 = INFINITY;
-  if (it.qseed) {
+  if (seeded) {
     tmax0 = -INFINITY;
     for (int i = lane; i < NT; i += 32) tmax0 = fmaxf(tmax0, qtab[i].w);
 #pragma unroll
@@ -1075,6 +1089,9 @@ __global__ void __launch_bounds__(32 * WPC) search_f32_kernel(SearchParams a) {
   it.row0 = b * a.Q;
   it.adj_count = a.adj_count ? a.adj_count + b * a.P : nullptr;
   it.qseed = a.qseed ? a.qseed + b * a.Q : nullptr;
+  it.cell_start = nullptr;
+  it.cbox = nullptr;
+  it.cbits = 0;
   it.Q = a.Q;
   it.P = a.P;
   it.K = a.K;
@@ -1108,6 +1125,8 @@ __global__ void __launch_bounds__(32 * WPC) search_ragged_kernel(SearchParams a)
   const float* crec = reinterpret_cast<const float*>(a.cs + ch->rec_off);
   const float* cpairs = reinterpret_cast<const float*>(a.cs + ch->pairs_off);
   const float* ctinfo = reinterpret_cast<const float*>(a.cs + ch->tinfo_off);
+  const float* cbnd = reinterpret_cast<const float*>(a.cs + ch->bnd_off);
+  const int* ccell = reinterpret_cast<const int*>(a.cs + ch->celloff_off);
   const int nseg = sh->nseg, n_items = sh->n_items;
   const int ntp_cap = search_tiles_pow2(a.ntile);
   constexpr int QPC = WPC * QPW;
@@ -1140,6 +1159,9 @@ __global__ void __launch_bounds__(32 * WPC) search_ragged_kernel(SearchParams a)
       it.row0 = g.q_off;
       it.adj_count = nullptr;
       it.qseed = nullptr;
+      it.cell_start = ccell + c.cell_off;
+      it.cbox = cbnd + (int64_t)g.cloud * 8;
+      it.cbits = c.bits;
       it.Q = g.Q;
       it.P = c.P;
       it.K = g.K;
