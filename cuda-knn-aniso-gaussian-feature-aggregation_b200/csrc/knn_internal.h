@@ -122,6 +122,8 @@ inline bool search_shape_ok(int shape) {
 //   queues    wpc x [qpw queries][kQCap] keys, then indices (after the tile
 //             loop: the CTA's sorted lists, weights and flags)
 //   qtab      [wpc qpw] float4 (x, y, z, threshold) of the CTA's queries
+//   ctab      per warp, the queries a tile matters to, compacted: [qpw]
+//             float4 (x, y, z, threshold) of the warp, then [qpw] their lanes
 //   misc      [wpc qpw] original query index, [wpc][6] warp query boxes,
 //             64 bytes of mbarriers / counters / flags
 //   region C  tile bounds and visit order [NTP x 8 B] + visit counter
@@ -130,8 +132,11 @@ __host__ __device__ inline constexpr size_t search_warp_queue_bytes(int qpw) { r
 __host__ __device__ inline constexpr size_t search_qtab_off(int wpc, int qpw) {
   return search_queue_off() + (size_t)wpc * search_warp_queue_bytes(qpw);
 }
-__host__ __device__ inline constexpr size_t search_misc_off(int wpc, int qpw) {
+__host__ __device__ inline constexpr size_t search_ctab_off(int wpc, int qpw) {
   return search_qtab_off(wpc, qpw) + (size_t)wpc * qpw * 16;
+}
+__host__ __device__ inline constexpr size_t search_misc_off(int wpc, int qpw) {
+  return search_ctab_off(wpc, qpw) + (size_t)wpc * qpw * 20;
 }
 __host__ __device__ inline constexpr size_t search_bars_off(int wpc, int qpw) {
   return search_misc_off(wpc, qpw) + (size_t)wpc * qpw * 4 + (size_t)wpc * 6 * 4;

@@ -462,7 +462,8 @@ struct SearchItem {
   const int* cell_start;
   const float* cbox;
   int cbits;
-  int Q, P, K, ntile, qblock;
+  int Q, P, K, ntile;
+  int q0, q1;          // the item's queries: sorted positions [q0, q1), at most WPC * QPW
 };
 
 // Lower bound on the key of any query in box [bmin, bmax] against any point
@@ -512,6 +513,8 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   float* qk = reinterpret_cast<float*>(smem + search_queue_off() + (size_t)warp * search_warp_queue_bytes(QPW));
   int* qv = reinterpret_cast<int*>(qk + QPW * kQCap);
   float4* qtab = reinterpret_cast<float4*>(smem + search_qtab_off(WPC, QPW));  // [NT]
+  float4* ctab = reinterpret_cast<float4*>(smem + search_ctab_off(WPC, QPW)) + warp * QPW;  // this warp's
+  int* cidx = reinterpret_cast<int*>(smem + search_ctab_off(WPC, QPW) + (size_t)NT * 16) + warp * QPW;
   int* qorig = reinterpret_cast<int*>(smem + search_misc_off(WPC, QPW));       // [NT] original query index (-1: none)
   float* qbox = reinterpret_cast<float*>(qorig + NT);                          // [WPC][6]
   uint64_t* full = search_barriers<WPC, QPW>(smem);
@@ -531,8 +534,8 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   int* out_f = reinterpret_cast<int*>(out_w + NT * L);
 
   const int lq = warp * QPW + lane;         // query of this (owner) lane within the item
-  const int sp = it.qblock * NT + lq;       // position in the spatial order
-  bool valid = owner && sp < it.Q;
+  const int sp = it.q0 + lq;                // position in the spatial order
+  bool valid = owner && sp < it.q1;
   int qi = it.perm_q[valid ? sp : it.Q - 1];
   if ((unsigned)qi >= (unsigned)it.Q) {  // the query order is a permutation: never taken
     if (valid) atomicOr(a.status, kStatusBadIndex);
@@ -844,9 +847,22 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     const float lbq = tile_lower_bound(tinfo_b + (int64_t)lbt[t] * 8, qpt, qpt);
     const unsigned need = __ballot_sync(FULL, valid && !(lbq > tau));
     if (need) {
+      // The queries the tile matters to, compacted in lane order: round r
+      // slot h takes entry r * H + h.  Owner lanes publish their entry and
+      // remember its rank (refreshed thresholds go there too).
+      const int n_need = __popc(need);
+      const int R = (n_need + H - 1) / H;  // rounds per pass
       const int slot = lane / QPW;
       const unsigned my_mask = SLOT_MASK << (slot * QPW);
       const unsigned lt_mask = (1u << lane) - 1u;
+      const int my_rank = (owner && ((need >> lane) & 1u)) ? __popc(need & lt_mask) : -1;
+      const int my_round = my_rank >= 0 ? my_rank / H : -1;
+      const unsigned my_slot_mask = SLOT_MASK << ((my_rank >= 0 ? my_rank % H : 0) * QPW);
+      if (my_rank >= 0) {
+        ctab[my_rank] = make_float4(qx, qy, qz, tau);
+        cidx[my_rank] = lane;
+      }
+      __syncwarp();
 #pragma unroll 1
       for (int pass = 0; pass < NPASS; ++pass) {
         float2 pr[kRecLen];
@@ -854,35 +870,25 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
 #pragma unroll
         for (int f = 0; f < kRecLen; ++f) pr[f] = tile[f * PPT + pidx];
         const int i0 = __float_as_int(pr[kRecPad].x), i1 = __float_as_int(pr[kRecPad].y);
-        unsigned rem = need;
-        while (rem) {
-          // two rounds per iteration (independent key evaluations in
-          // flight): in round u slot h takes the (u * H + h)-th lowest
-          // query still to do (-1: none)
-          int jh[2 * H];
-#pragma unroll
-          for (int h = 0; h < 2 * H; ++h) {
-            jh[h] = rem ? __ffs(rem) - 1 : -1;
-            rem &= rem - 1;
-          }
+#pragma unroll 1
+        for (int r0 = 0; r0 < R; r0 += 2) {
+          // two rounds per iteration (independent key evaluations in flight)
           int jr[2];
           float4 qr[2];
-          float2 sr[2];
 #pragma unroll
           for (int u = 0; u < 2; ++u) {
-            int j = jh[u * H];
-#pragma unroll
-            for (int h = 1; h < H; ++h) j = (slot == h) ? jh[u * H + h] : j;
-            jr[u] = j;
-            qr[u] = qtab[warp * QPW + (j >= 0 ? j : 0)];
+            const int e = (r0 + u) * H + slot;
+            jr[u] = e < n_need ? cidx[e] : -1;
+            qr[u] = ctab[e < n_need ? e : 0];
           }
+          float2 sr[2];
 #pragma unroll
           for (int u = 0; u < 2; ++u)
             sr[u] = key_pair(make_float2(qr[u].x, qr[u].x), make_float2(qr[u].y, qr[u].y),
                              make_float2(qr[u].z, qr[u].z), pr);
 #pragma unroll
           for (int u = 0; u < 2; ++u) {
-            if (u == 1 && jh[H] < 0) break;  // warp-uniform: no query left for round 1
+            if (u == 1 && r0 + 1 >= R) break;  // warp-uniform: no round 1
             const int j = jr[u];
             const float2 s2 = sr[u];
             const bool c0 = j >= 0 && s2.x <= qr[u].w, c1 = j >= 0 && s2.y <= qr[u].w;
@@ -895,6 +901,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
                 drain_queue<L>(keys, vals, tie_key, tau, my_cnt, qk, qv, lane);
                 my_cnt = 0;
                 if (owner) qtab[lq].w = tau;
+                if (my_rank >= 0) ctab[my_rank].w = tau;
                 __syncwarp();
                 c = 0;
               }
@@ -908,11 +915,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
                 qk[e] = s2.y;
                 qv[e] = i1;
               }
-#pragma unroll
-              for (int h = 0; h < H; ++h) {
-                const unsigned m = SLOT_MASK << (h * QPW);
-                if (lane == jh[u * H + h]) my_cnt += __popc(b0 & m) + __popc(b1 & m);
-              }
+              if (my_round == r0 + u) my_cnt += __popc(b0 & my_slot_mask) + __popc(b1 & my_slot_mask);
             }
           }
         }
@@ -921,6 +924,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
           drain_queue<L>(keys, vals, tie_key, tau, my_cnt, qk, qv, lane);
           my_cnt = 0;
           if (owner) qtab[lq].w = tau;
+          if (my_rank >= 0) ctab[my_rank].w = tau;
           __syncwarp();
         }
       }
@@ -1096,7 +1100,8 @@ __global__ void __launch_bounds__(32 * WPC) search_f32_kernel(SearchParams a) {
   it.P = a.P;
   it.K = a.K;
   it.ntile = a.ntile;
-  it.qblock = blockIdx.x;
+  it.q0 = blockIdx.x * (WPC * QPW);
+  it.q1 = min(it.q0 + WPC * QPW, a.Q);
   uint32_t uses[kTileBufs] = {};
   search_item<KMAX, WPC, QPW>(a, it, smem, search_tiles_pow2(a.ntile), uses);
 }
@@ -1166,7 +1171,8 @@ __global__ void __launch_bounds__(32 * WPC) search_ragged_kernel(SearchParams a)
       it.P = c.P;
       it.K = g.K;
       it.ntile = c.ntile;
-      it.qblock = item - g.item_off;
+      it.q0 = (item - g.item_off) * QPC;
+      it.q1 = min(it.q0 + QPC, g.Q);
       bool ok;
       if (KMAX > 8 && g.K <= 8)
         ok = search_item<8, WPC, QPW>(a, it, smem, ntp_cap, uses);
