@@ -37,6 +37,13 @@ enum RecField {
 // float2 f * 64 + m), so packed f32x2 arithmetic reads both points' field
 // with one load and a warp reads 32 pairs' field with one conflict-free load.
 constexpr int kTilePoints = 128;
+// Per search tile: {min xyz, max xyz, mu, 0} of the tile's box, then the same
+// for each of its 32-point sub-boxes (sorted points 32w .. 32w + 31); mu is
+// the key lower-bound factor of the points inside (-1: no bound, +inf with
+// the empty box: no points).
+constexpr int kSubBoxes = kTilePoints / 32;
+constexpr int kTinfoFloats = 8 * (1 + kSubBoxes);
+constexpr unsigned kTinfoBytes = kTinfoFloats * 4;
 constexpr int kPairFloats = 32;
 
 __host__ __device__ inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }

@@ -56,7 +56,7 @@ struct ExactParams {
 struct SearchParams {
   const float* q;
   const int* perm_q;   // sorted position -> query index, per batch element
-  const float* tinfo;  // per tile: box (6), key lower-bound factor mu, pad
+  const float* tinfo;  // per tile kTinfoFloats: its box and its sub-boxes (box, mu, pad)
   int ntile;           // tiles per batch element (ragged: the most of any cloud)
   const float* pairs;  // pair-interleaved tiles [B][P_pad/2][32]
   const float* rec;    // per-point records [B*P*16]
@@ -122,8 +122,9 @@ inline bool search_shape_ok(int shape) {
 //   queues    wpc x [qpw queries][kQCap] keys, then indices (after the tile
 //             loop: the CTA's sorted lists, weights and flags)
 //   qtab      [wpc qpw] float4 (x, y, z, threshold) of the CTA's queries
-//   ctab      per warp, the queries a tile matters to, compacted: [qpw]
+//   ctab      per warp, the queries a pass matters to, compacted: [qpw]
 //             float4 (x, y, z, threshold) of the warp, then [qpw] their lanes
+//   tring     kTileBufs tile infos (box and sub-boxes), copied with the tiles
 //   misc      [wpc qpw] original query index, [wpc][6] warp query boxes,
 //             64 bytes of mbarriers / counters / flags
 //   region C  tile bounds and visit order [NTP x 8 B] + visit counter
@@ -135,8 +136,11 @@ __host__ __device__ inline constexpr size_t search_qtab_off(int wpc, int qpw) {
 __host__ __device__ inline constexpr size_t search_ctab_off(int wpc, int qpw) {
   return search_qtab_off(wpc, qpw) + (size_t)wpc * qpw * 16;
 }
-__host__ __device__ inline constexpr size_t search_misc_off(int wpc, int qpw) {
+__host__ __device__ inline constexpr size_t search_tring_off(int wpc, int qpw) {
   return search_ctab_off(wpc, qpw) + (size_t)wpc * qpw * 20;
+}
+__host__ __device__ inline constexpr size_t search_misc_off(int wpc, int qpw) {
+  return search_tring_off(wpc, qpw) + (size_t)kTileBufs * kTinfoBytes;
 }
 __host__ __device__ inline constexpr size_t search_bars_off(int wpc, int qpw) {
   return search_misc_off(wpc, qpw) + (size_t)wpc * qpw * 4 + (size_t)wpc * 6 * 4;

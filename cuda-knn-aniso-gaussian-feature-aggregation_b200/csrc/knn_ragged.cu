@@ -49,7 +49,7 @@ size_t cloudset_layout(int C, const int* P, CloudSetHeader* h, CloudDesc* descs)
   x.rec_off = (int64_t)align256(256 + (size_t)C * sizeof(CloudDesc));
   x.pairs_off = x.rec_off + (int64_t)align256((size_t)total_p * kRecLen * 4);
   x.tinfo_off = x.pairs_off + (int64_t)align256((size_t)total_tiles * kTilePoints * kRecLen * 4);
-  x.bnd_off = x.tinfo_off + (int64_t)align256((size_t)total_tiles * 8 * 4);
+  x.bnd_off = x.tinfo_off + (int64_t)align256((size_t)total_tiles * kTinfoBytes);
   x.celloff_off = x.bnd_off + (int64_t)align256((size_t)C * 8 * 4);
   x.total_bytes = x.celloff_off + (int64_t)align256(((size_t)total_cells + 1) * 4);
   if (h) *h = x;

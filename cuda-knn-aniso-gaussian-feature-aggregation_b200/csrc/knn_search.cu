@@ -448,7 +448,7 @@ struct SearchItem {
   const int* perm_q;   // sorted position -> group-local query index
   const float* rec;    // the cloud's records
   const float* pairs;  // the cloud's search tiles
-  const float* tinfo;  // the cloud's tile boxes
+  const float* tinfo;  // the cloud's tile infos (kTinfoFloats per tile)
   const float* f;      // the cloud's feature rows
   float* f_out;        // rows of the group's queries
   float* w_out;        // entries of the group's queries (K per query)
@@ -515,6 +515,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   float4* qtab = reinterpret_cast<float4*>(smem + search_qtab_off(WPC, QPW));  // [NT]
   float4* ctab = reinterpret_cast<float4*>(smem + search_ctab_off(WPC, QPW)) + warp * QPW;  // this warp's
   int* cidx = reinterpret_cast<int*>(smem + search_ctab_off(WPC, QPW) + (size_t)NT * 16) + warp * QPW;
+  float* tring = reinterpret_cast<float*>(smem + search_tring_off(WPC, QPW));  // [kTileBufs][kTinfoFloats]
   int* qorig = reinterpret_cast<int*>(smem + search_misc_off(WPC, QPW));       // [NT] original query index (-1: none)
   float* qbox = reinterpret_cast<float*>(qorig + NT);                          // [WPC][6]
   uint64_t* full = search_barriers<WPC, QPW>(smem);
@@ -694,7 +695,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
       int ti = lane;
       bool keep = false;
       if (lane < it.ntile) {
-        lb = tile_lower_bound(tinfo_b + lane * 8, bmin, bmax);
+        lb = tile_lower_bound(tinfo_b + lane * kTinfoFloats, bmin, bmax);
         keep = !(lb > tmax0);
         lb = keep ? fminf(lb, 3.4e38f) : INFINITY;  // kept tiles sort before the rest
       }
@@ -714,7 +715,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     if (tid == 0) *s_ncand = 0;
     __syncthreads();
     for (int t = tid; t < it.ntile; t += NTH) {
-      const float lb = tile_lower_bound(tinfo_b + t * 8, bmin, bmax);
+      const float lb = tile_lower_bound(tinfo_b + (int64_t)t * kTinfoFloats, bmin, bmax);
       if (!(lb > tmax0)) {
         const int pos = atomicAdd(const_cast<int*>(s_ncand), 1);
         lbk[pos] = fminf(lb, 3.4e38f);
@@ -779,10 +780,11 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   // visit position v reads tile lbt[v] into buffer v % kTileBufs
   auto issue = [&](int v) {
     const int buf = v % kTileBufs;
-    mbar_arrive_expect_tx(&full[buf], (uint32_t)kSearchTileBytes);
+    mbar_arrive_expect_tx(&full[buf], (uint32_t)kSearchTileBytes + kTinfoBytes);
     if (v == a.stall_visit) return;  // test hook: this phase never completes
     bulk_copy_g2s(ring + buf * kSearchTileBytes, pairs_b + (int64_t)lbt[v] * PPT * kPairFloats,
                   (uint32_t)kSearchTileBytes, &full[buf]);
+    bulk_copy_g2s(tring + buf * kTinfoFloats, tinfo_b + (int64_t)lbt[v] * kTinfoFloats, kTinfoBytes, &full[buf]);
   };
   // Issue position v unless its bound exceeds every threshold (the order is
   // ascending, so nothing after it is needed either).  Decisions are made
@@ -844,82 +846,94 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     const float2* tile = reinterpret_cast<const float2*>(ring + buf * kSearchTileBytes);
     // queries of this warp the tile may matter to: bound against the query
     // point itself not above its threshold
-    const float lbq = tile_lower_bound(tinfo_b + (int64_t)lbt[t] * 8, qpt, qpt);
+    const float* tinf = tring + buf * kTinfoFloats;  // the tile's box, then its sub-boxes
+    const float lbq = tile_lower_bound(tinf, qpt, qpt);
     const unsigned need = __ballot_sync(FULL, valid && !(lbq > tau));
     if (need) {
-      // The queries the tile matters to, compacted in lane order: round r
-      // slot h takes entry r * H + h.  Owner lanes publish their entry and
-      // remember its rank (refreshed thresholds go there too).
-      const int n_need = __popc(need);
-      const int R = (n_need + H - 1) / H;  // rounds per pass
+      constexpr int SPP = QPW >= 16 ? QPW / 16 : 1;  // sub-boxes a pass covers (2 QPW points)
       const int slot = lane / QPW;
       const unsigned my_mask = SLOT_MASK << (slot * QPW);
       const unsigned lt_mask = (1u << lane) - 1u;
-      const int my_rank = (owner && ((need >> lane) & 1u)) ? __popc(need & lt_mask) : -1;
-      const int my_round = my_rank >= 0 ? my_rank / H : -1;
-      const unsigned my_slot_mask = SLOT_MASK << ((my_rank >= 0 ? my_rank % H : 0) * QPW);
-      if (my_rank >= 0) {
-        ctab[my_rank] = make_float4(qx, qy, qz, tau);
-        cidx[my_rank] = lane;
-      }
-      __syncwarp();
 #pragma unroll 1
       for (int pass = 0; pass < NPASS; ++pass) {
-        float2 pr[kRecLen];
-        const int pidx = pass * QPW + (lane & (QPW - 1));
+        // The queries this pass matters to: the tile's, less those whose
+        // bound against the pass's sub-box exceeds their threshold,
+        // compacted in lane order (round r slot h takes entry r * H + h).
+        // Owner lanes publish their entry and keep its rank (refreshed
+        // thresholds go there too).
+        const int sb0 = (2 * pass * QPW) / 32;
+        float lbp = INFINITY;
 #pragma unroll
-        for (int f = 0; f < kRecLen; ++f) pr[f] = tile[f * PPT + pidx];
-        const int i0 = __float_as_int(pr[kRecPad].x), i1 = __float_as_int(pr[kRecPad].y);
-#pragma unroll 1
-        for (int r0 = 0; r0 < R; r0 += 2) {
-          // two rounds per iteration (independent key evaluations in flight)
-          int jr[2];
-          float4 qr[2];
-#pragma unroll
-          for (int u = 0; u < 2; ++u) {
-            const int e = (r0 + u) * H + slot;
-            jr[u] = e < n_need ? cidx[e] : -1;
-            qr[u] = ctab[e < n_need ? e : 0];
+        for (int u = 0; u < SPP; ++u) lbp = fminf(lbp, tile_lower_bound(tinf + 8 * (1 + sb0 + u), qpt, qpt));
+        const unsigned need_p = __ballot_sync(FULL, ((need >> lane) & 1u) && !(lbp > tau));
+        const int n_need = __popc(need_p);
+        const int my_rank = ((need_p >> lane) & 1u) ? __popc(need_p & lt_mask) : -1;
+        if (need_p) {
+          const int R = (n_need + H - 1) / H;  // rounds of this pass
+          const int my_round = my_rank >= 0 ? my_rank / H : -1;
+          const unsigned my_slot_mask = SLOT_MASK << ((my_rank >= 0 ? my_rank % H : 0) * QPW);
+          __syncwarp();  // the previous pass's readers are done with the table
+          if (my_rank >= 0) {
+            ctab[my_rank] = make_float4(qx, qy, qz, tau);
+            cidx[my_rank] = lane;
           }
-          float2 sr[2];
+          __syncwarp();
+          float2 pr[kRecLen];
+          const int pidx = pass * QPW + (lane & (QPW - 1));
 #pragma unroll
-          for (int u = 0; u < 2; ++u)
-            sr[u] = key_pair(make_float2(qr[u].x, qr[u].x), make_float2(qr[u].y, qr[u].y),
-                             make_float2(qr[u].z, qr[u].z), pr);
+          for (int f = 0; f < kRecLen; ++f) pr[f] = tile[f * PPT + pidx];
+          const int i0 = __float_as_int(pr[kRecPad].x), i1 = __float_as_int(pr[kRecPad].y);
+#pragma unroll 1
+          for (int r0 = 0; r0 < R; r0 += 2) {
+            // two rounds per iteration (independent key evaluations in flight)
+            int jr[2];
+            float4 qr[2];
 #pragma unroll
-          for (int u = 0; u < 2; ++u) {
-            if (u == 1 && r0 + 1 >= R) break;  // warp-uniform: no round 1
-            const int j = jr[u];
-            const float2 s2 = sr[u];
-            const bool c0 = j >= 0 && s2.x <= qr[u].w, c1 = j >= 0 && s2.y <= qr[u].w;
-            const unsigned b0 = __ballot_sync(FULL, c0), b1 = __ballot_sync(FULL, c1);
-            if (b0 | b1) {
-              const int n = __popc(b0 & my_mask) + __popc(b1 & my_mask);
-              int c = __shfl_sync(FULL, my_cnt, j >= 0 ? j : 0);
-              if (__any_sync(FULL, j >= 0 && c + n > kQCap)) {  // a queue would overflow: fold every queue first
-                __syncwarp();
-                drain_queue<L>(keys, vals, tie_key, tau, my_cnt, qk, qv, lane);
-                my_cnt = 0;
-                if (owner) qtab[lq].w = tau;
-                if (my_rank >= 0) ctab[my_rank].w = tau;
-                __syncwarp();
-                c = 0;
+            for (int u = 0; u < 2; ++u) {
+              const int e = (r0 + u) * H + slot;
+              jr[u] = e < n_need ? cidx[e] : -1;
+              qr[u] = ctab[e < n_need ? e : 0];
+            }
+            float2 sr[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u)
+              sr[u] = key_pair(make_float2(qr[u].x, qr[u].x), make_float2(qr[u].y, qr[u].y),
+                               make_float2(qr[u].z, qr[u].z), pr);
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              if (u == 1 && r0 + 1 >= R) break;  // warp-uniform: no round 1
+              const int j = jr[u];
+              const float2 s2 = sr[u];
+              const bool c0 = j >= 0 && s2.x <= qr[u].w, c1 = j >= 0 && s2.y <= qr[u].w;
+              const unsigned b0 = __ballot_sync(FULL, c0), b1 = __ballot_sync(FULL, c1);
+              if (b0 | b1) {
+                const int n = __popc(b0 & my_mask) + __popc(b1 & my_mask);
+                int c = __shfl_sync(FULL, my_cnt, j >= 0 ? j : 0);
+                if (__any_sync(FULL, j >= 0 && c + n > kQCap)) {  // a queue would overflow: fold every queue first
+                  __syncwarp();
+                  drain_queue<L>(keys, vals, tie_key, tau, my_cnt, qk, qv, lane);
+                  my_cnt = 0;
+                  if (owner) qtab[lq].w = tau;
+                  if (my_rank >= 0) ctab[my_rank].w = tau;
+                  __syncwarp();
+                  c = 0;
+                }
+                if (c0) {
+                  const int e = queue_slot(j, c + __popc(b0 & my_mask & lt_mask));
+                  qk[e] = s2.x;
+                  qv[e] = i0;
+                }
+                if (c1) {
+                  const int e = queue_slot(j, c + __popc(b0 & my_mask) + __popc(b1 & my_mask & lt_mask));
+                  qk[e] = s2.y;
+                  qv[e] = i1;
+                }
+                if (my_round == r0 + u) my_cnt += __popc(b0 & my_slot_mask) + __popc(b1 & my_slot_mask);
               }
-              if (c0) {
-                const int e = queue_slot(j, c + __popc(b0 & my_mask & lt_mask));
-                qk[e] = s2.x;
-                qv[e] = i0;
-              }
-              if (c1) {
-                const int e = queue_slot(j, c + __popc(b0 & my_mask) + __popc(b1 & my_mask & lt_mask));
-                qk[e] = s2.y;
-                qv[e] = i1;
-              }
-              if (my_round == r0 + u) my_cnt += __popc(b0 & my_slot_mask) + __popc(b1 & my_slot_mask);
             }
           }
         }
-        if ((pass + 1) % H == 0) {  // every query met 64 more points since the last fold
+        if ((pass + 1) % H == 0) {  // every query met at most 64 more points since the last fold
           __syncwarp();
           drain_queue<L>(keys, vals, tie_key, tau, my_cnt, qk, qv, lane);
           my_cnt = 0;
@@ -1084,7 +1098,7 @@ __global__ void __launch_bounds__(32 * WPC) search_f32_kernel(SearchParams a) {
   it.perm_q = a.perm_q + b * a.Q;
   it.rec = a.rec + b * a.P * kRecLen;
   it.pairs = a.pairs + b * (a.P_pad / 2) * kPairFloats;
-  it.tinfo = a.tinfo + b * a.ntile * 8;
+  it.tinfo = a.tinfo + b * a.ntile * kTinfoFloats;
   it.f = a.f + b * a.P * a.F;
   it.f_out = a.f_out + b * a.Q * a.F;
   it.w_out = a.w_out + b * a.Q * a.K;
@@ -1155,7 +1169,7 @@ __global__ void __launch_bounds__(32 * WPC) search_ragged_kernel(SearchParams a)
       it.perm_q = a.perm_q + g.q_off;
       it.rec = crec + c.p_off * kRecLen;
       it.pairs = cpairs + c.tile_off * (kTilePoints / 2) * kPairFloats;
-      it.tinfo = ctinfo + c.tile_off * 8;
+      it.tinfo = ctinfo + c.tile_off * kTinfoFloats;
       it.f = a.f + c.p_off * a.F;
       it.f_out = a.f_out + g.q_off * a.F;
       it.w_out = a.w_out + g.e_off;
@@ -1360,7 +1374,7 @@ FwdLayout fwd_layout(int B, int Q, int P, int K, int dtype, bool own_rec) {
     L.perm_q = off + (size_t)B * P * 4;
     off += align256((size_t)B * P * 4 + (size_t)B * Q * 4);
     L.tinfo = off;
-    off += align256((size_t)B * (L.P_pad / kTilePoints) * 8 * 4);
+    off += align256((size_t)B * (L.P_pad / kTilePoints) * kTinfoBytes);
     L.qseed = off;
     off += align256((size_t)B * Q * 4);
   }

@@ -265,7 +265,8 @@ __device__ double sym3_min_eig(double a00, double a11, double a22, double a01, d
 // reads its pair's 16 fields conflict-free and one packed f32x2 evaluation
 // gives both keys -- (field kRecPad carries the original point index, -1
 // for padding, whose sigma is NaN so its key is never a candidate) and
-// writes tinfo[tile*8] = {min xyz, max xyz, mu, 0}.
+// writes tinfo[tile * kTinfoFloats]: the tile's {min xyz, max xyz, mu, 0},
+// then one such box per warp's 32 points (the sub-boxes).
 __global__ void __launch_bounds__(kTilePoints) tile_info_kernel(const float* __restrict__ rec,
                                                                 const int* __restrict__ perm,
                                                                 const CloudDesc* __restrict__ cd, int P, int ntile,
@@ -340,6 +341,13 @@ __global__ void __launch_bounds__(kTilePoints) tile_info_kernel(const float* __r
     }
     red[warp][6] = mu;
     red[warp][7] = bad ? 1.0f : 0.0f;
+    float* o = tinfo + (g.t0 + t) * kTinfoFloats + 8 * (1 + warp);  // this warp's sub-box
+    for (int a = 0; a < 3; ++a) {
+      o[a] = mn[a];
+      o[3 + a] = mx[a];
+    }
+    o[6] = bad ? -1.0f : mu;  // +inf: no points (the box is empty)
+    o[7] = 0.0f;
   }
   __syncthreads();
   {
@@ -356,7 +364,7 @@ __global__ void __launch_bounds__(kTilePoints) tile_info_kernel(const float* __r
       mu = fminf(mu, red[w][6]);
       bad = bad || red[w][7] != 0.0f;
     }
-    float* o = tinfo + (g.t0 + t) * 8;
+    float* o = tinfo + (g.t0 + t) * kTinfoFloats;
     for (int a = 0; a < 3; ++a) {
       o[a] = mn[a];
       o[3 + a] = mx[a];

@@ -83,8 +83,18 @@ def test_noalloc_other_layouts_and_the_size_limit():
     fn, capi = lib_and_capi()
     dev = torch.device("cuda:0")
     lim = 8 << 20
-    near_P = 59392  # FP32, K=16, Q=512: the largest P whose scratch fits
     L = capi.lib()
+    # FP32, K=16, Q=512: the largest P whose scratch fits (bisection on the
+    # library's own workspace size)
+    lo, hi = 1, 1 << 20
+    while lo < hi:
+        mid = (lo + hi + 1) // 2
+        if L.knnag_forward_workspace_bytes(1, 512, mid, 8, 16, capi.F32) <= lim:
+            lo = mid
+        else:
+            hi = mid - 1
+    near_P = lo
+    assert 50000 < near_P < 70000  # about 140 bytes per point
     assert L.knnag_forward_workspace_bytes(1, 512, near_P, 8, 16, capi.F32) <= lim
     assert L.knnag_forward_workspace_bytes(1, 512, near_P + 1, 8, 16, capi.F32) > lim
     cases = [W.make("small", B=2, Q=300, P=400, F=6, K=9, seed=33, dtype=torch.float64),
