@@ -578,40 +578,58 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     if (P >= NS) {
       const int gl = lane % LG;  // lane within the query's group
       const float2* pairs2 = reinterpret_cast<const float2*>(it.pairs);
+      // two rounds per iteration: both windows' loads in flight together,
+      // then the two sorts interleaved (QPW / GPR is even)
 #pragma unroll 1
-      for (int r = 0; r < QPW / GPR; ++r) {
-        const int jj = r * GPR + lane / LG;  // warp-local query of this group
-        const int center = __shfl_sync(FULL, my_seed, jj);
-        const bool qok = __shfl_sync(FULL, valid, jj);
-        int a0 = center - NS / 2;
-        a0 = (a0 < 0 ? 0 : (a0 > P - NS ? P - NS : a0)) & ~1;
-        const int pos = a0 + 2 * gl;  // even, pos + 1 < P
-        const float2* tp = pairs2 + (int64_t)(pos >> 7) * (PPT * kRecLen) + ((pos & (kTilePoints - 1)) >> 1);
-        float2 pr[kRecLen];
+      for (int r = 0; r < QPW / GPR; r += 2) {
+        int jj[2];
+        bool qok[2];
+        float2 pr[2][kRecLen];
 #pragma unroll
-        for (int f = 0; f < kRecLen; ++f) pr[f] = __ldg(tp + f * PPT);
-        const float4 qq = qtab[warp * QPW + jj];
-        const float2 s2 = key_pair(make_float2(qq.x, qq.x), make_float2(qq.y, qq.y), make_float2(qq.z, qq.z), pr);
-        float v0 = s2.x == s2.x ? s2.x : INFINITY, v1 = s2.y == s2.y ? s2.y : INFINITY;
+        for (int u = 0; u < 2; ++u) {
+          jj[u] = (r + u) * GPR + lane / LG;  // warp-local query of this group
+          const int center = __shfl_sync(FULL, my_seed, jj[u]);
+          qok[u] = __shfl_sync(FULL, valid, jj[u]);
+          int a0 = center - NS / 2;
+          a0 = (a0 < 0 ? 0 : (a0 > P - NS ? P - NS : a0)) & ~1;
+          const int pos = a0 + 2 * gl;  // even, pos + 1 < P
+          const float2* tp = pairs2 + (int64_t)(pos >> 7) * (PPT * kRecLen) + ((pos & (kTilePoints - 1)) >> 1);
+#pragma unroll
+          for (int f = 0; f < kRecLen; ++f) pr[u][f] = __ldg(tp + f * PPT);
+        }
+        float v0[2], v1[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const float4 qq = qtab[warp * QPW + jj[u]];
+          const float2 s2 =
+              key_pair(make_float2(qq.x, qq.x), make_float2(qq.y, qq.y), make_float2(qq.z, qq.z), pr[u]);
+          v0[u] = s2.x == s2.x ? s2.x : INFINITY;
+          v1[u] = s2.y == s2.y ? s2.y : INFINITY;
+        }
         // element e = 2 * gl + h; ascending bitonic network over NS elements
 #pragma unroll
         for (int kk = 2; kk <= NS; kk <<= 1) {
           const bool up = ((2 * gl) & kk) == 0;
 #pragma unroll
           for (int j = kk >> 1; j > 0; j >>= 1) {
-            if (j == 1) {
-              const float lo = fminf(v0, v1), hi = fmaxf(v0, v1);
-              v0 = up ? lo : hi;
-              v1 = up ? hi : lo;
-            } else {
-              const float o0 = __shfl_xor_sync(FULL, v0, j >> 1), o1 = __shfl_xor_sync(FULL, v1, j >> 1);
-              const bool take_min = (((2 * gl) & j) == 0) == up;
-              v0 = take_min ? fminf(v0, o0) : fmaxf(v0, o0);
-              v1 = take_min ? fminf(v1, o1) : fmaxf(v1, o1);
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              if (j == 1) {
+                const float lo = fminf(v0[u], v1[u]), hi = fmaxf(v0[u], v1[u]);
+                v0[u] = up ? lo : hi;
+                v1[u] = up ? hi : lo;
+              } else {
+                const float o0 = __shfl_xor_sync(FULL, v0[u], j >> 1), o1 = __shfl_xor_sync(FULL, v1[u], j >> 1);
+                const bool take_min = (((2 * gl) & j) == 0) == up;
+                v0[u] = take_min ? fminf(v0[u], o0) : fmaxf(v0[u], o0);
+                v1[u] = take_min ? fminf(v1[u], o1) : fmaxf(v1[u], o1);
+              }
             }
           }
         }
-        if (qok && gl == (K >> 1)) qtab[warp * QPW + jj].w = (K & 1) ? v1 : v0;
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+          if (qok[u] && gl == (K >> 1)) qtab[warp * QPW + jj[u]].w = (K & 1) ? v1[u] : v0[u];
       }
     }
     __syncwarp();
@@ -1046,8 +1064,8 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
       const int l = x / C4, c = x - l * C4;
       if (out_f[l]) continue;
       float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-      // eight rows in flight, summed in k order
-      constexpr int RB = 8;
+      // sixteen rows in flight, summed in k order
+      constexpr int RB = 16;
       for (int k0 = 0; k0 < K; k0 += RB) {
         float4 v[RB];
         float w[RB];
