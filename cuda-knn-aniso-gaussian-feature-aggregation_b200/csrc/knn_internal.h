@@ -88,6 +88,12 @@ struct SearchParams {
   // -> a position in the sorted point order near the query (the middle of
   // its cell's points), where the seed window of the threshold is taken
   const int* qseed;
+  // optional (uniform calls): the plan kernels' outputs, read by the search:
+  // seed thresholds per sorted query [B*Q], the CTA items (batch element,
+  // first and end sorted query, 0), and the per-block estimates
+  float* tau0;
+  int4* items;
+  int* plan_est;
 };
 
 // Search CTA: WPC warps (1, 2 or 4), each owning QPW queries (32, 16 or 8;
@@ -166,6 +172,7 @@ struct FwdLayout {
   // [B*cells(+1)], point and query permutations, tile boxes [B*ntile*8]
   size_t bounds, cell_count, cell_offset, perm_p, perm_q, tinfo;
   size_t qseed;  // [B*Q] ints: seed positions of the sorted queries
+  size_t tau0, plan_est, items;  // search plan: seeds [B*Q], estimates, CTA items
   int P_pad, bits;
 };
 int spatial_bits(int P);

@@ -33,10 +33,10 @@
 
 namespace knnag {
 
-// 8 MiB: the forward's scratch is about 138 bytes per point (records, search
-// tiles, spatial-index keys and permutation, tile bounds) plus 12 bytes per
-// query (flag list, query permutation, seed positions): up to ~59k points
-// with few queries, or ~30k points with ~360k queries.
+// 8 MiB: the forward's scratch is about 139 bytes per point (records, search
+// tiles, spatial-index keys and permutation, tile infos) plus 19 bytes per
+// query (flag list, query permutation, seed positions, search plan): up to
+// ~59k points with few queries, or ~30k points with ~230k queries.
 constexpr size_t kNoallocScratchBytes = size_t(8) << 20;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];

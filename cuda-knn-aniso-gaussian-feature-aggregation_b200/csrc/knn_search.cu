@@ -6,6 +6,8 @@
 // (launcher) and csrc/mink.cuh of the reference.
 #include <math.h>
 
+#include <algorithm>
+
 #include "knn_common.cuh"
 #include "knn_internal.h"
 
@@ -441,6 +443,84 @@ __device__ __forceinline__ void drain_queue(float (&keys)[L], int (&vals)[L], fl
   tau = fminf(tau, keys[L - 1]);
 }
 
+// Seed thresholds of a warp's NQ queries (NQ = 8, 16 or 32).  Any K+1
+// distinct points bound a query's (K+1)-th smallest key from above by their
+// own (K+1)-th smallest key, so keys above that can be dropped from the start
+// instead of streaming through the list.  The points are a window of NS
+// points of the sorted order around `my_seed` (held by lane j for query j:
+// the middle of the query's cell, so the window is near it and the bound
+// tight); the half-warp (the warp for NS = 64) of a query evaluates two
+// points per lane and sorts the NS keys (bitonic, NaN as +inf), and the lane
+// holding element K writes the bound into tab[j].w (tab[j] holds the query's
+// x, y, z) for every valid query.  Nothing is written when P < NS.
+template <int KMAX, int NQ>
+__device__ __forceinline__ void seed_warp(float4* tab, int my_seed, bool valid, const float* pairs, int P, int K,
+                                          int lane) {
+  constexpr int NS = KMAX <= 16 ? 32 : 64;  // >= K + 1
+  constexpr int LG = NS / 2;                // lanes per query
+  constexpr int GPR = 32 / LG;              // queries per round
+  constexpr int PPT = kTilePoints / 2;
+  constexpr unsigned FULL = 0xffffffffu;
+  static_assert((NQ / GPR) % 2 == 0, "two rounds per iteration");
+  if (P >= NS) {
+    const int gl = lane % LG;  // lane within the query's group
+    const float2* pairs2 = reinterpret_cast<const float2*>(pairs);
+    // two rounds per iteration: both windows' loads in flight together,
+    // then the two sorts interleaved (NQ / GPR is even)
+#pragma unroll 1
+    for (int r = 0; r < NQ / GPR; r += 2) {
+      int jj[2];
+      bool qok[2];
+      float2 pr[2][kRecLen];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        jj[u] = (r + u) * GPR + lane / LG;  // warp-local query of this group
+        const int center = __shfl_sync(FULL, my_seed, jj[u]);
+        qok[u] = __shfl_sync(FULL, valid, jj[u]);
+        int a0 = center - NS / 2;
+        a0 = (a0 < 0 ? 0 : (a0 > P - NS ? P - NS : a0)) & ~1;
+        const int pos = a0 + 2 * gl;  // even, pos + 1 < P
+        const float2* tp = pairs2 + (int64_t)(pos >> 7) * (PPT * kRecLen) + ((pos & (kTilePoints - 1)) >> 1);
+#pragma unroll
+        for (int f = 0; f < kRecLen; ++f) pr[u][f] = __ldg(tp + f * PPT);
+      }
+      float v0[2], v1[2];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const float4 qq = tab[jj[u]];
+        const float2 s2 =
+            key_pair(make_float2(qq.x, qq.x), make_float2(qq.y, qq.y), make_float2(qq.z, qq.z), pr[u]);
+        v0[u] = s2.x == s2.x ? s2.x : INFINITY;
+        v1[u] = s2.y == s2.y ? s2.y : INFINITY;
+      }
+      // element e = 2 * gl + h; ascending bitonic network over NS elements
+#pragma unroll
+      for (int kk = 2; kk <= NS; kk <<= 1) {
+        const bool up = ((2 * gl) & kk) == 0;
+#pragma unroll
+        for (int j = kk >> 1; j > 0; j >>= 1) {
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            if (j == 1) {
+              const float lo = fminf(v0[u], v1[u]), hi = fmaxf(v0[u], v1[u]);
+              v0[u] = up ? lo : hi;
+              v1[u] = up ? hi : lo;
+            } else {
+              const float o0 = __shfl_xor_sync(FULL, v0[u], j >> 1), o1 = __shfl_xor_sync(FULL, v1[u], j >> 1);
+              const bool take_min = (((2 * gl) & j) == 0) == up;
+              v0[u] = take_min ? fminf(v0[u], o0) : fmaxf(v0[u], o0);
+              v1[u] = take_min ? fminf(v1[u], o1) : fmaxf(v1[u], o1);
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+        if (qok[u] && gl == (K >> 1)) tab[jj[u]].w = (K & 1) ? v1[u] : v0[u];
+    }
+  }
+}
+
 // One search work item: up to WPC * QPW queries of one batch element or
 // segment, all against one cloud.  Pointers are offset to the group already.
 struct SearchItem {
@@ -457,6 +537,7 @@ struct SearchItem {
   int64_t row0;        // global query row of group-local query 0
   int* adj_count;      // the group's per-point entry counts (optional)
   const int* qseed;    // seed positions of the group's sorted queries (optional)
+  const float* tau0;   // or their seed thresholds, from the plan kernel (optional)
   // or seeds from the query's cell: the scanned point counts of the
   // cloud's grid cells (global positions, cell 0 first), its box and grid
   const int* cell_start;
@@ -534,9 +615,12 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   float* out_w = reinterpret_cast<float*>(out_i + NT * L);
   int* out_f = reinterpret_cast<int*>(out_w + NT * L);
 
-  const int lq = warp * QPW + lane;         // query of this (owner) lane within the item
-  const int sp = it.q0 + lq;                // position in the spatial order
-  bool valid = owner && sp < it.q1;
+  // the item's queries split evenly over the warps (m <= QPW each: a split
+  // item gives each warp fewer queries and so a shorter critical path)
+  const int m = (it.q1 - it.q0 + WPC - 1) / WPC;
+  const int lq = warp * QPW + lane;         // slot of this (owner) lane's query within the item
+  const int sp = it.q0 + warp * m + lane;   // position in the spatial order
+  bool valid = owner && lane < m && sp < it.q1;
   int qi = it.perm_q[valid ? sp : it.Q - 1];
   if ((unsigned)qi >= (unsigned)it.Q) {  // the query order is a permutation: never taken
     if (valid) atomicOr(a.status, kStatusBadIndex);
@@ -551,20 +635,13 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
     qtab[lq] = make_float4(qx, qy, qz, valid ? INFINITY : -INFINITY);
   }
 
-  // ---- seed thresholds.  Any K+1 distinct points bound the query's
-  // (K+1)-th smallest key from above by their own (K+1)-th smallest key, so
-  // keys above that can be dropped from the start instead of streaming
-  // through the list.  The points are a window of NS points of the sorted
-  // order around the middle of the query's cell (near the query, so the
-  // bound is tight); the half-warp (the warp for NS = 64) of a query
-  // evaluates two points per lane and sorts the NS keys (bitonic, NaN as
-  // +inf), and the lane holding element K writes the bound into the query
-  // table.
-  const bool seeded = it.qseed || it.cell_start;
-  if (seeded) {
-    constexpr int NS = KMAX <= 16 ? 32 : 64;  // >= K + 1
-    constexpr int LG = NS / 2;                // lanes per query
-    constexpr int GPR = 32 / LG;              // queries per round
+  // ---- seed thresholds (seed_warp): from the plan kernel when it ran,
+  // else computed here from the query's cell
+  const bool seeded = it.tau0 || it.qseed || it.cell_start;
+  if (it.tau0) {  // computed by the plan kernel
+    if (valid) qtab[lq].w = it.tau0[sp];
+    __syncwarp();
+  } else if (seeded) {
     int my_seed = 0;  // the middle of the query's cell in the sorted points
     if (valid) {
       if (it.qseed) {
@@ -575,63 +652,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
       }
     }
     __syncwarp();
-    if (P >= NS) {
-      const int gl = lane % LG;  // lane within the query's group
-      const float2* pairs2 = reinterpret_cast<const float2*>(it.pairs);
-      // two rounds per iteration: both windows' loads in flight together,
-      // then the two sorts interleaved (QPW / GPR is even)
-#pragma unroll 1
-      for (int r = 0; r < QPW / GPR; r += 2) {
-        int jj[2];
-        bool qok[2];
-        float2 pr[2][kRecLen];
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          jj[u] = (r + u) * GPR + lane / LG;  // warp-local query of this group
-          const int center = __shfl_sync(FULL, my_seed, jj[u]);
-          qok[u] = __shfl_sync(FULL, valid, jj[u]);
-          int a0 = center - NS / 2;
-          a0 = (a0 < 0 ? 0 : (a0 > P - NS ? P - NS : a0)) & ~1;
-          const int pos = a0 + 2 * gl;  // even, pos + 1 < P
-          const float2* tp = pairs2 + (int64_t)(pos >> 7) * (PPT * kRecLen) + ((pos & (kTilePoints - 1)) >> 1);
-#pragma unroll
-          for (int f = 0; f < kRecLen; ++f) pr[u][f] = __ldg(tp + f * PPT);
-        }
-        float v0[2], v1[2];
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          const float4 qq = qtab[warp * QPW + jj[u]];
-          const float2 s2 =
-              key_pair(make_float2(qq.x, qq.x), make_float2(qq.y, qq.y), make_float2(qq.z, qq.z), pr[u]);
-          v0[u] = s2.x == s2.x ? s2.x : INFINITY;
-          v1[u] = s2.y == s2.y ? s2.y : INFINITY;
-        }
-        // element e = 2 * gl + h; ascending bitonic network over NS elements
-#pragma unroll
-        for (int kk = 2; kk <= NS; kk <<= 1) {
-          const bool up = ((2 * gl) & kk) == 0;
-#pragma unroll
-          for (int j = kk >> 1; j > 0; j >>= 1) {
-#pragma unroll
-            for (int u = 0; u < 2; ++u) {
-              if (j == 1) {
-                const float lo = fminf(v0[u], v1[u]), hi = fmaxf(v0[u], v1[u]);
-                v0[u] = up ? lo : hi;
-                v1[u] = up ? hi : lo;
-              } else {
-                const float o0 = __shfl_xor_sync(FULL, v0[u], j >> 1), o1 = __shfl_xor_sync(FULL, v1[u], j >> 1);
-                const bool take_min = (((2 * gl) & j) == 0) == up;
-                v0[u] = take_min ? fminf(v0[u], o0) : fmaxf(v0[u], o0);
-                v1[u] = take_min ? fminf(v1[u], o1) : fmaxf(v1[u], o1);
-              }
-            }
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < 2; ++u)
-          if (qok[u] && gl == (K >> 1)) qtab[warp * QPW + jj[u]].w = (K & 1) ? v1[u] : v0[u];
-      }
-    }
+    seed_warp<KMAX, QPW>(qtab + warp * QPW, my_seed, valid, it.pairs, P, K, lane);
     __syncwarp();
   }
 
@@ -647,7 +668,7 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   // ---- box of this CTA's queries and the tile visit order
   {
     float bx[6] = {qx, qy, qz, qx, qy, qz};
-    if (!owner) {
+    if (!valid) {
       bx[0] = bx[1] = bx[2] = INFINITY;
       bx[3] = bx[4] = bx[5] = -INFINITY;
     }
@@ -1110,7 +1131,16 @@ __global__ void __launch_bounds__(32 * WPC) search_f32_kernel(SearchParams a) {
     fence_mbar_init();
   }
   __syncthreads();
-  const int64_t b = blockIdx.y;
+  // the plan kernel's item (batch element, sorted query range), else block
+  // (blockIdx.x, blockIdx.y) of WPC * QPW queries
+  int64_t b = blockIdx.y;
+  int q0 = blockIdx.x * (WPC * QPW), q1 = min(q0 + WPC * QPW, a.Q);
+  if (a.items) {
+    const int4 itm = a.items[blockIdx.x];
+    b = itm.x;
+    q0 = itm.y;
+    q1 = itm.z;
+  }
   SearchItem it;
   it.q = a.q + b * a.Q * 3;
   it.perm_q = a.perm_q + b * a.Q;
@@ -1132,10 +1162,196 @@ __global__ void __launch_bounds__(32 * WPC) search_f32_kernel(SearchParams a) {
   it.P = a.P;
   it.K = a.K;
   it.ntile = a.ntile;
-  it.q0 = blockIdx.x * (WPC * QPW);
-  it.q1 = min(it.q0 + WPC * QPW, a.Q);
+  it.q0 = q0;
+  it.q1 = q1;
+  it.tau0 = a.items ? a.tau0 + b * a.Q : nullptr;
   uint32_t uses[kTileBufs] = {};
   search_item<KMAX, WPC, QPW>(a, it, smem, search_tiles_pow2(a.ntile), uses);
+}
+
+// ------------------------------------------------------------ search plan
+//
+// search_plan_kernel, one CTA per block of qpc sorted queries (grid (nb, B),
+// 16 queries per warp): the seed thresholds of the block's queries
+// (seed_warp) into tau0, and the block's estimate -- the number of tiles
+// whose bound against the block's query box is at most its largest seed,
+// the tiles its search may visit -- into plan_est.
+// search_items_kernel, one CTA of 1024 threads, turns the estimates into the
+// search's CTA items (batch element, query range): blocks ordered by
+// estimate, heaviest first, in kPlanGroups groups of about equal population
+// (block order inside a group), so the heaviest blocks start in the first
+// waves and the light ones fill the last.  The plan runs only when the
+// blocks take more than one wave: in one wave every block starts at once and
+// the order changes nothing (splitting the heaviest blocks over the spare
+// slots of a wave was measured, and gained less than the plan cost).
+// Items only decide which CTA runs which queries: results do not change.
+constexpr int kPlanBins = 1024;
+constexpr int kPlanGroups = 8;
+constexpr int kPlanQPW = 16;              // queries per warp of the plan kernel
+constexpr int kPlanItemsThreads = 1024;
+constexpr int kPlanMaxBlocks = 32768;     // estimates staged in shared memory (128 KB)
+
+// Exclusive scan of one int per thread over the CTA; *total gets the sum.
+// wsum: 33 ints of shared memory.  Every thread of the CTA must call it.
+__device__ __forceinline__ int cta_scan_excl(int v, int* wsum, int* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  int incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const int w = lane < nw ? wsum[lane] : 0;
+    int wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += t;
+    }
+    if (lane < nw) wsum[lane] = wi - w;
+    if (lane == 31) wsum[32] = wi;
+  }
+  __syncthreads();
+  const int r = wsum[warp] + incl - v;
+  *total = wsum[32];
+  __syncthreads();  // wsum is reused by the next call
+  return r;
+}
+
+__device__ __forceinline__ int4 plan_item(int bt, int nb, int qpc, int Q) {
+  const int b = bt / nb, blk = bt - b * nb;
+  const int q0 = blk * qpc;
+  return make_int4(b, q0, min(q0 + qpc, Q), 0);
+}
+
+template <int KMAX>
+__global__ void __launch_bounds__(256) search_plan_kernel(SearchParams a, int qpc, int nb) {
+  constexpr int NQ = kPlanQPW;
+  __shared__ float4 tab[256 / 32 * NQ];
+  __shared__ float red[8][8];
+  __shared__ int wsum[33];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+  const int b = blockIdx.y, blk = blockIdx.x;
+  const int q0 = blk * qpc, q1 = min(q0 + qpc, a.Q);
+  const int sp = q0 + warp * NQ + lane;
+  const bool valid = lane < NQ && sp < q1;
+  const int64_t qrow = (int64_t)b * a.Q;
+  int qi = valid ? a.perm_q[qrow + sp] : 0;
+  if ((unsigned)qi >= (unsigned)a.Q) qi = 0;  // the search flags a bad permutation
+  const float* qb = a.q + qrow * 3;
+  const float x = qb[(int64_t)qi * 3 + 0], y = qb[(int64_t)qi * 3 + 1], z = qb[(int64_t)qi * 3 + 2];
+  if (lane < NQ) tab[warp * NQ + lane] = make_float4(x, y, z, INFINITY);
+  const int my_seed = valid ? a.qseed[qrow + sp] : 0;
+  __syncwarp();
+  seed_warp<KMAX, NQ>(tab + warp * NQ, my_seed, valid, a.pairs + (int64_t)b * (a.P_pad / 2) * kPairFloats, a.P,
+                      a.K, lane);
+  __syncwarp();
+  float t0 = -INFINITY;
+  if (valid) {
+    t0 = tab[warp * NQ + lane].w;
+    a.tau0[qrow + sp] = t0;
+  }
+  // the block's query box and largest seed
+  float v[7] = {valid ? x : INFINITY,  valid ? y : INFINITY,  valid ? z : INFINITY, valid ? x : -INFINITY,
+                valid ? y : -INFINITY, valid ? z : -INFINITY, t0};
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v[c] = fminf(v[c], __shfl_xor_sync(0xffffffffu, v[c], o));
+#pragma unroll
+    for (int c = 3; c < 7; ++c) v[c] = fmaxf(v[c], __shfl_xor_sync(0xffffffffu, v[c], o));
+  }
+  if (lane == 0)
+#pragma unroll
+    for (int c = 0; c < 7; ++c) red[warp][c] = v[c];
+  __syncthreads();
+  float bmin[3], bmax[3], tmax0 = -INFINITY;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    bmin[c] = INFINITY;
+    bmax[c] = -INFINITY;
+  }
+  for (int w = 0; w < nw; ++w) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      bmin[c] = fminf(bmin[c], red[w][c]);
+      bmax[c] = fmaxf(bmax[c], red[w][3 + c]);
+    }
+    tmax0 = fmaxf(tmax0, red[w][6]);
+  }
+  // the tiles the block's search may visit
+  const float* tinfo_b = a.tinfo + (int64_t)b * a.ntile * kTinfoFloats;
+  int c = 0;
+  for (int t = tid; t < a.ntile; t += blockDim.x)
+    c += tile_lower_bound(tinfo_b + (int64_t)t * kTinfoFloats, bmin, bmax) > tmax0 ? 0 : 1;
+  int est;
+  cta_scan_excl(c, wsum, &est);
+  if (tid == 0) a.plan_est[(int64_t)b * nb + blk] = est;
+}
+
+// The item table from the estimates of nbt = B * nb blocks (one CTA of
+// kPlanItemsThreads threads; dynamic shared memory: nbt ints).
+__global__ void __launch_bounds__(kPlanItemsThreads) search_items_kernel(SearchParams a, int nb, int qpc) {
+  extern __shared__ int est[];  // [nbt]
+  __shared__ int hist[kPlanBins];
+  __shared__ int wsum[33];
+  __shared__ int misc[2 * kPlanGroups];
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int nbt = a.B * nb;
+  const int nbins = a.ntile + 1 < kPlanBins ? a.ntile + 1 : kPlanBins;  // estimates are in [0, ntile]
+  for (int i = tid; i < nbt; i += nth) {
+    const int e = a.plan_est[i];
+    est[i] = e < nbins - 1 ? e : nbins - 1;  // the bin
+  }
+  for (int i = tid; i < kPlanBins; i += nth) hist[i] = 0;
+  if (tid < 2 * kPlanGroups) misc[tid] = 0;
+  __syncthreads();
+  for (int i = tid; i < nbt; i += nth) atomicAdd(&hist[est[i]], 1);
+  __syncthreads();
+  // blocks in bins above bin t (heaviest first): one bin per thread
+  const int t = nbins - 1 - tid;  // thread tid holds bin t (tid < nbins)
+  const int h = tid < nbins ? hist[t] : 0;
+  int tot;
+  const int above = cta_scan_excl(h, wsum, &tot);
+  const int chunk = (nbt + nth - 1) / nth;  // thread tid takes blocks [i0, i1) in order
+  const int i0 = min(nbt, tid * chunk), i1 = min(nbt, i0 + chunk);
+  // group of each bin (heaviest bins first), each group's size and first item
+  __syncthreads();  // every thread read its bin's count
+  if (tid < nbins) {
+    const int g = min(kPlanGroups - 1, (int)((int64_t)above * kPlanGroups / nbt));
+    hist[t] = g;
+    atomicAdd(&misc[g], h);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int o = 0;
+    for (int g = 0; g < kPlanGroups; ++g) {
+      misc[kPlanGroups + g] = o;
+      o += misc[g];
+    }
+  }
+  __syncthreads();
+  int cnt[kPlanGroups], base[kPlanGroups];
+#pragma unroll
+  for (int g = 0; g < kPlanGroups; ++g) cnt[g] = 0;
+  for (int i = i0; i < i1; ++i) {
+    const int g = hist[est[i]];
+#pragma unroll
+    for (int u = 0; u < kPlanGroups; ++u) cnt[u] += g == u ? 1 : 0;
+  }
+#pragma unroll
+  for (int g = 0; g < kPlanGroups; ++g) base[g] = misc[kPlanGroups + g] + cta_scan_excl(cnt[g], wsum, &tot);
+  for (int i = i0; i < i1; ++i) {
+    const int g = hist[est[i]];
+    int p = 0;
+#pragma unroll
+    for (int u = 0; u < kPlanGroups; ++u)
+      if (g == u) p = base[u]++;
+    a.items[p] = plan_item(i, nb, qpc, a.Q);
+  }
 }
 
 // Ragged search: a persistent CTA takes work items in order from a counter
@@ -1196,6 +1412,7 @@ __global__ void __launch_bounds__(32 * WPC) search_ragged_kernel(SearchParams a)
       it.row0 = g.q_off;
       it.adj_count = nullptr;
       it.qseed = nullptr;
+      it.tau0 = nullptr;
       it.cell_start = ccell + c.cell_off;
       it.cbox = cbnd + (int64_t)g.cloud * 8;
       it.cbits = c.bits;
@@ -1247,9 +1464,48 @@ int launch_search_t(const SearchParams& a, cudaStream_t st) {
     attr_set[dev] = (int)smem;
   }
   constexpr int QPC = WPC * QPW;
-  dim3 grid((a.Q + QPC - 1) / QPC, a.B);
-  profile_begin(st);
-  search_f32_kernel<KMAX, WPC, QPW><<<grid, 32 * WPC, smem, st>>>(a);
+  const int nb = (a.Q + QPC - 1) / QPC;
+  dim3 grid(nb, a.B);
+  const int64_t nbt = (int64_t)nb * a.B;
+  bool plan = false;
+  if (a.items && nbt <= kPlanMaxBlocks) {
+    // the plan pays when the blocks take more than one wave of the search
+    static int occ_smem[64], occ_val[64];
+    int occ = 0;
+    if (dev >= 0 && dev < 64 && occ_smem[dev] == (int)smem) {
+      occ = occ_val[dev];
+    } else {
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, search_f32_kernel<KMAX, WPC, QPW>, 32 * WPC, smem) !=
+          cudaSuccess)
+        return KNNAG_ERR_CUDA;
+      if (dev >= 0 && dev < 64) {
+        occ_smem[dev] = (int)smem;
+        occ_val[dev] = occ;
+      }
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    plan = nbt > (int64_t)occ * sms;
+  }
+  if (plan) {
+    grid = dim3((unsigned)nbt, 1);
+    static int items_smem[64];
+    if (dev >= 0 && dev < 64 && items_smem[dev] < kPlanMaxBlocks * 4) {
+      if (cudaFuncSetAttribute(search_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kPlanMaxBlocks * 4) != cudaSuccess)
+        return KNNAG_ERR_CUDA;
+      items_smem[dev] = kPlanMaxBlocks * 4;
+    }
+  }
+  SearchParams ap = a;
+  if (!plan) ap.items = nullptr;  // one wave (or too many blocks to plan): the plain grid
+  profile_begin(st);  // the plan does the seed work of the search: timed with it
+  if (plan) {
+    search_plan_kernel<KMAX><<<dim3(nb, a.B), 32 * ((QPC + kPlanQPW - 1) / kPlanQPW), 0, st>>>(ap, QPC, nb);
+    search_items_kernel<<<1, kPlanItemsThreads, (size_t)nbt * 4, st>>>(ap, nb, QPC);
+    note_launches(2);
+  }
+  search_f32_kernel<KMAX, WPC, QPW><<<grid, 32 * WPC, smem, st>>>(ap);
   profile_end(st);
   note_launches(1);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
@@ -1374,7 +1630,8 @@ FwdLayout fwd_layout(int B, int Q, int P, int K, int dtype, bool own_rec) {
   L.rec = off;
   if (own_rec) off += align256((size_t)B * P * kRecLen * esz);
   L.P_pad = (int)round_up(P, kTilePoints);
-  L.pairs = L.bounds = L.cell_count = L.cell_offset = L.perm_p = L.perm_q = L.tinfo = L.qseed = off;
+  L.pairs = L.bounds = L.cell_count = L.cell_offset = L.perm_p = L.perm_q = L.tinfo = L.qseed = L.tau0 =
+      L.plan_est = L.items = off;
   L.bits = 0;
   if (dtype == KNNAG_F32 && K <= 32) {
     L.bits = spatial_bits(P);
@@ -1395,6 +1652,15 @@ FwdLayout fwd_layout(int B, int Q, int P, int K, int dtype, bool own_rec) {
     off += align256((size_t)B * (L.P_pad / kTilePoints) * kTinfoBytes);
     L.qseed = off;
     off += align256((size_t)B * Q * 4);
+    // search plan: seed thresholds, per-block estimates, CTA items (for the
+    // smallest blocks, 8 queries)
+    const size_t nb_max = (size_t)B * ((Q + 7) / 8);
+    L.tau0 = off;
+    off += align256((size_t)B * Q * 4);
+    L.plan_est = off;
+    off += align256(nb_max * 4);
+    L.items = off;
+    off += align256(nb_max * 16);
   }
   L.total = off;
   return L;
@@ -1501,6 +1767,9 @@ int forward_impl(const void* q, const void* p, const void* f, const void* sigma,
   sp.flag_list = flag_list;
   sp.adj_count = adj_count;
   sp.qseed = reinterpret_cast<const int*>(ws + L.qseed);
+  sp.tau0 = reinterpret_cast<float*>(ws + L.tau0);
+  sp.plan_est = reinterpret_cast<int*>(ws + L.plan_est);
+  sp.items = reinterpret_cast<int4*>(ws + L.items);
   apply_search_debug(sp);
   const int G = choose_splits(B, Q, dev);
   {

@@ -103,8 +103,8 @@ int knnag_forward(const void* q, const void* p, const void* f, const void* sigma
  * allocation.  The scratch is one fixed 8 MiB device array inside the
  * library, held by every GPU that loads it until process exit; sizes whose
  * scratch would exceed it return KNNAG_ERR_SCRATCH_LIMIT (the scratch is
- * about 138 bytes per point plus 12 bytes per query: up to ~59k points with
- * few queries, or ~30k points with ~360k queries).  The first call on each device looks the
+ * about 139 bytes per point plus 19 bytes per query: up to ~59k points with
+ * few queries, or ~30k points with ~230k queries).  The first call on each device looks the
  * array's address up (cudaGetSymbolAddress) and should come before any
  * stream capture.  All calls share the array: calls that overlap on the GPU
  * race.  No counterpart in the reference.
