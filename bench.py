@@ -785,8 +785,15 @@ def main():
     ap.add_argument("--workload", default="table", choices=["table", "ragged", "served", "sphere"],
                     help="table: the headline line (with the ragged and served blocks attached); ragged / "
                          "served: only that block, as its own JSON line (for profiling)")
+    ap.add_argument("--search-splits", type=int, default=0,
+                    help="launch shape of the uniform search (knnag_set_search_splits; 0: automatic, "
+                         "128: the tensor-core search), for profiling one kernel")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.search_splits and args.impl == "ours":
+        from cuda_knn_aggregate import capi
+
+        capi.set_search_splits(args.search_splits)
     if args.workload != "table" and args.impl == "ours":
         device = torch.device("cuda", 0)
         torch.cuda.set_device(device)

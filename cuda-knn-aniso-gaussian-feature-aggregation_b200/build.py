@@ -28,9 +28,9 @@ BUILD = os.path.join(HERE, "_build")
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 
-CU_SOURCES = ["knn_search.cu", "knn_spatial.cu", "knn_adjoint.cu", "knn_capi.cu", "knn_noalloc.cu", "knn_variants.cu",
+CU_SOURCES = ["knn_search.cu", "knn_search_tc.cu", "knn_spatial.cu", "knn_adjoint.cu", "knn_capi.cu", "knn_noalloc.cu", "knn_variants.cu",
               "knn_ragged.cu"]
-HEADERS = ["knn_common.cuh", "knn_internal.h", "knn_ragged.h"]
+HEADERS = ["knn_common.cuh", "knn_internal.h", "knn_ragged.h", "knn_search_dev.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"] + ARCH
 

@@ -359,7 +359,7 @@ void knnag_set_profile_events(void* ev_begin, void* ev_end) {
 long long knnag_launch_count(void) { return g_launches.load(); }
 
 int knnag_set_search_splits(int splits) {
-  if (splits != 0 && !search_shape_ok(splits)) return KNNAG_ERR_ARG;
+  if (splits != 0 && !search_setting_ok(splits)) return KNNAG_ERR_ARG;
   g_search_splits.store(splits, std::memory_order_relaxed);
   return KNNAG_OK;
 }

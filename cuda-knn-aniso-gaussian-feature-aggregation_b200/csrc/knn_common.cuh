@@ -45,6 +45,15 @@ constexpr int kSubBoxes = kTilePoints / 32;
 constexpr int kTinfoFloats = 8 * (1 + kSubBoxes);
 constexpr unsigned kTinfoBytes = kTinfoFloats * 4;
 constexpr int kPairFloats = 32;
+// Tensor-core filter, per search tile: the B operand of the approximate-key
+// GEMM (128 points x 32 TF32 values in the no-swizzle K-major core-matrix
+// layout, 16 KB) and 16 floats of error-bound terms (origin, feature
+// bounds, rounding factors).
+constexpr int kTcK = 32;
+constexpr int kTcOpsFloats = kTilePoints * kTcK;
+constexpr unsigned kTcOpsBytes = kTcOpsFloats * 4;
+constexpr int kTcInfoFloats = 16;
+constexpr unsigned kTcInfoBytes = kTcInfoFloats * 4;
 
 __host__ __device__ inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
@@ -132,6 +141,9 @@ __device__ __forceinline__ float2 key_pair(float2 qx2, float2 qy2, float2 qz2, c
   return __ffma2_rn(__fmul2_rn(l, l), pr[kS2],
                     __ffma2_rn(__fmul2_rn(j, j), pr[kS0], __fmul2_rn(__fmul2_rn(k, k), pr[kS1])));
 }
+
+// The TF32 part of x (low 13 mantissa bits cleared); x - tf32_hi(x) is exact.
+__device__ __forceinline__ float tf32_hi(float x) { return __int_as_float(__float_as_int(x) & 0xffffe000); }
 
 // Weight of a key: the reference's fast-math __expf in FP32
 // (csrc/forward.cu:102); full-precision exp in FP64.

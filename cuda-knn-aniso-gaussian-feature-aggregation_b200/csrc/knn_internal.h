@@ -94,6 +94,11 @@ struct SearchParams {
   float* tau0;
   int4* items;
   int* plan_est;
+  // tensor-core filtered search (uniform calls): per tile the B operand of
+  // the approximate-key GEMM [B*ntile][kTcOpsFloats] and its error-bound
+  // terms [B*ntile][kTcInfoFloats], written by the tile-info kernel
+  const float* tcops;
+  const float* tcinfo;
 };
 
 // Search CTA: WPC warps (1, 2 or 4), each owning QPW queries (32, 16 or 8;
@@ -122,6 +127,12 @@ __host__ __device__ inline constexpr int search_qpc(int shape) { return search_w
 inline bool search_shape_ok(int shape) {
   return shape == 1 || shape == 2 || shape == 4 || shape == 8 || shape == 16 || shape == 32 || shape == 64;
 }
+// Launch-shape code of the uniform search that filters candidates with
+// approximate keys from the tensor cores (search_tc_kernel: 128 queries per
+// CTA, one thread per query); uniform calls only (segment tables take the
+// codes above).
+constexpr int kShapeTensorFilter = 128;
+inline bool search_setting_ok(int shape) { return search_shape_ok(shape) || shape == kShapeTensorFilter; }
 
 // Shared-memory layout of the search kernel with `wpc` warps of `qpw` queries:
 //   ring      kTileBufs tiles
@@ -173,11 +184,13 @@ struct FwdLayout {
   size_t bounds, cell_count, cell_offset, perm_p, perm_q, tinfo;
   size_t qseed;  // [B*Q] ints: seed positions of the sorted queries
   size_t tau0, plan_est, items;  // search plan: seeds [B*Q], estimates, CTA items
+  size_t tcops, tcinfo;          // tensor-core filter: per tile B operand and bound terms
   int P_pad, bits;
 };
 int spatial_bits(int P);
+// tc_ops: also write the tensor-core filter's per-tile operands (L.tcops, L.tcinfo)
 int launch_spatial_index(const float* q, const float* rec, int B, int Q, int P, int P_pad, char* ws, const FwdLayout& L,
-                         cudaStream_t st);
+                         cudaStream_t st, bool tc_ops = false);
 int launch_exclusive_scan(int* count, int n, int* out, cudaStream_t st);
 int launch_cloudset_index(char* cs, const CloudSetHeader& h, const CloudDesc* cd_dev, int max_p, int max_ntile,
                           int* cnt, int* perm_p, cudaStream_t st);
@@ -216,6 +229,13 @@ struct AdjLayout {
   size_t rowptr, cursor, unsorted, entries, total;
 };
 AdjLayout adj_layout(int B, int Q, int P, int K);
+
+// Tensor-core filtered search of a uniform FP32 call (knn_search_tc.cu);
+// KNNAG_ERR_TOO_LARGE when its shared memory does not fit (the caller then
+// takes the CUDA-core search).
+int launch_search_tc(const SearchParams& a, cudaStream_t st);
+// Whether the tensor-core search's shared memory fits for `ntile` tiles.
+bool search_tc_fits(int ntile);
 
 // Process-wide split count of the uniform search (0: automatic), set by
 // knnag_set_search_splits (defined in knn_capi.cu).

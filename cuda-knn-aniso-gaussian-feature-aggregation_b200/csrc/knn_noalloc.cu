@@ -33,10 +33,11 @@
 
 namespace knnag {
 
-// 8 MiB: the forward's scratch is about 139 bytes per point (records, search
-// tiles, spatial-index keys and permutation, tile infos) plus 19 bytes per
-// query (flag list, query permutation, seed positions, search plan): up to
-// ~59k points with few queries, or ~30k points with ~230k queries.
+// 8 MiB: the forward's scratch is about 276 bytes per point (records, search
+// tiles, spatial-index keys and permutation, tile infos, the tensor-core
+// filter's tile operands) plus 19 bytes per query (flag list, query
+// permutation, seed positions, search plan): up to ~31k points with few
+// queries, or ~15k points with ~230k queries.
 constexpr size_t kNoallocScratchBytes = size_t(8) << 20;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];

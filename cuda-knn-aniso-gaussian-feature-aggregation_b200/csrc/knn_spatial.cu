@@ -259,6 +259,128 @@ __device__ double sym3_min_eig(double a00, double a11, double a22, double a01, d
   return qm + 2.0 * p * cos(phi + 2.0943951023931957);  // + 2 pi / 3
 }
 
+// Tensor-core filter operands of one tile, by the tile-info CTA (thread k:
+// sorted point k, `real` unless padding; `tile` holds the records field-major,
+// red[w][0..5] the box of warp w's points).  With o the tile's box centre,
+// p' = p - o and M = R^T diag(sigma) R (in double), the point's features
+//   psi = (M00, M11, M22, 2 M01, 2 M02, 2 M12, -2 (M p')_0..2, p'^T M p')
+// meet a query's phi = (x^2, y^2, z^2, xy, xz, yz, x, y, z, 1), (x,y,z) =
+// q - o, in phi . psi = (q - p)^T M (q - p), the key in exact arithmetic.
+// Row k of the B operand holds (hi(psi), lo(psi), hi(psi), 0, 0), hi = psi
+// with its low 13 mantissa bits cleared (a TF32 value), lo = psi - hi (exact);
+// the search's A rows hold (hi(phi), hi(phi), lo(phi), 0, 0), so one K = 32
+// TF32 product sums hi.hi + hi.lo + lo.hi.  Padding rows: psi = (0, .., 1e30).
+// tcinfo: o (3) | 2^-12 max|psi_k| (10) | 1e-5 max nu (13) | max |p'|_1 (14)
+// | 2^-20 max sum|M_ab| (15), nu = sum_a |sigma_a| |R_a|^2; entry 13 is +inf
+// when a value of the tile is not finite (no bound: every point is a
+// candidate).  The search turns these into its error bound.
+__device__ void tc_tile_operand(const float* tile, float (*red)[8], int k, bool real, float* __restrict__ ops,
+                                float* __restrict__ info) {
+  __shared__ float red2[kTilePoints / 32][16];
+  const int lane = k & 31, warp = k >> 5;
+  float o[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float lo = INFINITY, hi = -INFINITY;
+    for (int w = 0; w < kTilePoints / 32; ++w) {
+      lo = fminf(lo, red[w][a]);
+      hi = fmaxf(hi, red[w][3 + a]);
+    }
+    o[a] = (lo <= hi && isfinite(lo) && isfinite(hi)) ? 0.5f * lo + 0.5f * hi : 0.0f;
+  }
+  float psi[10];
+  float nu = 0.f, lam = 0.f, p1 = 0.f;
+  bool bad = false;
+  if (real) {
+    double r[kRecLen];
+#pragma unroll
+    for (int m = 0; m < kRecLen; ++m) r[m] = tile[m * kTilePoints + k];
+    double pp[3], M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, nud = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) pp[a] = -r[kNPX + a] - (double)o[a];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double sg = r[kS0 + a];
+      double rn = 0.0;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        const double ra = r[kR00 + 3 * a + m];
+        rn += ra * ra;
+#pragma unroll
+        for (int n2 = 0; n2 < 3; ++n2) M[m][n2] += sg * ra * r[kR00 + 3 * a + n2];
+      }
+      nud += fabs(sg) * rn;
+    }
+    double mp[3], pmp = 0.0, lamd = 0.0;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      mp[m] = M[m][0] * pp[0] + M[m][1] * pp[1] + M[m][2] * pp[2];
+      pmp += pp[m] * mp[m];
+#pragma unroll
+      for (int n2 = 0; n2 < 3; ++n2) lamd += fabs(M[m][n2]);
+    }
+    const double pd[10] = {M[0][0], M[1][1], M[2][2], 2 * M[0][1], 2 * M[0][2], 2 * M[1][2],
+                           -2 * mp[0], -2 * mp[1], -2 * mp[2], pmp};
+#pragma unroll
+    for (int j = 0; j < 10; ++j) {
+      psi[j] = (float)pd[j];
+      if (!isfinite(psi[j])) bad = true;
+    }
+#pragma unroll
+    for (int m = 0; m < kRecLen - 1; ++m)
+      if (!isfinite(r[m])) bad = true;
+    nu = (float)(nud * (1.0 + 1e-6));
+    lam = (float)(lamd * (1.0 + 1e-6));
+    p1 = (float)((fabs(pp[0]) + fabs(pp[1]) + fabs(pp[2])) * (1.0 + 1e-6));
+    if (!isfinite(nu) || !isfinite(lam) || !isfinite(p1)) bad = true;
+  } else {
+#pragma unroll
+    for (int j = 0; j < 9; ++j) psi[j] = 0.f;
+    psi[9] = 1e30f;
+  }
+  // B row k: (hi, lo, hi, 0, 0) in the core-matrix layout: 8-row groups of
+  // 8 chunks of 4 values, 128 B per (group, chunk)
+  float row[kTcK];
+#pragma unroll
+  for (int j = 0; j < 10; ++j) {
+    const float h = tf32_hi(psi[j]);
+    row[j] = h;
+    row[10 + j] = psi[j] - h;
+    row[20 + j] = h;
+  }
+  row[30] = row[31] = 0.f;
+  float4* dst = reinterpret_cast<float4*>(ops + (k >> 3) * (8 * 32) + (k & 7) * 4);
+#pragma unroll
+  for (int c = 0; c < kTcK / 4; ++c) dst[c * 8] = make_float4(row[4 * c], row[4 * c + 1], row[4 * c + 2], row[4 * c + 3]);
+  // tile maxima of the bound terms over its real points
+  float v[14];
+#pragma unroll
+  for (int j = 0; j < 10; ++j) v[j] = real ? fabsf(psi[j]) : 0.f;
+  v[10] = nu;
+  v[11] = p1;
+  v[12] = lam;
+  v[13] = bad ? 1.f : 0.f;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+    for (int j = 0; j < 14; ++j) v[j] = fmaxf(v[j], __shfl_xor_sync(0xffffffffu, v[j], off));
+  if (lane == 0)
+#pragma unroll
+    for (int j = 0; j < 14; ++j) red2[warp][j] = v[j];
+  __syncthreads();
+  if (k < kTcInfoFloats) {
+    auto tmax = [&](int j) { return fmaxf(fmaxf(red2[0][j], red2[1][j]), fmaxf(red2[2][j], red2[3][j])); };
+    const bool nonfinite = red2[0][13] != 0.f || red2[1][13] != 0.f || red2[2][13] != 0.f || red2[3][13] != 0.f;
+    float out;
+    if (k < 3) out = o[k];
+    else if (k < 13) out = ldexpf(tmax(k - 3), -12);
+    else if (k == 13) out = nonfinite ? INFINITY : 1e-5f * tmax(10);
+    else if (k == 14) out = tmax(11);
+    else out = ldexpf(tmax(12), -20);
+    info[k] = out;
+  }
+}
+
 // One CTA of 128 threads per search tile (tile blockIdx.x of group
 // blockIdx.y), one sorted point per thread: packs the tile field-major --
 // field f of point pair m (points 2m, 2m+1) at float2 f * 64 + m, so a lane
@@ -271,7 +393,9 @@ __global__ void __launch_bounds__(kTilePoints) tile_info_kernel(const float* __r
                                                                 const int* __restrict__ perm,
                                                                 const CloudDesc* __restrict__ cd, int P, int ntile,
                                                                 float* __restrict__ pairs,
-                                                                float* __restrict__ tinfo) {
+                                                                float* __restrict__ tinfo,
+                                                                float* __restrict__ tcops,
+                                                                float* __restrict__ tcinfo) {
   const TileGroup g = tile_group(cd, blockIdx.y, P, ntile);
   const int t = blockIdx.x;
   if (t >= g.ntile) return;
@@ -355,6 +479,7 @@ __global__ void __launch_bounds__(kTilePoints) tile_info_kernel(const float* __r
     float4* dst = reinterpret_cast<float4*>(pairs + (g.t0 + t) * kTilePoints * kRecLen);
     for (int i = k; i < kTilePoints * kRecLen / 4; i += kTilePoints) dst[i] = src[i];
   }
+  if (tcops) tc_tile_operand(tile, red, k, pos < g.P, tcops + (g.t0 + t) * kTcOpsFloats, tcinfo + (g.t0 + t) * kTcInfoFloats);
   if (k == 0) {
     for (int w = 1; w < kTilePoints / 32; ++w) {
       for (int a = 0; a < 3; ++a) {
@@ -388,7 +513,7 @@ unsigned grid_x(int64_t n, int sms, int groups) {
 }  // namespace
 
 int launch_spatial_index(const float* q, const float* rec, int B, int Q, int P, int P_pad, char* ws, const FwdLayout& L,
-                         cudaStream_t st) {
+                         cudaStream_t st, bool tc_ops) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -420,7 +545,9 @@ int launch_spatial_index(const float* q, const float* rec, int B, int Q, int P, 
     if (rc) return rc;
     cell_scatter_kernel<<<grid, 256, 0, st>>>(jp, jq, bnd, off, cnt, perm);
   }
-  tile_info_kernel<<<dim3(ntile, B), kTilePoints, 0, st>>>(rec, perm, nullptr, P, ntile, pairs, tinfo);
+  tile_info_kernel<<<dim3(ntile, B), kTilePoints, 0, st>>>(rec, perm, nullptr, P, ntile, pairs, tinfo,
+                                                            tc_ops ? reinterpret_cast<float*>(ws + L.tcops) : nullptr,
+                                                            tc_ops ? reinterpret_cast<float*>(ws + L.tcinfo) : nullptr);
   note_launches(3);  // + 1 scan, counted by launch_exclusive_scan
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }
@@ -448,7 +575,8 @@ int launch_cloudset_index(char* cs, const CloudSetHeader& h, const CloudDesc* cd
   int rc = launch_exclusive_scan(cnt, h.total_cells, off, st);
   if (rc) return rc;
   cell_scatter_kernel<<<grid, 256, 0, st>>>(jp, jp, bnd, off, cnt, perm_p);
-  tile_info_kernel<<<dim3(max_ntile, C), kTilePoints, 0, st>>>(rec, perm_p, cd_dev, 0, 0, pairs, tinfo);
+  tile_info_kernel<<<dim3(max_ntile, C), kTilePoints, 0, st>>>(rec, perm_p, cd_dev, 0, 0, pairs, tinfo, nullptr,
+                                                                nullptr);
   note_launches(4);  // + 1 scan
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
 }

@@ -5,7 +5,8 @@ The tuned knobs change only the time, never a result:
 * ``splits``, the search launch shape (the C ABI's
   ``knnag_set_search_splits``): 1, 2, 4 -> 4, 2, 1 warps of 32 queries per
   CTA; 8 -> 2 warps of 16 queries; 16 -> 4 warps of 8; 32 -> 1 warp of 16;
-  64 -> 1 warp of 8 -- queries per CTA and per warp;
+  64 -> 1 warp of 8 -- queries per CTA and per warp; 128 -> the tensor-core
+  filtered search (128 queries per CTA, two threads per query);
 * the K register layout: the list length is the K bucket (8, 16, 32) --
   part of the shape bucket, not a free knob.
 
@@ -31,7 +32,7 @@ import torch
 
 from . import capi
 
-SPLITS = (1, 2, 4, 8, 16, 32, 64)
+SPLITS = (1, 2, 4, 8, 16, 32, 64, 128)
 _CACHE: dict = {}      # in-memory: full key -> choice dict
 _LOADED: set = set()   # files already read into _CACHE
 TIMED = {"runs": 0}    # number of candidate timings made in this process

@@ -103,8 +103,8 @@ int knnag_forward(const void* q, const void* p, const void* f, const void* sigma
  * allocation.  The scratch is one fixed 8 MiB device array inside the
  * library, held by every GPU that loads it until process exit; sizes whose
  * scratch would exceed it return KNNAG_ERR_SCRATCH_LIMIT (the scratch is
- * about 139 bytes per point plus 19 bytes per query: up to ~59k points with
- * few queries, or ~30k points with ~230k queries).  The first call on each device looks the
+ * about 276 bytes per point plus 19 bytes per query: up to ~31k points with
+ * few queries, or ~15k points with ~230k queries).  The first call on each device looks the
  * array's address up (cudaGetSymbolAddress) and should come before any
  * stream capture.  All calls share the array: calls that overlap on the GPU
  * race.  No counterpart in the reference.
@@ -348,10 +348,12 @@ long long knnag_launch_count(void);
  * cached per shape bucket): 1, 2, 4 -> CTAs of 4, 2, 1 warps of 32 queries;
  * 8 -> 2 warps of 16 queries; 16 -> 4 warps of 8 queries; 32 -> 1 warp of
  * 16; 64 -> 1 warp of 8 (fewer queries per warp give more warps for small
- * query sets); 0 restores the automatic
- * choice (by the warps the query set gives).  Results do not depend on it.
- * Returns KNNAG_ERR_ARG for other values.  The same codes are the `splits`
- * of segment tables.  No reference counterpart. */
+ * query sets); 128 -> the tensor-core filtered search (approximate keys of
+ * 128 queries x 128 points per tcgen05 MMA, exact keys for the candidates);
+ * 0 restores the automatic choice (the tensor-core search for grids of more
+ * than 8 waves of its CTAs, else by the warps the query set gives).  Results
+ * do not depend on it.  Returns KNNAG_ERR_ARG for other values.  Codes 1-64
+ * are also the `splits` of segment tables.  No reference counterpart. */
 int knnag_set_search_splits(int splits);
 int knnag_get_search_splits(void);
 

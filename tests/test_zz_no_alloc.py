@@ -94,7 +94,7 @@ def test_noalloc_other_layouts_and_the_size_limit():
         else:
             hi = mid - 1
     near_P = lo
-    assert 50000 < near_P < 70000  # about 140 bytes per point
+    assert 25000 < near_P < 40000  # about 276 bytes per point
     assert L.knnag_forward_workspace_bytes(1, 512, near_P, 8, 16, capi.F32) <= lim
     assert L.knnag_forward_workspace_bytes(1, 512, near_P + 1, 8, 16, capi.F32) > lim
     cases = [W.make("small", B=2, Q=300, P=400, F=6, K=9, seed=33, dtype=torch.float64),
