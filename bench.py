@@ -580,7 +580,7 @@ def fp32_peak_tflops(device):
 # profiles/search_f32_table.md (dram__bytes_read.sum + dram__bytes_write.sum
 # of one launch); update it with that summary whenever the search kernel
 # changes.
-SEARCH_TRAFFIC_BYTES = 3226112
+SEARCH_TRAFFIC_BYTES = 3230720
 SEARCH_TRAFFIC_SOURCE = "ncu capture of one search_f32_kernel<16,2,16> launch (profiles/search_f32_table.md)"
 
 CONFIG = {"workload": "table: B=2 Q=12288 P=4096 F=64 K=16, fwd + dq(create_graph) + Eikonal backward",

@@ -236,6 +236,13 @@ AdjLayout adj_layout(int B, int Q, int P, int K);
 int launch_search_tc(const SearchParams& a, cudaStream_t st);
 // Whether the tensor-core search's shared memory fits for `ntile` tiles.
 bool search_tc_fits(int ntile);
+// The search plan (knn_search.cu) for blocks of qpc sorted queries, nb per
+// batch element: seed thresholds into a.tau0, the blocks' estimates into
+// a.plan_est, the CTA items, heaviest first, into a.items.
+int launch_search_plan(const SearchParams& a, int qpc, int nb, cudaStream_t st);
+// Most blocks the plan orders (its estimates are staged in shared memory).
+int search_plan_max_blocks();
+int num_sms(int dev);
 
 // Process-wide split count of the uniform search (0: automatic), set by
 // knnag_set_search_splits (defined in knn_capi.cu).

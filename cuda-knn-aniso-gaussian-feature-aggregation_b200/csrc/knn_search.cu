@@ -484,9 +484,20 @@ __device__ __forceinline__ bool search_item(const SearchParams& a, const SearchI
   }
 
   // MinK's fill phase stores points 0..K-1 whatever their key: a NaN there
-  // changes the result in ways only the replay reproduces.
+  // changes the result in ways only the replay reproduces.  With those
+  // records finite and at most 1e6 in magnitude, and the query too, no key
+  // can overflow or be NaN (|key| < 1.2e32), so the keys are evaluated only
+  // otherwise (lane i checks record i, K <= 32).
+  bool fill_ok = true;
+  if (lane < K) {
+    float r[kRecLen];
+    load_rec(recb + (int64_t)lane * kRecLen, r);
+#pragma unroll
+    for (int m = 0; m < kRecLen - 1; ++m) fill_ok = fill_ok && fabsf(r[m]) <= 1e6f;  // NaN fails
+  }
+  fill_ok = __all_sync(FULL, fill_ok) && fabsf(qx) <= 1e6f && fabsf(qy) <= 1e6f && fabsf(qz) <= 1e6f;
   bool nan_fill = false;
-  if (owner)
+  if (owner && !fill_ok)
     for (int i = 0; i < K; ++i) {
       const float s = key_rec<float>(qx, qy, qz, recb + (int64_t)i * kRecLen);
       if (s != s) nan_fill = true;
@@ -1264,8 +1275,6 @@ __global__ void __launch_bounds__(32 * WPC) search_ragged_kernel(SearchParams a)
 
 // ------------------------------------------------------------------ host
 
-namespace {
-
 int num_sms(int dev) {
   static int cache[64] = {0};
   if (dev < 0 || dev >= 64) return 148;
@@ -1276,6 +1285,8 @@ int num_sms(int dev) {
   }
   return cache[dev];
 }
+
+namespace {
 
 template <int KMAX, int WPC, int QPW>
 int launch_search_t(const SearchParams& a, cudaStream_t st) {
@@ -1426,6 +1437,33 @@ inline unsigned grid_for(int64_t n, int threads, int dev) {
 }
 
 }  // namespace
+
+int search_plan_max_blocks() { return kPlanMaxBlocks; }
+
+int launch_search_plan(const SearchParams& a, int qpc, int nb, cudaStream_t st) {
+  const int64_t nbt = (int64_t)nb * a.B;
+  if (nbt > kPlanMaxBlocks || !a.items || !a.tau0 || !a.plan_est) return KNNAG_ERR_ARG;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  static int items_smem[64];
+  if (dev >= 0 && dev < 64 && items_smem[dev] < kPlanMaxBlocks * 4) {
+    if (cudaFuncSetAttribute(search_items_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPlanMaxBlocks * 4) !=
+        cudaSuccess)
+      return KNNAG_ERR_CUDA;
+    items_smem[dev] = kPlanMaxBlocks * 4;
+  }
+  const dim3 grid((unsigned)nb, (unsigned)a.B);
+  const unsigned threads = 32 * ((qpc + kPlanQPW - 1) / kPlanQPW);
+  if (a.K <= 8)
+    search_plan_kernel<8><<<grid, threads, 0, st>>>(a, qpc, nb);
+  else if (a.K <= 16)
+    search_plan_kernel<16><<<grid, threads, 0, st>>>(a, qpc, nb);
+  else
+    search_plan_kernel<32><<<grid, threads, 0, st>>>(a, qpc, nb);
+  search_items_kernel<<<1, kPlanItemsThreads, (size_t)nbt * 4, st>>>(a, nb, qpc);
+  note_launches(2);
+  return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
+}
 
 template <typename T>
 int launch_exact(const ExactParams<T>& a, cudaStream_t st) {

@@ -199,7 +199,16 @@ __global__ void __launch_bounds__(kTcThreads, KMAX <= 16 ? 2 : 1) search_tc_kern
   tc_fence_after();
   const uint32_t tmem = *s_tmem;
 
-  const int64_t b = blockIdx.y;
+  // the plan's item (batch element, sorted query range) when the plan ran,
+  // else block (blockIdx.x, blockIdx.y) of 128 queries
+  int64_t b = blockIdx.y;
+  int q0 = blockIdx.x * kTcQ, q1 = min(q0 + kTcQ, a.Q);
+  if (a.items) {
+    const int4 itm = a.items[blockIdx.x];
+    b = itm.x;
+    q0 = itm.y;
+    q1 = itm.z;
+  }
   const int Q = a.Q, P = a.P, K = a.K, ntile = a.ntile;
   const float* rec_b = a.rec + b * P * kRecLen;
   const float* pairs_b = a.pairs + b * (a.P_pad / 2) * kPairFloats;
@@ -208,8 +217,8 @@ __global__ void __launch_bounds__(kTcThreads, KMAX <= 16 ? 2 : 1) search_tc_kern
   const float* tcinfo_b = a.tcinfo + b * ntile * kTcInfoFloats;
 
   // ---- this thread's query (sorted position sp of batch element b)
-  const int sp = blockIdx.x * kTcQ + qs;
-  bool valid = sp < Q;
+  const int sp = q0 + qs;
+  bool valid = sp < q1;
   int qi = a.perm_q[b * Q + (valid ? sp : Q - 1)];
   if ((unsigned)qi >= (unsigned)Q) {  // the query order is a permutation: never taken
     if (valid && half == 0) atomicOr(a.status, kStatusBadIndex);
@@ -239,11 +248,14 @@ __global__ void __launch_bounds__(kTcThreads, KMAX <= 16 ? 2 : 1) search_tc_kern
     if (lane == 0) *s_fillok = ok ? 1 : 0;
   }
   __syncthreads();
-  // seeds: warp w computes those of queries 32 (w % 4) + 16 h .. + 15
-  {
+  if (a.items) {
+    // seeds from the plan kernel
+    if (half == 0 && valid) qtab[qs].w = a.tau0[b * Q + sp];
+  } else {
+    // seeds: warp w computes those of queries 32 (w % 4) + 16 h .. + 15
     const int g0 = 32 * sub + 16 * half;
     const int sq = g0 + (lane & 15);
-    const int ssp = blockIdx.x * kTcQ + sq;
+    const int ssp = q0 + sq;
     const bool sval = lane < 16 && qorig[sq] >= 0;
     const int my_seed = sval ? a.qseed[b * Q + ssp] : 0;
     seed_warp<KMAX, 16>(qtab + g0, my_seed, sval, pairs_b, P, K, lane);
@@ -683,8 +695,8 @@ __global__ void __launch_bounds__(kTcThreads, KMAX <= 16 ? 2 : 1) search_tc_kern
 }
 
 template <int KMAX>
-int launch_tc_t(const SearchParams& a, cudaStream_t st) {
-  const size_t smem = tc_smem_bytes(a.ntile);
+int launch_tc_t(const SearchParams& a0, cudaStream_t st) {
+  const size_t smem = tc_smem_bytes(a0.ntile);
   if (smem > 227 * 1024) return KNNAG_ERR_TOO_LARGE;
   static int attr_set[64] = {0};  // largest size already allowed, per device
   int dev = 0;
@@ -695,8 +707,24 @@ int launch_tc_t(const SearchParams& a, cudaStream_t st) {
       return KNNAG_ERR_CUDA;
     attr_set[dev] = (int)smem;
   }
-  const dim3 grid((unsigned)((a.Q + kTcQ - 1) / kTcQ), (unsigned)a.B);
-  profile_begin(st);
+  // Grids of more than one wave run the search plan first (seeds and the
+  // blocks' tile estimates, then the blocks ordered heaviest first), so the
+  // last waves hold light blocks; in one wave every block starts at once.
+  const int nb = (a0.Q + kTcQ - 1) / kTcQ;
+  const int64_t nbt = (int64_t)nb * a0.B;
+  SearchParams a = a0;
+  const bool plan = a.items && a.tau0 && a.plan_est && nbt <= search_plan_max_blocks() &&
+                    nbt > (int64_t)(KMAX <= 16 ? 2 : 1) * num_sms(dev);
+  if (!plan) a.items = nullptr;
+  const dim3 grid = plan ? dim3((unsigned)nbt, 1) : dim3((unsigned)nb, (unsigned)a.B);
+  profile_begin(st);  // the plan does the seed work of the search: timed with it
+  if (plan) {
+    const int rc = launch_search_plan(a, kTcQ, nb, st);
+    if (rc) {
+      profile_end(st);
+      return rc;
+    }
+  }
   search_tc_kernel<KMAX><<<grid, kTcThreads, smem, st>>>(a);
   profile_end(st);
   note_launches(1);
