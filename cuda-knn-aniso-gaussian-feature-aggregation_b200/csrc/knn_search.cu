@@ -158,6 +158,7 @@ __device__ void bubble_sort_slots(T* sk, int* sv, int size) {
 template <typename T>
 __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams<T> a) {
   constexpr int CH = replay_chunk<T>();
+  constexpr int HC = CH / 2;  // keys per chunk: two chunk buffers
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* skey = reinterpret_cast<T*>(smem_raw);
@@ -215,24 +216,91 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
 
     int size = 0, max_idx = 0, my_v = -1;
     T max_key = T(0), my_k = T(0);
-    for (int c0 = 0; c0 < P; c0 += CH) {
-      const int n = min(CH, P - c0);
+    // Keys of chunk [c0, c0 + HC) into buf by threads first .. first + nth - 1
+    // (four keys in flight per thread).
+    auto fill = [&](int c0, T* buf, int first, int nth) {
+      const int n = min(HC, P - c0);
       if (a.iso_p) {
         // squared Euclidean distance, accumulated as d = 0; d += c*c (csrc/forward.cu:32-36)
         const T* pb = a.iso_p + b * (int64_t)P * 3;
-        for (int i = tid; i < n; i += kReplayThreads) {
+#pragma unroll 4
+        for (int i = tid - first; i < n; i += nth) {
           const T* pp = pb + (int64_t)(c0 + i) * 3;
           const T x = qx - pp[0], y = qy - pp[1], z = qz - pp[2];
-          skey[i] = fma_rn(z, z, fma_rn(y, y, mul_rn(x, x)));
+          buf[i] = fma_rn(z, z, fma_rn(y, y, mul_rn(x, x)));
         }
       } else {
-        for (int i = tid; i < n; i += kReplayThreads) skey[i] = key_rec<T>(qx, qy, qz, recb + (int64_t)(c0 + i) * kRecLen);
+#pragma unroll 4
+        for (int i = tid - first; i < n; i += nth) buf[i] = key_rec<T>(qx, qy, qz, recb + (int64_t)(c0 + i) * kRecLen);
       }
-      __syncthreads();
-      if (warp == 0) {
-        for (int base = 0; base < n; base += 32) {
+    };
+    // Two chunk buffers: while warp 0 runs MinK over chunk c in index order,
+    // the other warps compute the keys of chunk c + 1.
+    fill(0, skey, 0, kReplayThreads);
+    __syncthreads();
+    for (int c0 = 0, ci = 0; c0 < P; c0 += HC, ++ci) {
+      const int n = min(HC, P - c0);
+      const T* cur = skey + (ci & 1) * HC;
+      if (warp != 0) {
+        if (c0 + HC < P) fill(c0 + HC, skey + ((ci + 1) & 1) * HC, 32, kReplayThreads - 32);
+      } else {
+        // An accepted key kl (strictly below the max) at point index idx
+        // replaces the max slot; the max is found again.
+        auto accept = [&](T kl, int idx) {
+          if (in_lanes) {
+            if (lane == max_idx) {
+              my_k = kl;
+              my_v = idx;
+            }
+            const T v = (lane < K && my_k > kl) ? my_k : T(-INFINITY);
+            const T m = warp_max(v);
+            if (m > kl) {
+              max_key = m;
+              max_idx = __ffs(__ballot_sync(FULL, lane < K && v == m)) - 1;
+            } else {
+              max_key = kl;
+            }
+          } else {
+            if (lane == 0) {
+              slot_k[max_idx] = kl;
+              slot_v[max_idx] = idx;
+            }
+            __syncwarp();
+            max_key = kl;
+            for (int s2 = 0; s2 < K; ++s2) {
+              const T c = slot_k[s2];
+              if (c > max_key) {
+                max_key = c;
+                max_idx = s2;
+              }
+            }
+            __syncwarp();
+          }
+        };
+        for (int base = 0; base < n;) {
+          if (size >= K && base + 128 <= n) {
+            // full list: 128 keys per step, lane l holding keys 4l .. 4l+3;
+            // candidates in index order (lanes ascending, then t), each
+            // checked against the max at its turn
+            T k4[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) k4[t] = cur[base + 4 * lane + t];
+            const bool any = k4[0] < max_key || k4[1] < max_key || k4[2] < max_key || k4[3] < max_key;
+            unsigned cand = __ballot_sync(FULL, any);
+            while (cand) {
+              const int l = __ffs(cand) - 1;
+              cand &= cand - 1;
+#pragma unroll
+              for (int t = 0; t < 4; ++t) {
+                const T kl = __shfl_sync(FULL, k4[t], l);
+                if (kl < max_key) accept(kl, c0 + base + 4 * l + t);
+              }
+            }
+            base += 128;
+            continue;
+          }
           const int nvalid = min(32, n - base);
-          const T key = lane < nvalid ? skey[base + lane] : T(0);
+          const T key = lane < nvalid ? cur[base + lane] : T(0);
           int j = 0;
           while (j < nvalid && size < K) {  // fill phase (uniform across the warp)
             const T kj = __shfl_sync(FULL, key, j);
@@ -260,37 +328,10 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
               cand &= cand - 1;
               const T kl = __shfl_sync(FULL, key, l);
               if (!(kl < max_key)) continue;
-              if (in_lanes) {
-                if (lane == max_idx) {
-                  my_k = kl;
-                  my_v = c0 + base + l;
-                }
-                const T v = (lane < K && my_k > kl) ? my_k : T(-INFINITY);
-                const T m = warp_max(v);
-                if (m > kl) {
-                  max_key = m;
-                  max_idx = __ffs(__ballot_sync(FULL, lane < K && v == m)) - 1;
-                } else {
-                  max_key = kl;
-                }
-              } else {
-                if (lane == 0) {
-                  slot_k[max_idx] = kl;
-                  slot_v[max_idx] = c0 + base + l;
-                }
-                __syncwarp();
-                max_key = kl;
-                for (int s2 = 0; s2 < K; ++s2) {
-                  const T c = slot_k[s2];
-                  if (c > max_key) {
-                    max_key = c;
-                    max_idx = s2;
-                  }
-                }
-                __syncwarp();
-              }
+              accept(kl, c0 + base + l);
             }
           }
+          base += 32;
         }
       }
       __syncthreads();
