@@ -155,8 +155,8 @@ __device__ void bubble_sort_slots(T* sk, int* sv, int size) {
       }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams<T> a) {
+template <typename T, int NTH>
+__global__ void __launch_bounds__(NTH) mink_replay_kernel(ExactParams<T> a) {
   constexpr int CH = replay_chunk<T>();
   constexpr int HC = CH / 2;  // keys per chunk: two chunk buffers
   constexpr unsigned FULL = 0xffffffffu;
@@ -236,13 +236,13 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
     };
     // Two chunk buffers: while warp 0 runs MinK over chunk c in index order,
     // the other warps compute the keys of chunk c + 1.
-    fill(0, skey, 0, kReplayThreads);
+    fill(0, skey, 0, NTH);
     __syncthreads();
     for (int c0 = 0, ci = 0; c0 < P; c0 += HC, ++ci) {
       const int n = min(HC, P - c0);
       const T* cur = skey + (ci & 1) * HC;
       if (warp != 0) {
-        if (c0 + HC < P) fill(c0 + HC, skey + ((ci + 1) & 1) * HC, 32, kReplayThreads - 32);
+        if (c0 + HC < P) fill(c0 + HC, skey + ((ci + 1) & 1) * HC, 32, NTH - 32);
       } else {
         // An accepted key kl (strictly below the max) at point index idx
         // replaces the max slot; the max is found again.
@@ -361,13 +361,13 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
       // isotropic weights w_k = exp(-(d_k * sigma[idx_k][0])) and their sum
       // in k order (csrc/forward.cu:43-52); keep w_k in slot_k
       const T* sg = a.iso_sigma + b * (int64_t)P * a.iso_stride;
-      for (int k = tid; k < K; k += kReplayThreads) {
+      for (int k = tid; k < K; k += NTH) {
         const int64_t e = e0 + k;
         a.dists[e] = slot_k[k];
         a.idxs[e] = (int64_t)slot_v[k];
       }
       __syncthreads();
-      for (int k = tid; k < K; k += kReplayThreads)
+      for (int k = tid; k < K; k += NTH)
         slot_k[k] = weight_of(mul_rn(slot_k[k], sg[(int64_t)slot_v[k] * a.iso_stride]));
       __syncthreads();
       if (tid == 0) {
@@ -376,7 +376,7 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
         a.w_out[bq] = ws;
       }
     } else {
-      for (int k = tid; k < K; k += kReplayThreads) {
+      for (int k = tid; k < K; k += NTH) {
         const int64_t e = e0 + k;
         a.dists[e] = slot_k[k];
         a.idxs[e] = (int64_t)slot_v[k];
@@ -384,10 +384,10 @@ __global__ void __launch_bounds__(kReplayThreads) mink_replay_kernel(ExactParams
         if (a.adj_count && (unsigned)slot_v[k] < (unsigned)P) atomicAdd(&a.adj_count[b * P + slot_v[k]], 1);
       }
       __syncthreads();
-      for (int k = tid; k < K; k += kReplayThreads) slot_k[k] = weight_of(slot_k[k]);
+      for (int k = tid; k < K; k += NTH) slot_k[k] = weight_of(slot_k[k]);
       __syncthreads();
     }
-    for (int c = tid; c < F; c += kReplayThreads) {
+    for (int c = tid; c < F; c += NTH) {
       T acc = T(0);
       for (int k = 0; k < K; ++k) acc = fma_rn(fb[(int64_t)slot_v[k] * F + c], slot_k[k], acc);
       a.f_out[bq * F + c] = acc;
@@ -1510,9 +1510,13 @@ template <typename T>
 int launch_exact(const ExactParams<T>& a, cudaStream_t st) {
   const size_t smem = (size_t)replay_chunk<T>() * sizeof(T) + (size_t)a.K * (sizeof(T) + sizeof(int));
   if (smem > 200 * 1024) return KNNAG_ERR_TOO_LARGE;
-  if (smem > 48 * 1024 &&
-      cudaFuncSetAttribute(mink_replay_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-          cudaSuccess)
+  // A list of flagged queries is short: 512 threads per CTA, fifteen warps
+  // computing keys beside the warp that runs MinK.  Every query of a call:
+  // 256 threads, more queries per SM at once.
+  auto kernel = a.use_list ? mink_replay_kernel<T, 2 * kReplayThreads> : mink_replay_kernel<T, kReplayThreads>;
+  const int threads = a.use_list ? 2 * kReplayThreads : kReplayThreads;
+  if (smem > 48 * 1024 && cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+                              cudaSuccess)
     return KNNAG_ERR_CUDA;
   int dev = 0;
   cudaGetDevice(&dev);
@@ -1526,7 +1530,7 @@ int launch_exact(const ExactParams<T>& a, cudaStream_t st) {
   }
   if (blocks < 1) blocks = 1;
   if (!a.use_list) profile_begin(st);
-  mink_replay_kernel<T><<<(unsigned)blocks, kReplayThreads, smem, st>>>(a);
+  kernel<<<(unsigned)blocks, threads, smem, st>>>(a);
   if (!a.use_list) profile_end(st);
   note_launches(1);
   return cudaGetLastError() == cudaSuccess ? KNNAG_OK : KNNAG_ERR_CUDA;
