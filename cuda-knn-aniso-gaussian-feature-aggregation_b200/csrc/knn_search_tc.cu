@@ -11,7 +11,7 @@
 //      high part and an FP32 remainder, and the K = 32 product sums
 //      hi.hi + hi.lo + lo.hi, accurate to about 2^-20 of sum |phi_k psi_k|;
 //   2. a rigorous bound E(q, tile) on |approximate - exact| (the GEMM's error
-//      with a 16x margin, the rounding of the exact FP32 key, the rounding of
+//      with a 32x margin, the rounding of the exact FP32 key, the rounding of
 //      q - o); a point is a candidate when its approximate key is at most
 //      the query's threshold + E (NaN: always), so every point whose exact
 //      key is at most the threshold is a candidate;
@@ -22,8 +22,8 @@
 //
 // Results are the CUDA-core search's: the same list, the same exactness
 // flags (ties, empty slots, NaN in MinK's fill phase -> the exact replay),
-// the same epilogue.  One CTA of 128 threads holds 128 sorted queries (one
-// TMEM lane each); tiles arrive by 1-D bulk copies (no multicast) on
+// the same epilogue.  One CTA of 256 threads holds 128 sorted queries (one
+// TMEM lane and two threads each); tiles arrive by 1-D bulk copies (no multicast) on
 // mbarriers with bounded waits; the TMEM accumulator (128 columns) is
 // allocated at the start and freed on every exit path.
 #include <math.h>
